@@ -1,0 +1,413 @@
+"""Benchmark of the VecGeom hot path on B200: Mpoints/s per shape op.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl vgb|reference]
+                    [--workload shapes|box] [--precision fp64|fp32r]
+
+One step = every (shape, op) pair of the workload run once over its whole
+point batch through libvgb.  Workloads (seeded synthetic inputs):
+  shapes  tube (rmin 5, rmax 20, dz 30, phi 0-270 deg), cone (0/10, 5/20,
+          dz 25) and sphere (rmin 10, rmax 30, theta 0-90 deg), 2^22 points each,
+          1/3 inside, 1/3 outside in a 1.5x box, 1/3 within 1e-6 mm of the
+          surface, isotropic directions; Inside, Contains, SafetyToIn,
+          DistanceToIn on all points, SafetyToOut and DistanceToOut on the
+          points Contains() accepts.
+  box     box (10, 20, 30) mm, 2^20 points uniform in 1.5x the box; the same
+          ops (DistanceToOut/SafetyToOut on the inside subset).
+value = point-ops / device time (inputs resident in HBM, L2 flushed before
+every op, CUDA events around each launch); e2e = the same ops through the
+public API with pinned host buffers (copies inside the timed region).
+Rank 0 prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+# algorithmic bytes per point through the FP64 SOA API
+BYTES = {"contains": 25, "inside": 28, "safety_to_in": 32, "safety_to_out": 32,
+         "distance_to_in": 64, "distance_to_out": 64}
+OPS = ("inside", "contains", "safety_to_in", "safety_to_out", "distance_to_in",
+       "distance_to_out")
+LOCAL_OPS = ("safety_to_out", "distance_to_out")   # run on the Contains() subset
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="vgb", choices=["vgb", "reference"])
+    ap.add_argument("--workload", default="shapes", choices=["shapes", "box"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32r"])
+    ap.add_argument("--n", type=int, default=0, help="points per shape (0 = workload default)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def workload_shapes(name: str):
+    from vecgeom_b200 import workloads as W
+    if name == "box":
+        return {"box": W.config1_box()}, 1 << 20, "uniform"
+    return W.config2_shapes(), 1 << 22, "mixed"
+
+
+def workload_desc(name, n, precision):
+    if name == "box":
+        return {"workload": "box (10,20,30) mm fp64, 2^20 uniform points in 1.5x box",
+                "points_per_shape": n, "ops": list(OPS), "precision": precision}
+    return {"workload": "tube/cone/sphere, 2^22 mixed points each (1/3 in, 1/3 out, "
+                        "1/3 within 1e-6 mm of the surface)",
+            "shapes": ["tube(5,20,30,0-270deg)", "cone(0,10,5,20,25)", "sphere(10,30,th 0-90deg)"],
+            "points_per_shape": n, "ops": list(OPS), "precision": precision}
+
+
+# ---------------------------------------------------------------------------
+# clocks
+# ---------------------------------------------------------------------------
+
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": float(max(smax)) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the reference Scalar backend (oracle/_ref) or the C oracle
+# ---------------------------------------------------------------------------
+
+def cpu_rate(shapes: dict, n_total: int, seed: int, budget_s: float = 12.0) -> dict:
+    """Point-ops/s of the reference on this host's cores, all threads, on a
+    bounded sample (the first points of the same workload)."""
+    import oracle
+    from oracle import oracle_unplaced, ref_unplaced
+    from vecgeom_b200 import workloads as W
+    threads = os.cpu_count() or 1
+    use_ref = oracle.RefLib.available()
+    kind = "reference" if use_ref else "port"
+    sample = min(n_total, 1 << 18)
+    per = budget_s / (len(shapes) * len(OPS))
+    tot_pts, tot_t = 0, 0.0
+    if use_ref:
+        ref = oracle.RefLib()
+    else:
+        orc = oracle.Oracle()
+        threads = 1
+    for si, (name, spec) in enumerate(shapes.items()):
+        wl = W.make_workload(spec, sample, seed + si, mix="uniform" if name == "box" else "mixed")
+        pts = (wl.x, wl.y, wl.z)
+        dirs = (wl.dx, wl.dy, wl.dz)
+        if use_ref:
+            pv = ref.placed(ref_unplaced(ref, spec))
+            run = lambda op, p, d, s: ref.batch(pv, op, p, d, s, nthreads=threads)  # noqa
+        else:
+            sh = oracle_unplaced(orc, spec)
+            xf = orc.xform()
+            run = lambda op, p, d, s: orc.batch(sh, xf, op, p, d, s)  # noqa
+        inside = run(oracle.CONTAINS, pts, None, None).astype(bool)
+        sub = tuple(np.ascontiguousarray(a[inside]) for a in pts)
+        subd = tuple(np.ascontiguousarray(a[inside]) for a in dirs)
+        for opname in OPS:
+            op = getattr(oracle, opname.upper())
+            p, d = (sub, subd) if opname in LOCAL_OPS else (pts, dirs)
+            use_dir = opname.startswith("distance")
+            m = len(p[0])
+            st = np.full(m, 1e30)
+            reps, t0 = 0, time.perf_counter()
+            while True:
+                run(op, p, d if use_dir else None, st if use_dir else None)
+                reps += 1
+                el = time.perf_counter() - t0
+                if el >= per:
+                    break
+            tot_pts += reps * m
+            tot_t += el
+    return {"value": tot_pts / tot_t / 1e6, "unit": "Mpoints/s", "cores": threads, "kind": kind,
+            "sample": f"{sample} points per shape (first points of the same seeded workload), "
+                      f"each op repeated for ~{per:.2f} s, {threads} threads"}
+
+
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from vecgeom_b200 import workloads as W
+    shapes, n, _ = workload_shapes(args.workload)
+    if args.n:
+        n = args.n
+    for _ in range(args.warmup):
+        pass
+    times = []
+    cb = None
+    for _ in range(max(1, args.steps)):
+        cb = cpu_rate(shapes, n, W.SEED_BASE + 2, budget_s=max(2.0, 60.0 / max(1, args.steps)))
+        times.append(cb["value"])
+    v = float(np.median(times))
+    line = {"impl": "reference", "metric": "Mpoints/s per shape op (fp64)", "value": v,
+            "unit": "Mpoints/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": workload_desc(args.workload, n, "fp64"),
+            "cpu_baseline": {"value": v, "unit": "Mpoints/s", "cores": cb["cores"],
+                             "kind": cb["kind"], "sample": cb["sample"]},
+            "e2e": {"value": v, "unit": "Mpoints/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# the GPU arm
+# ---------------------------------------------------------------------------
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference_arm(args)
+        return
+    import torch
+    import torch.distributed as dist
+
+    import vecgeom_b200 as V
+    from vecgeom_b200 import workloads as W
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    L = V.lib()
+    prec = V.PREC_FP64 if args.precision == "fp64" else V.PREC_FP32_REFINE
+
+    shapes, n, mix = workload_shapes(args.workload)
+    if args.n:
+        n = args.n
+    stream = torch.cuda.current_stream()
+
+    # --- geometry + inputs resident in HBM --------------------------------
+    g = V.Geometry()
+    placed = {}
+    for name, spec in shapes.items():
+        lv = g.LogicalVolume(name, W.build_unplaced(g, spec))
+        placed[name] = lv.Place(g.Transformation3D())
+    g.CloseGeometry()
+
+    def dev(a):
+        return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+    tasks = []   # (shape, opname, n, callable on device, callable on host)
+    h2d_bytes = d2h_bytes = 0
+    for si, (name, spec) in enumerate(shapes.items()):
+        wl = W.make_workload(spec, n, W.SEED_BASE + 1000 * rank + si, mix=mix)
+        pv = placed[name]
+        P = V.SOA3D(dev(wl.x), dev(wl.y), dev(wl.z))
+        D = V.SOA3D(dev(wl.dx), dev(wl.dy), dev(wl.dz))
+        S = dev(wl.step)
+        c = torch.empty(n, dtype=torch.uint8, device="cuda")
+        pv.Contains(P, c, precision=prec)
+        torch.cuda.synchronize()
+        sel = c.bool()
+        PS = V.SOA3D(P.x[sel].contiguous(), P.y[sel].contiguous(), P.z[sel].contiguous())
+        DS = V.SOA3D(D.x[sel].contiguous(), D.y[sel].contiguous(), D.z[sel].contiguous())
+        SS = S[sel].contiguous()
+        ns = int(sel.sum().item())
+        # pinned host copies for the end-to-end leg
+        pin = lambda t: t.cpu().pin_memory()  # noqa: E731
+        HP = V.SOA3D(pin(P.x), pin(P.y), pin(P.z))
+        HD = V.SOA3D(pin(D.x), pin(D.y), pin(D.z))
+        HS = pin(S)
+        HPS = V.SOA3D(pin(PS.x), pin(PS.y), pin(PS.z))
+        HDS = V.SOA3D(pin(DS.x), pin(DS.y), pin(DS.z))
+        HSS = pin(SS)
+        for opname in OPS:
+            local_op = opname in LOCAL_OPS
+            m = ns if local_op else n
+            dt = {"contains": torch.uint8, "inside": torch.int32}.get(opname, torch.float64)
+            out_d = torch.empty(m, dtype=dt, device="cuda")
+            out_h = torch.empty(m, dtype=dt).pin_memory()
+            pts_d, dirs_d, st_d = (PS, DS, SS) if local_op else (P, D, S)
+            pts_h, dirs_h, st_h = (HPS, HDS, HSS) if local_op else (HP, HD, HS)
+            meth = {"contains": "Contains", "inside": "Inside", "safety_to_in": "SafetyToIn",
+                    "safety_to_out": "SafetyToOut", "distance_to_in": "DistanceToIn",
+                    "distance_to_out": "DistanceToOut"}[opname]
+            fn = getattr(pv, meth)
+            if opname.startswith("distance"):
+                run_d = (lambda fn=fn, a=pts_d, b=dirs_d, s=st_d, o=out_d:
+                         fn(a, b, s, o, precision=prec))
+                run_h = (lambda fn=fn, a=pts_h, b=dirs_h, s=st_h, o=out_h:
+                         fn(a, b, s, o, precision=prec))
+                h2d_bytes += m * 56
+            else:
+                run_d = lambda fn=fn, a=pts_d, o=out_d: fn(a, o, precision=prec)  # noqa: E731
+                run_h = lambda fn=fn, a=pts_h, o=out_h: fn(a, o, precision=prec)  # noqa: E731
+                h2d_bytes += m * 24
+            d2h_bytes += m * out_d.element_size()
+            tasks.append((name, opname, m, run_d, run_h))
+
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")   # > 126 MB L2
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in tasks]
+
+    def one_step(timed: bool):
+        for k, t in enumerate(tasks):
+            flush.zero_()
+            if timed:
+                ev[k][0].record(stream)
+            t[3]()
+            if timed:
+                ev[k][1].record(stream)
+
+    for _ in range(max(3, args.warmup)):
+        one_step(False)
+    torch.cuda.synchronize()
+
+    per_task_ms = np.zeros(len(tasks))
+    clocks = ClockSampler(local)
+    clocks.start()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    L.vgb_launch_count_reset()
+    for _ in range(args.steps):
+        one_step(True)
+        torch.cuda.synchronize()
+        per_task_ms += np.array([a.elapsed_time(b) for a, b in ev])
+    launches = int(L.vgb_launch_count())
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+
+    step_ms = float(per_task_ms.sum()) / args.steps
+    if world > 1:
+        t = torch.tensor([step_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        step_ms = float(t.item())
+    pts_per_step = sum(t[2] for t in tasks)
+    value = world * pts_per_step / (step_ms * 1e-3) / 1e6
+
+    # roofline of the dominant kernel (largest share of the step)
+    k = int(np.argmax(per_task_ms))
+    name, opname, m, _, _ = tasks[k]
+    avg_s = per_task_ms[k] / args.steps * 1e-3
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        pass
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    achieved = BYTES[opname] * m / avg_s / 1e9
+    traffic = None
+    try:
+        prof = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))
+        traffic = prof.get(f"{name}:{opname}:{args.precision}")
+    except (OSError, ValueError):
+        pass
+    roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
+            "frac": round(achieved / hbm_peak, 4), "traffic": traffic,
+            "kernel": f"{name} {opname}", "bytes_per_point": BYTES[opname],
+            "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"}
+
+    # end-to-end through the public API with pinned host buffers
+    e2e = None
+    if not args.no_e2e:
+        for _ in range(2):
+            for t in tasks:
+                t[4]()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e2e_steps = max(1, min(args.steps, 3))
+        for _ in range(e2e_steps):
+            for t in tasks:
+                t[4]()
+        e2e_s = (time.perf_counter() - t0) / e2e_steps
+        if world > 1:
+            tt = torch.tensor([e2e_s], device="cuda")
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            e2e_s = float(tt.item())
+        e2e = {"value": round(world * pts_per_step / e2e_s / 1e6, 2), "unit": "Mpoints/s",
+               "h2d_bytes_per_step": int(h2d_bytes), "d2h_bytes_per_step": int(d2h_bytes)}
+
+    per_op = {f"{t[0]}:{t[1]}": round(t[2] / (per_task_ms[i] / args.steps * 1e-3) / 1e6, 1)
+              for i, t in enumerate(tasks)}
+    line = {"metric": "Mpoints/s per shape op" + (" (fp64)" if args.precision == "fp64"
+                                                  else " (fp32+refine)"),
+            "value": round(value, 2), "unit": "Mpoints/s", "n_gpus": world,
+            "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": round(step_ms, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if args.precision == "fp64" else "f32+f64",
+            "data": "synthetic (seeded)",
+            "config": dict(workload_desc(args.workload, n, args.precision),
+                           l2="flushed (256 MB write) before every op, outside the events"),
+            "per_op_mpoints_s": per_op, "roofline": roof, "e2e": e2e,
+            "gpu_launches": launches, "clocks": clk}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_rate(shapes, n, W.SEED_BASE + 2)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

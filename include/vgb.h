@@ -1,0 +1,218 @@
+/* vgb.h -- C ABI of the B200-native VecGeom hot path (libvgb.so).
+ *
+ * The library replaces, for one NVIDIA B200 (sm_100a), the data-parallel hot
+ * path of VecGeom: the VPlacedVolume SOA3D batch virtuals (Inside/Contains,
+ * DistanceToIn/DistanceToOut, SafetyToIn/SafetyToOut and their Minimize
+ * forms), the CudaManager geometry upload, and the SimpleNavigator step
+ * (FindNextBoundaryAndStep, GetSafety) over a device NavStatePool.
+ *
+ * Conventions kept from the reference (base/Global.h:196-207, :267-302):
+ *   - Precision is double; Inside_t is int with kInside=0, kSurface=1, kOutside=2.
+ *   - kTolerance = 1e-9 (mm); kInfinity = +inf.
+ *   - Contains/Inside/DistanceToIn/SafetyToIn take mother-frame points and apply
+ *     the volume's placement; DistanceToOut/SafetyToOut take local points
+ *     (volumes/PlacedVolume.h:145-250).
+ *   - DistanceToIn returns -1 for a point inside a box and kInfinity on a miss.
+ * Every pointer argument may be device memory (the kernels read it in place) or
+ * host memory (the call stages it through device buffers on the given stream).
+ * Buffers belong to the caller.  Nothing aborts: every entry point returns a
+ * vgb_status and vgb_last_error() describes the last failure on this thread.
+ */
+#ifndef VGB_H
+#define VGB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes; the reference instead asserts and aborts
+ * (source/backend/cuda/Interface.cpp:20-39). */
+typedef enum {
+  VGB_OK = 0,
+  VGB_EINVAL = 1,    /* bad argument, unknown id, geometry not closed, ... */
+  VGB_ENOMEM = 2,    /* device or host allocation failed */
+  VGB_ECUDA = 3,     /* a CUDA runtime call failed */
+  VGB_ELOOPCAP = 4,  /* a device loop hit its iteration cap (e.g. navigation steps) */
+  VGB_ETIMEDOUT = 5, /* a bounded host wait ran out */
+  VGB_ENOTSUP = 6,   /* operation not supported for this shape / mode */
+  VGB_ENOSPC = 7     /* a fixed-size buffer is too small for the request */
+} vgb_status;
+
+/* base/Global.h:196-207 EnumInside */
+enum { VGB_kInside = 0, VGB_kSurface = 1, VGB_kOutside = 2 };
+
+/* Arithmetic of the batch kernels.  FP64 reproduces the reference Scalar
+ * backend operation by operation; FP32_REFINE does the bulk in float and
+ * re-resolves in double where stability needs it. */
+typedef enum { VGB_PREC_FP64 = 0, VGB_PREC_FP32_REFINE = 1 } vgb_precision;
+
+/* Operations of the VPlacedVolume SOA3D interface (volumes/PlacedVolume.h). */
+typedef enum {
+  VGB_OP_CONTAINS = 0,                /* :147  Contains(SOA3D, bool*)                  */
+  VGB_OP_INSIDE = 1,                  /* :165  Inside(SOA3D, Inside_t*)                */
+  VGB_OP_DISTANCE_TO_IN = 2,          /* :176  DistanceToIn(SOA3D, SOA3D, step*, out*) */
+  VGB_OP_DISTANCE_TO_OUT = 3,         /* :212  DistanceToOut(SOA3D, SOA3D, step*, out*)*/
+  VGB_OP_SAFETY_TO_IN = 4,            /* :231  SafetyToIn(SOA3D, out*)                 */
+  VGB_OP_SAFETY_TO_OUT = 5,           /* :243  SafetyToOut(SOA3D, out*)                */
+  VGB_OP_DISTANCE_TO_IN_MINIMIZE = 6, /* :181  DistanceToInMinimize(...)               */
+  VGB_OP_SAFETY_TO_IN_MINIMIZE = 7,   /* :237  SafetyToInMinimize(SOA3D, inout*)       */
+  VGB_OP_SAFETY_TO_OUT_MINIMIZE = 8,  /* :249  SafetyToOutMinimize(SOA3D, inout*)      */
+  VGB_OP_DISTANCE_TO_OUT_NODE = 9,    /* :217  DistanceToOut(..., int* nextnodeindex)  */
+  VGB_OP_PLACED_DISTANCE_TO_OUT = 10, /* :207  PlacedDistanceToOut (applies placement) */
+  VGB_OP_COUNT = 11
+} vgb_op;
+
+/* Shape types (volumes/Unplaced*.h). */
+typedef enum {
+  VGB_SHAPE_BOX = 1,
+  VGB_SHAPE_TUBE = 2,
+  VGB_SHAPE_CONE = 3,
+  VGB_SHAPE_SPHERE = 4,
+  VGB_SHAPE_TORUS = 5,
+  VGB_SHAPE_POLYCONE = 6,
+  VGB_SHAPE_POLYHEDRON = 7,
+  VGB_SHAPE_BOOLEAN = 8,
+  VGB_SHAPE_TRD = 9
+} vgb_shape_type;
+
+/* volumes/UnplacedBooleanVolume.h:10-14 */
+enum { VGB_BOOL_UNION = 0, VGB_BOOL_INTERSECTION = 1, VGB_BOOL_SUBTRACTION = 2 };
+
+typedef struct vgb_geometry vgb_geometry;
+
+/* ---------------------------------------------------------------------------
+ * Library
+ * ------------------------------------------------------------------------- */
+const char *vgb_last_error(void);
+const char *vgb_version(void);
+/* Number of kernels this thread launched since the last reset (the count a
+ * benchmark reports as its launches). */
+int64_t vgb_launch_count(void);
+void vgb_launch_count_reset(void);
+
+/* ---------------------------------------------------------------------------
+ * Geometry construction and upload.
+ * Replaces the host object graph (Unplaced*, LogicalVolume, Transformation3D,
+ * GeoManager) and its CudaManager upload (source/CudaManager.cpp:39-322): the
+ * geometry is recorded on the host, then vgb_geometry_close() flattens it into
+ * device tables with one copy per table (no per-object constructor kernels).
+ * Ids are dense, non-negative ints returned in *id.
+ * ------------------------------------------------------------------------- */
+vgb_status vgb_geometry_create(vgb_geometry **g);
+vgb_status vgb_geometry_destroy(vgb_geometry *g);
+
+/* Unplaced shapes; arguments as the reference constructors take them.       */
+/* volumes/UnplacedBox.h:30 */
+vgb_status vgb_unplaced_box(vgb_geometry *g, double dx, double dy, double dz, int32_t *id);
+/* volumes/UnplacedTube.h:65 (angles in radians) */
+vgb_status vgb_unplaced_tube(vgb_geometry *g, double rmin, double rmax, double dz, double sphi,
+                             double dphi, int32_t *id);
+/* volumes/UnplacedCone.h:108 (angles in radians) */
+vgb_status vgb_unplaced_cone(vgb_geometry *g, double rmin1, double rmax1, double rmin2,
+                             double rmax2, double dz, double sphi, double dphi, int32_t *id);
+/* volumes/UnplacedSphere.h:219 (angles in radians) */
+vgb_status vgb_unplaced_sphere(vgb_geometry *g, double rmin, double rmax, double sphi,
+                               double dphi, double stheta, double dtheta, int32_t *id);
+/* volumes/UnplacedTorus.h:61 (angles in radians) */
+vgb_status vgb_unplaced_torus(vgb_geometry *g, double rmin, double rmax, double rtor, double sphi,
+                              double dphi, int32_t *id);
+/* volumes/UnplacedPolycone.h:82 (angles in radians) */
+vgb_status vgb_unplaced_polycone(vgb_geometry *g, double sphi, double dphi, int32_t nz,
+                                 const double *rmin, const double *rmax, const double *z,
+                                 int32_t *id);
+/* volumes/UnplacedPolyhedron.h:169 (phi in degrees, as the reference) */
+vgb_status vgb_unplaced_polyhedron(vgb_geometry *g, double phi_start_deg, double phi_delta_deg,
+                                   int32_t sides, int32_t nz, const double *z,
+                                   const double *rmin, const double *rmax, int32_t *id);
+/* volumes/UnplacedTrd.h:73 */
+vgb_status vgb_unplaced_trd(vgb_geometry *g, double dx1, double dx2, double dy1, double dy2,
+                            double dz, int32_t *id);
+/* volumes/UnplacedBooleanVolume.h:46 (left/right are placed-volume ids) */
+vgb_status vgb_unplaced_boolean(vgb_geometry *g, int32_t op, int32_t left_placed,
+                                int32_t right_placed, int32_t *id);
+
+/* Transformation3D(tx,ty,tz, phi,theta,psi) with Euler angles in degrees
+ * (source/Transformation3D.cpp:36-44, :93-114). */
+vgb_status vgb_transformation(vgb_geometry *g, double tx, double ty, double tz, double phi,
+                              double theta, double psi, int32_t *id);
+/* Transformation3D(tx,ty,tz, r0..r8) (source/Transformation3D.cpp:46-55). */
+vgb_status vgb_transformation_matrix(vgb_geometry *g, double tx, double ty, double tz,
+                                     const double *r9, int32_t *id);
+
+/* LogicalVolume(label, unplaced) (volumes/LogicalVolume.h:66). */
+vgb_status vgb_logical_volume(vgb_geometry *g, const char *label, int32_t unplaced,
+                              int32_t *id);
+/* LogicalVolume::Place(transformation) (source/LogicalVolume.cpp:60-64). */
+vgb_status vgb_place(vgb_geometry *g, int32_t logical, int32_t transformation, int32_t *placed);
+/* LogicalVolume::PlaceDaughter(volume, transformation) (source/LogicalVolume.cpp:80-97);
+ * daughter order is insertion order. */
+vgb_status vgb_place_daughter(vgb_geometry *g, int32_t mother_logical, int32_t daughter_logical,
+                              int32_t transformation, int32_t *placed);
+/* GeoManager::SetWorld (management/GeoManager.h:164). */
+vgb_status vgb_set_world(vgb_geometry *g, int32_t placed);
+/* GeoManager::CloseGeometry + CudaManager::LoadGeometry/Synchronize: computes
+ * the maximum depth and uploads all tables to the current device. */
+vgb_status vgb_geometry_close(vgb_geometry *g);
+/* GeoManager::getMaxDepth (management/GeoManager.h:191). */
+vgb_status vgb_geometry_max_depth(const vgb_geometry *g, int32_t *depth);
+/* Bytes the geometry occupies on the device. */
+vgb_status vgb_geometry_device_bytes(const vgb_geometry *g, int64_t *bytes);
+
+/* ---------------------------------------------------------------------------
+ * Batched shape operations (the VPlacedVolume SOA3D virtuals).
+ *
+ * One call runs one operation over n points for one placed volume.
+ *   x,y,z        positions (SOA3D x(), y(), z())
+ *   dx,dy,dz     directions (unit vectors), DistanceTo* only
+ *   step_max     per-point step limit, DistanceTo* only
+ *   out          uint8 (Contains), int32 (Inside) or double; for the Minimize
+ *                forms it is the in/out distance or safety array
+ *   aux          int32: DistanceToInMinimize's next-daughter id list (in/out)
+ *                and DistanceToOut's node index (-1 leaves, -2 stays)
+ *   daughter     the daughter index written by DistanceToInMinimize
+ *   stream       cudaStream_t (NULL = legacy default stream)
+ * The call is asynchronous for device pointers; with host pointers it returns
+ * once the results are back in host memory.
+ * ------------------------------------------------------------------------- */
+vgb_status vgb_batch(const vgb_geometry *g, int32_t placed, int32_t op, int64_t n,
+                     const double *x, const double *y, const double *z, const double *dx,
+                     const double *dy, const double *dz, const double *step_max, void *out,
+                     int32_t *aux, int32_t daughter, int32_t precision, void *stream);
+
+/* Per-operation forms with the reference's argument order. */
+vgb_status vgb_Contains(const vgb_geometry *g, int32_t placed, int64_t n, const double *x,
+                        const double *y, const double *z, uint8_t *out, void *stream);
+vgb_status vgb_Inside(const vgb_geometry *g, int32_t placed, int64_t n, const double *x,
+                      const double *y, const double *z, int32_t *out, void *stream);
+vgb_status vgb_DistanceToIn(const vgb_geometry *g, int32_t placed, int64_t n, const double *x,
+                            const double *y, const double *z, const double *dx,
+                            const double *dy, const double *dz, const double *step_max,
+                            double *out, void *stream);
+vgb_status vgb_DistanceToOut(const vgb_geometry *g, int32_t placed, int64_t n, const double *x,
+                             const double *y, const double *z, const double *dx,
+                             const double *dy, const double *dz, const double *step_max,
+                             double *out, void *stream);
+vgb_status vgb_SafetyToIn(const vgb_geometry *g, int32_t placed, int64_t n, const double *x,
+                          const double *y, const double *z, double *out, void *stream);
+vgb_status vgb_SafetyToOut(const vgb_geometry *g, int32_t placed, int64_t n, const double *x,
+                           const double *y, const double *z, double *out, void *stream);
+
+/* Several operations over the same points in one pass (one read of x,y,z and
+ * the directions).  ops is a bit mask of (1 << vgb_op) over CONTAINS, INSIDE,
+ * DISTANCE_TO_IN, DISTANCE_TO_OUT, SAFETY_TO_IN, SAFETY_TO_OUT; outs[op] is the
+ * output of each requested op.  With VGB_FUSED_DTO_INSIDE_ONLY set in flags,
+ * DistanceToOut is evaluated only for points Contains() accepts; the others
+ * get kInfinity. */
+enum { VGB_FUSED_DTO_INSIDE_ONLY = 1 };
+vgb_status vgb_batch_fused(const vgb_geometry *g, int32_t placed, uint32_t ops, int64_t n,
+                           const double *x, const double *y, const double *z, const double *dx,
+                           const double *dy, const double *dz, const double *step_max,
+                           void *const *outs, uint32_t flags, int32_t precision, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* VGB_H */

@@ -1,0 +1,210 @@
+"""CPU checkers for libvgb -- test infrastructure, NOT product code.
+
+Two checkers, loaded with ctypes:
+  * ``Oracle`` -- liboracle.so, the plain-C restatement of the reference
+    algorithms in vgb_oracle.c (always built; travels with the repository).
+  * ``RefLib`` -- _ref/libvgref.so, the reference VecGeom Scalar backend itself,
+    compiled from the reference's own sources by oracle/Makefile.  Present
+    wherever it was built; tests that need it skip when it is absent.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this
+package.  The product (vecgeom_b200/) never imports it.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libvgref.so")
+
+# or_op / or_shape (vgb_oracle.h)
+CONTAINS, INSIDE, DISTANCE_TO_IN, DISTANCE_TO_OUT, SAFETY_TO_IN, SAFETY_TO_OUT = range(6)
+_vp, _d, _i, _i64 = ctypes.c_void_p, ctypes.c_double, ctypes.c_int, ctypes.c_int64
+
+
+def build(with_ref: bool = True) -> None:
+    """Compile the C restatement (and the reference shim when the tree is here)."""
+    targets = ["oracle"] + (["ref"] if with_ref else [])
+    subprocess.run(["make", "-C", HERE, "-j8"] + targets, check=True,
+                   stdout=subprocess.DEVNULL)
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(_vp)
+
+
+def out_array(op: int, n: int) -> np.ndarray:
+    if op == CONTAINS:
+        return np.zeros(n, np.uint8)
+    if op == INSIDE:
+        return np.zeros(n, np.int32)
+    return np.zeros(n, np.float64)
+
+
+class Xform(ctypes.Structure):
+    _fields_ = [("t", ctypes.c_double * 3), ("r", ctypes.c_double * 9),
+                ("trans_code", ctypes.c_int), ("rot_code", ctypes.c_int)]
+
+
+class Oracle:
+    """The C restatement (vgb_oracle.c)."""
+
+    def __init__(self):
+        if not os.path.exists(ORACLE_SO):
+            build(with_ref=False)
+        L = ctypes.CDLL(ORACLE_SO)
+        L.or_box.restype = _vp
+        L.or_box.argtypes = [_d, _d, _d]
+        L.or_shape_free.argtypes = [_vp]
+        L.or_xform_euler.argtypes = [ctypes.POINTER(Xform)] + [_d] * 6
+        L.or_xform_matrix.argtypes = [ctypes.POINTER(Xform), _d, _d, _d, _vp]
+        L.or_xform_set_generic.argtypes = [ctypes.POINTER(Xform)]
+        L.or_batch.restype = _i
+        L.or_batch.argtypes = [_vp, ctypes.POINTER(Xform), _i, _i64] + [_vp] * 8
+        self.L = L
+
+    def shape(self, kind: str, *params):
+        fn = getattr(self.L, "or_" + kind)
+        return fn(*params)
+
+    def xform(self, tx=0., ty=0., tz=0., phi=0., theta=0., psi=0., generic=False) -> Xform:
+        x = Xform()
+        self.L.or_xform_euler(ctypes.byref(x), tx, ty, tz, phi, theta, psi)
+        if generic:
+            self.L.or_xform_set_generic(ctypes.byref(x))
+        return x
+
+    def batch(self, shape, xf: Xform, op: int, pts, dirs=None, step=None) -> np.ndarray:
+        x, y, z = (np.ascontiguousarray(a, np.float64) for a in pts)
+        n = len(x)
+        if dirs is not None:
+            dx, dy, dz = (np.ascontiguousarray(a, np.float64) for a in dirs)
+        else:
+            dx = dy = dz = None
+        out = out_array(op, n)
+        rc = self.L.or_batch(shape, ctypes.byref(xf), op, n, _p(x), _p(y), _p(z), _p(dx),
+                             _p(dy), _p(dz), _p(step), _p(out))
+        if rc != 0:
+            raise RuntimeError(f"or_batch failed for op {op}")
+        return out
+
+
+class RefLib:
+    """The reference VecGeom Scalar backend (oracle/_ref/libvgref.so)."""
+
+    @staticmethod
+    def available() -> bool:
+        return os.path.exists(REF_SO)
+
+    def __init__(self):
+        L = ctypes.CDLL(REF_SO)
+        for name, argn in (("vgref_box", 3), ("vgref_tube", 5), ("vgref_cone", 7),
+                           ("vgref_sphere", 6), ("vgref_torus", 5), ("vgref_trd", 5)):
+            f = getattr(L, name)
+            f.restype = _vp
+            f.argtypes = [_d] * argn
+        L.vgref_polycone.restype = _vp
+        L.vgref_polycone.argtypes = [_d, _d, _i, _vp, _vp, _vp]
+        L.vgref_polyhedron.restype = _vp
+        L.vgref_polyhedron.argtypes = [_d, _d, _i, _i, _vp, _vp, _vp]
+        L.vgref_boolean.restype = _vp
+        L.vgref_boolean.argtypes = [_i, _vp, _vp]
+        L.vgref_transform_euler.restype = _vp
+        L.vgref_transform_euler.argtypes = [_d] * 6
+        L.vgref_transform_matrix.restype = _vp
+        L.vgref_transform_matrix.argtypes = [_d, _d, _d, _vp]
+        L.vgref_transform_get.argtypes = [_vp, _vp, _vp]
+        L.vgref_logical.restype = _vp
+        L.vgref_logical.argtypes = [ctypes.c_char_p, _vp]
+        L.vgref_place.restype = _vp
+        L.vgref_place.argtypes = [_vp, _vp]
+        L.vgref_place_daughter.restype = _vp
+        L.vgref_place_daughter.argtypes = [_vp, _vp, _vp]
+        L.vgref_batch.restype = _i
+        L.vgref_batch.argtypes = [_vp, _i, _i64] + [_vp] * 9 + [_i, _i]
+        L.vgref_set_world.argtypes = [_vp]
+        L.vgref_close_geometry.restype = _i
+        L.vgref_placed_id.restype = _i
+        L.vgref_placed_id.argtypes = [_vp]
+        L.vgref_nav_trace.restype = _i
+        L.vgref_nav_trace.argtypes = [_i64] + [_vp] * 6 + [_d, _i] + [_vp] * 4 + [_i]
+        L.vgref_locate.restype = _i
+        L.vgref_locate.argtypes = [_d, _d, _d, _vp]
+        self.L = L
+        self._keep = []
+
+    def placed(self, unplaced, tx=0., ty=0., tz=0., phi=0., theta=0., psi=0., label="v"):
+        t = self.L.vgref_transform_euler(tx, ty, tz, phi, theta, psi)
+        lv = self.L.vgref_logical(label.encode(), unplaced)
+        return self.L.vgref_place(lv, t)
+
+    def batch(self, placed, op: int, pts, dirs=None, step=None, nthreads: int = 1,
+              out=None, aux=None, daughter: int = 0) -> np.ndarray:
+        x, y, z = (np.ascontiguousarray(a, np.float64) for a in pts)
+        n = len(x)
+        if dirs is not None:
+            dx, dy, dz = (np.ascontiguousarray(a, np.float64) for a in dirs)
+        else:
+            dx = dy = dz = None
+        if out is None:
+            out = np.zeros(n, np.bool_) if op == CONTAINS else out_array(op, n)
+        self.L.vgref_batch(placed, op, n, _p(x), _p(y), _p(z), _p(dx), _p(dy), _p(dz),
+                           _p(step), _p(out), _p(aux), daughter, nthreads)
+        return out.view(np.uint8) if op == CONTAINS else out
+
+
+def ref_unplaced(ref: RefLib, spec):
+    """Create spec's unplaced shape with the reference's own constructors."""
+    import math
+    L = ref.L
+    p = spec.params
+    k = spec.kind
+    if k == "box":
+        return L.vgref_box(p["dx"], p["dy"], p["dz"])
+    if k == "tube":
+        return L.vgref_tube(p["rmin"], p["rmax"], p["dz"], p["sphi"], p["dphi"])
+    if k == "cone":
+        return L.vgref_cone(p["rmin1"], p["rmax1"], p["rmin2"], p["rmax2"], p["dz"], p["sphi"],
+                            p["dphi"])
+    if k == "sphere":
+        return L.vgref_sphere(p["rmin"], p["rmax"], p["sphi"], p["dphi"], p["stheta"],
+                              p["dtheta"])
+    if k == "torus":
+        return L.vgref_torus(p["rmin"], p["rmax"], p["rtor"], p["sphi"], p["dphi"])
+    if k == "trd":
+        return L.vgref_trd(p["dx1"], p["dx2"], p["dy1"], p["dy2"], p["dz"])
+    if k in ("polycone", "polyhedron"):
+        z, rmin, rmax = (np.ascontiguousarray(p[a], np.float64) for a in ("z", "rmin", "rmax"))
+        ref._keep += [z, rmin, rmax]
+        if k == "polycone":
+            return L.vgref_polycone(p["sphi"], p["dphi"], len(z), z.ctypes.data,
+                                    rmin.ctypes.data, rmax.ctypes.data)
+        return L.vgref_polyhedron(p["phi_start_deg"], p["phi_delta_deg"], p["sides"], len(z),
+                                  z.ctypes.data, rmin.ctypes.data, rmax.ctypes.data)
+    if k == "boolsub":
+        bx, by, bz = p["box_half"]
+        left = ref.placed(L.vgref_box(bx, by, bz), label="sub_box")
+        right = ref.placed(L.vgref_tube(0., p["tube_rmax"], p["tube_dz"], 0., 2 * math.pi),
+                           label="sub_tube")
+        return L.vgref_boolean(2, left, right)
+    raise ValueError(k)
+
+
+def oracle_unplaced(orc: Oracle, spec):
+    """Create spec's shape in the C restatement."""
+    p = spec.params
+    k = spec.kind
+    if k == "box":
+        return orc.shape("box", p["dx"], p["dy"], p["dz"])
+    raise NotImplementedError(k)
+
+
+def oracle_generic_xform(spec) -> bool:
+    """Shapes whose placed volumes always use the generic transform
+    (source/UnplacedPolyhedron.cpp:321-333)."""
+    return spec.kind == "polyhedron"

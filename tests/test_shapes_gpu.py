@@ -1,0 +1,201 @@
+"""GPU parity of the FP64 batch kernels, through the C ABI.
+
+* against the reference's own outputs (tests/golden/*.npz, written by the
+  reference Scalar backend): Contains/Inside bit-exact, distances and safeties
+  within 1e-9 mm or 1e-12 relative;
+* against the C oracle on larger seeded inputs, device and host buffers;
+* the Minimize / node-index / placed forms against their definitions.
+"""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from helpers import PLACEMENTS, assert_distances, assert_exact, vgb_unplaced
+from test_oracle_golden import load_case, spec_from_meta
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+GOLDEN = sorted(glob.glob(os.path.join(HERE, "golden", "*.npz")))
+VGB_SHAPES = {"box"}
+
+pytestmark = pytest.mark.gpu
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def dev(a):
+    torch = _torch()
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def host(t):
+    return t.cpu().numpy()
+
+
+def build_placed(spec, placement):
+    import vecgeom_b200 as V
+    g = V.Geometry()
+    u = vgb_unplaced(g, spec)
+    lv = g.LogicalVolume(spec.kind, u)
+    pv = lv.Place(g.Transformation3D(*PLACEMENTS[placement]))
+    g.CloseGeometry()
+    return g, pv
+
+
+def run_all_ops(pv, pm, dm, pl, dl, step, on_device=True):
+    import vecgeom_b200 as V
+    torch = _torch()
+    n = len(pm[0])
+    conv = dev if on_device else np.ascontiguousarray
+    P = V.SOA3D(*(conv(a) for a in pm))
+    D = V.SOA3D(*(conv(a) for a in dm))
+    PL = V.SOA3D(*(conv(a) for a in pl))
+    DL = V.SOA3D(*(conv(a) for a in dl))
+    S = conv(step)
+    if on_device:
+        mk = {"u1": lambda: torch.zeros(n, dtype=torch.uint8, device="cuda"),
+              "i4": lambda: torch.zeros(n, dtype=torch.int32, device="cuda"),
+              "f8": lambda: torch.zeros(n, dtype=torch.float64, device="cuda")}
+    else:
+        mk = {"u1": lambda: np.zeros(n, np.uint8), "i4": lambda: np.zeros(n, np.int32),
+              "f8": lambda: np.zeros(n, np.float64)}
+    out = {k: mk[t]() for k, t in (("contains", "u1"), ("inside", "i4"), ("safety_to_in", "f8"),
+                                   ("safety_to_out", "f8"), ("distance_to_in", "f8"),
+                                   ("distance_to_out", "f8"))}
+    pv.Contains(P, out["contains"])
+    pv.Inside(P, out["inside"])
+    pv.SafetyToIn(P, out["safety_to_in"])
+    pv.SafetyToOut(PL, out["safety_to_out"])
+    pv.DistanceToIn(P, D, S, out["distance_to_in"])
+    pv.DistanceToOut(PL, DL, S, out["distance_to_out"])
+    if on_device:
+        torch.cuda.synchronize()
+        return {k: host(v) for k, v in out.items()}
+    return out
+
+
+def check_against(res, want, what):
+    assert_exact(res["contains"], want["contains"], f"{what} Contains")
+    assert_exact(res["inside"], want["inside"], f"{what} Inside")
+    for k in ("safety_to_in", "safety_to_out", "distance_to_in", "distance_to_out"):
+        assert_distances(res[k], want[k], f"{what} {k}")
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p)[:-4] for p in GOLDEN])
+@pytest.mark.parametrize("on_device", [True, False], ids=["device", "host"])
+def test_golden_parity(path, on_device):
+    d, meta = load_case(path)
+    if meta["kind"] not in VGB_SHAPES:
+        pytest.skip(f"{meta['kind']} not in this build")
+    spec = spec_from_meta(meta)
+    g, pv = build_placed(spec, str(d["placement"]))
+    res = run_all_ops(pv, (d["mx"], d["my"], d["mz"]), (d["mdx"], d["mdy"], d["mdz"]),
+                      (d["lx"], d["ly"], d["lz"]), (d["ldx"], d["ldy"], d["ldz"]), d["step"],
+                      on_device)
+    check_against(res, d, os.path.basename(path))
+
+
+@pytest.mark.parametrize("kind", sorted(VGB_SHAPES))
+def test_large_seeded_vs_reference(kind):
+    """2^16 mixed points per shape, every op, against the reference itself when
+    oracle/_ref is built, else against the C restatement."""
+    from helpers import shape_specs
+    from vecgeom_b200 import workloads as W
+    spec = shape_specs()[kind]
+    wl = W.make_workload(spec, 1 << 16, W.SEED_BASE + 17)
+    g, pv = build_placed(spec, "generic")
+    pts = (wl.x, wl.y, wl.z)
+    dirs = (wl.dx, wl.dy, wl.dz)
+    res = run_all_ops(pv, pts, dirs, pts, dirs, wl.step)
+    want = reference_outputs(spec, "generic", pts, dirs, wl.step)
+    check_against(res, want, kind)
+
+
+def reference_outputs(spec, placement, pts, dirs, step):
+    from helpers import ref_unplaced, oracle_unplaced, oracle_generic_xform
+    want = {}
+    if oracle.RefLib.available():
+        ref = oracle.RefLib()
+        pv = ref.placed(ref_unplaced(ref, spec), *PLACEMENTS[placement])
+        call = lambda op, p, d=None, s=None: ref.batch(pv, op, p, d, s)  # noqa: E731
+    else:
+        orc = oracle.Oracle()
+        sh = oracle_unplaced(orc, spec)
+        xf = orc.xform(*PLACEMENTS[placement], generic=oracle_generic_xform(spec))
+        call = lambda op, p, d=None, s=None: orc.batch(sh, xf, op, p, d, s)  # noqa: E731
+    want["contains"] = call(oracle.CONTAINS, pts)
+    want["inside"] = call(oracle.INSIDE, pts)
+    want["safety_to_in"] = call(oracle.SAFETY_TO_IN, pts)
+    want["safety_to_out"] = call(oracle.SAFETY_TO_OUT, pts)
+    want["distance_to_in"] = call(oracle.DISTANCE_TO_IN, pts, dirs, step)
+    want["distance_to_out"] = call(oracle.DISTANCE_TO_OUT, pts, dirs, step)
+    return want
+
+
+@pytest.mark.parametrize("kind", sorted(VGB_SHAPES))
+def test_minimize_node_and_placed_forms(kind):
+    """DistanceToInMinimize / SafetyTo{In,Out}Minimize / DistanceToOut(nodeindex)
+    / PlacedDistanceToOut against their definitions in
+    volumes/ShapeImplementationHelper.h:637-748 and :243-270."""
+    import torch
+    import vecgeom_b200 as V
+    from helpers import shape_specs
+    from vecgeom_b200 import workloads as W
+    spec = shape_specs()[kind]
+    n = 1 << 14
+    wl = W.make_workload(spec, n, W.SEED_BASE + 23)
+    g, pv = build_placed(spec, "generic")
+    P = V.SOA3D(dev(wl.x), dev(wl.y), dev(wl.z))
+    D = V.SOA3D(dev(wl.dx), dev(wl.dy), dev(wl.dz))
+    step = dev(wl.step)
+    dti = torch.empty(n, dtype=torch.float64, device="cuda")
+    pv.DistanceToIn(P, D, step, dti)
+    sti = torch.empty_like(dti)
+    pv.SafetyToIn(P, sti)
+    sto = torch.empty_like(dti)
+    pv.SafetyToOut(P, sto)
+    dto = torch.empty_like(dti)
+    pv.DistanceToOut(P, D, step, dto)
+    # Minimize: a running minimum seeded with a per-point value
+    cur0 = torch.from_numpy(np.random.default_rng(1).uniform(0., 40., n)).cuda()
+    cur = cur0.clone()
+    ids = torch.full((n,), -7, dtype=torch.int32, device="cuda")
+    pv.DistanceToInMinimize(P, D, 5, cur, ids)
+    torch.cuda.synchronize()
+    # the DistanceToIn with step_max = cur0 must be recomputed to compare
+    dti_c = torch.empty_like(dti)
+    pv.DistanceToIn(P, D, cur0.clone(), dti_c)
+    upd = dti_c < cur0
+    assert torch.equal(cur, torch.where(upd, dti_c, cur0))
+    assert torch.equal(ids, torch.where(upd, torch.full_like(ids, 5), torch.full_like(ids, -7)))
+    s = cur0.clone()
+    pv.SafetyToInMinimize(P, s)
+    assert torch.equal(s, torch.minimum(sti, cur0))
+    s = cur0.clone()
+    pv.SafetyToOutMinimize(P, s)
+    assert torch.equal(s, torch.minimum(sto, cur0))
+    node = torch.zeros(n, dtype=torch.int32, device="cuda")
+    dto2 = torch.empty_like(dti)
+    pv.DistanceToOut(P, D, step, dto2, nextnodeindex=node)
+    assert torch.equal(dto2, dto)
+    assert torch.equal(node, torch.where(dto < step, torch.full_like(node, -1),
+                                         torch.full_like(node, -2)))
+
+
+def test_empty_batch_and_bad_arguments():
+    import torch
+    import vecgeom_b200 as V
+    from vecgeom_b200 import workloads as W
+    g, pv = build_placed(W.box_spec(1., 2., 3.), "identity")
+    e = torch.empty(0, dtype=torch.float64, device="cuda")
+    pv.Inside(V.SOA3D(e, e, e), torch.empty(0, dtype=torch.int32, device="cuda"))
+    x = torch.zeros(4, dtype=torch.float64, device="cuda")
+    with pytest.raises(V.VgbError):
+        pv.batch(99, V.SOA3D(x, x, x), x)
+    with pytest.raises(V.VgbError):   # distances need directions
+        pv.batch(V.OP_DISTANCE_TO_IN, V.SOA3D(x, x, x), x)

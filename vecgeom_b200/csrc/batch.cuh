@@ -1,0 +1,141 @@
+// batch.cuh -- the SOA batch kernels behind vgb_batch / vgb_batch_fused.
+//
+// One thread per point, grid-stride over the batch.  The shape's parameter
+// record and the placement transform are kernel arguments, so every thread
+// reads them from the constant bank (a broadcast) and the only global traffic
+// is the coalesced SOA stream: x,y,z (+ dx,dy,dz, step_max) in, one result out.
+// Replaces the reference's per-op CUDA kernels (source/benchmarking/Benchmarker.cu:13-79),
+// which make a device virtual call per point, with shape and op resolved at
+// compile time.
+#pragma once
+#include "shapes.cuh"
+
+namespace vgb {
+
+constexpr int kBatchBlock = 256;
+
+struct BatchIO {
+  const double *x, *y, *z;
+  const double *dx, *dy, *dz;
+  const double *step;
+  void *out;
+  int32_t *aux;
+  int64_t n;
+  int32_t daughter;
+  int32_t pad;
+};
+
+// Fused: the outputs of every op of the mask, one read of the inputs.
+struct FusedIO {
+  const double *x, *y, *z;
+  const double *dx, *dy, *dz;
+  const double *step;
+  void *out[6];
+  int64_t n;
+  uint32_t ops;
+  uint32_t flags;
+};
+
+template <class T> VGB_D T ldg(const T *p) { return __ldg(p); }
+
+template <class Ops, class P, int OP>
+__device__ __forceinline__ void batch_point(const P &prm, const DXform &X, const BatchIO &io,
+                                            int64_t i) {
+  using R = double;
+  const V3<R> m = {ldg(io.x + i), ldg(io.y + i), ldg(io.z + i)};
+  if constexpr (OP == VGB_OP_CONTAINS) {
+    static_cast<uint8_t *>(io.out)[i] = (uint8_t)Ops::contains(prm, xf_point(X, m));
+  } else if constexpr (OP == VGB_OP_INSIDE) {
+    static_cast<int32_t *>(io.out)[i] = Ops::inside(prm, xf_point(X, m));
+  } else if constexpr (OP == VGB_OP_SAFETY_TO_IN) {
+    static_cast<double *>(io.out)[i] = Ops::safety_to_in(prm, xf_point(X, m));
+  } else if constexpr (OP == VGB_OP_SAFETY_TO_OUT) {
+    static_cast<double *>(io.out)[i] = Ops::safety_to_out(prm, m);
+  } else if constexpr (OP == VGB_OP_SAFETY_TO_IN_MINIMIZE) {
+    // volumes/ShapeImplementationHelper.h:708-720
+    double *o = static_cast<double *>(io.out);
+    const R r = Ops::safety_to_in(prm, xf_point(X, m));
+    const R cur = o[i];
+    o[i] = (r < cur) ? r : cur;
+  } else if constexpr (OP == VGB_OP_SAFETY_TO_OUT_MINIMIZE) {
+    // volumes/ShapeImplementationHelper.h:734-746
+    double *o = static_cast<double *>(io.out);
+    const R r = Ops::safety_to_out(prm, m);
+    const R cur = o[i];
+    o[i] = (r < cur) ? r : cur;
+  } else {
+    const V3<R> d = {ldg(io.dx + i), ldg(io.dy + i), ldg(io.dz + i)};
+    if constexpr (OP == VGB_OP_DISTANCE_TO_IN) {
+      static_cast<double *>(io.out)[i] =
+          Ops::distance_to_in(prm, xf_point(X, m), xf_dir(X, d), ldg(io.step + i));
+    } else if constexpr (OP == VGB_OP_DISTANCE_TO_OUT) {
+      static_cast<double *>(io.out)[i] = Ops::distance_to_out(prm, m, d, ldg(io.step + i));
+    } else if constexpr (OP == VGB_OP_DISTANCE_TO_OUT_NODE) {
+      // volumes/ShapeImplementationHelper.h:676-692: -1 leaves, -2 stays
+      const R s = ldg(io.step + i);
+      const R r = Ops::distance_to_out(prm, m, d, s);
+      static_cast<double *>(io.out)[i] = r;
+      io.aux[i] = (r < s) ? -1 : -2;
+    } else if constexpr (OP == VGB_OP_PLACED_DISTANCE_TO_OUT) {
+      // volumes/ShapeImplementationHelper.h:243-270
+      static_cast<double *>(io.out)[i] =
+          Ops::distance_to_out(prm, xf_point(X, m), xf_dir(X, d), ldg(io.step + i));
+    } else if constexpr (OP == VGB_OP_DISTANCE_TO_IN_MINIMIZE) {
+      // volumes/ShapeImplementationHelper.h:637-658 (Scalar form): the current
+      // distance is the step limit; update only on a strictly smaller result.
+      double *o = static_cast<double *>(io.out);
+      const R cur = o[i];
+      const R r = Ops::distance_to_in(prm, xf_point(X, m), xf_dir(X, d), cur);
+      if (r < cur) {
+        o[i] = r;
+        io.aux[i] = io.daughter;
+      }
+    }
+  }
+}
+
+template <class Ops, class P, int OP>
+__global__ void __launch_bounds__(kBatchBlock) k_batch(const P prm, const DXform X,
+                                                       const BatchIO io) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < io.n; i += stride)
+    batch_point<Ops, P, OP>(prm, X, io, i);
+}
+
+// All requested ops for one point.  With VGB_FUSED_DTO_INSIDE_ONLY the
+// DistanceToOut result is computed only where Contains() holds.
+template <class Ops, class P>
+__global__ void __launch_bounds__(kBatchBlock) k_fused(const P prm, const DXform X,
+                                                       const FusedIO io) {
+  using R = double;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const uint32_t ops = io.ops;
+  const bool need_dir = ops & ((1u << VGB_OP_DISTANCE_TO_IN) | (1u << VGB_OP_DISTANCE_TO_OUT));
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < io.n; i += stride) {
+    const V3<R> m = {ldg(io.x + i), ldg(io.y + i), ldg(io.z + i)};
+    const V3<R> l = xf_point(X, m);
+    V3<R> d = {0, 0, 0};
+    if (need_dir) d = {ldg(io.dx + i), ldg(io.dy + i), ldg(io.dz + i)};
+    bool c = false;
+    if ((ops & (1u << VGB_OP_CONTAINS)) || (io.flags & VGB_FUSED_DTO_INSIDE_ONLY))
+      c = Ops::contains(prm, l);
+    if (ops & (1u << VGB_OP_CONTAINS)) static_cast<uint8_t *>(io.out[VGB_OP_CONTAINS])[i] = c;
+    if (ops & (1u << VGB_OP_INSIDE))
+      static_cast<int32_t *>(io.out[VGB_OP_INSIDE])[i] = Ops::inside(prm, l);
+    if (ops & (1u << VGB_OP_SAFETY_TO_IN))
+      static_cast<double *>(io.out[VGB_OP_SAFETY_TO_IN])[i] = Ops::safety_to_in(prm, l);
+    if (ops & (1u << VGB_OP_SAFETY_TO_OUT))
+      static_cast<double *>(io.out[VGB_OP_SAFETY_TO_OUT])[i] = Ops::safety_to_out(prm, m);
+    if (ops & (1u << VGB_OP_DISTANCE_TO_IN))
+      static_cast<double *>(io.out[VGB_OP_DISTANCE_TO_IN])[i] =
+          Ops::distance_to_in(prm, l, xf_dir(X, d), ldg(io.step + i));
+    if (ops & (1u << VGB_OP_DISTANCE_TO_OUT)) {
+      R r = Lim<R>::inf();
+      if (!(io.flags & VGB_FUSED_DTO_INSIDE_ONLY) || c)
+        r = Ops::distance_to_out(prm, m, d, ldg(io.step + i));
+      static_cast<double *>(io.out[VGB_OP_DISTANCE_TO_OUT])[i] = r;
+    }
+  }
+}
+
+}  // namespace vgb

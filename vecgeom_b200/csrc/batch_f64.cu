@@ -1,0 +1,87 @@
+// batch_f64.cu -- FP64 instantiations of the batch kernels.
+//
+// Compiled with -fmad=false (see the Makefile): no a*b+c is contracted into an
+// FMA, so each result rounds exactly as the reference Scalar build compiled
+// with -ffp-contract=off.
+#include "batch.cuh"
+#include "dispatch.h"
+#include "geometry.h"
+
+namespace vgb {
+
+static int grid_for(int64_t n) {
+  // enough CTAs to fill 148 SMs x 8 resident 256-thread CTAs; grid-stride beyond
+  const int64_t want = (n + kBatchBlock - 1) / kBatchBlock;
+  const int64_t cap = 148 * 8 * 4;
+  return (int)(want < 1 ? 1 : (want > cap ? cap : want));
+}
+
+template <class Ops, class P>
+static vgb_status launch_ops(const P &prm, const DXform &X, int op, const BatchIO &io,
+                             cudaStream_t s) {
+  const int grid = grid_for(io.n);
+  switch (op) {
+#define VGB_OP_CASE(OPC)                                                      \
+  case OPC:                                                                   \
+    k_batch<Ops, P, OPC><<<grid, kBatchBlock, 0, s>>>(prm, X, io);            \
+    break;
+    VGB_OP_CASE(VGB_OP_CONTAINS)
+    VGB_OP_CASE(VGB_OP_INSIDE)
+    VGB_OP_CASE(VGB_OP_DISTANCE_TO_IN)
+    VGB_OP_CASE(VGB_OP_DISTANCE_TO_OUT)
+    VGB_OP_CASE(VGB_OP_SAFETY_TO_IN)
+    VGB_OP_CASE(VGB_OP_SAFETY_TO_OUT)
+    VGB_OP_CASE(VGB_OP_DISTANCE_TO_IN_MINIMIZE)
+    VGB_OP_CASE(VGB_OP_SAFETY_TO_IN_MINIMIZE)
+    VGB_OP_CASE(VGB_OP_SAFETY_TO_OUT_MINIMIZE)
+    VGB_OP_CASE(VGB_OP_DISTANCE_TO_OUT_NODE)
+    VGB_OP_CASE(VGB_OP_PLACED_DISTANCE_TO_OUT)
+#undef VGB_OP_CASE
+  default:
+    return set_error(VGB_EINVAL, "vgb_batch: unknown op %d", op);
+  }
+  count_launch();
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_error(e, "vgb_batch: kernel launch");
+  return VGB_OK;
+}
+
+template <class Ops, class P>
+static vgb_status launch_fused(const P &prm, const DXform &X, const FusedIO &io,
+                               cudaStream_t s) {
+  k_fused<Ops, P><<<grid_for(io.n), kBatchBlock, 0, s>>>(prm, X, io);
+  count_launch();
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_error(e, "vgb_batch_fused: kernel launch");
+  return VGB_OK;
+}
+
+vgb_status launch_batch_f64(const vgb_geometry *g, int32_t placed, int op, const BatchIO &io,
+                            cudaStream_t s) {
+  const PlacedRec &pr = g->placed[placed];
+  const DXform &X = g->xforms[pr.xform];
+  const int type = g->unplaced[pr.unplaced].type;
+  const void *prm = shape_params(g, pr.unplaced);
+  switch (type) {
+  case VGB_SHAPE_BOX:
+    return launch_ops<BoxOps<double>>(*static_cast<const BoxP *>(prm), X, op, io, s);
+  default:
+    return set_error(VGB_ENOTSUP, "vgb_batch: shape type %d not supported", type);
+  }
+}
+
+vgb_status launch_fused_f64(const vgb_geometry *g, int32_t placed, const FusedIO &io,
+                            cudaStream_t s) {
+  const PlacedRec &pr = g->placed[placed];
+  const DXform &X = g->xforms[pr.xform];
+  const int type = g->unplaced[pr.unplaced].type;
+  const void *prm = shape_params(g, pr.unplaced);
+  switch (type) {
+  case VGB_SHAPE_BOX:
+    return launch_fused<BoxOps<double>>(*static_cast<const BoxP *>(prm), X, io, s);
+  default:
+    return set_error(VGB_ENOTSUP, "vgb_batch_fused: shape type %d not supported", type);
+  }
+}
+
+}  // namespace vgb

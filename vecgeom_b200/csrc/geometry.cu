@@ -1,0 +1,390 @@
+// geometry.cu -- geometry construction, derived shape parameters and the bulk
+// device upload (replaces CudaManager, source/CudaManager.cpp:39-322).
+//
+// Host code here is compiled with -ffp-contract=off: the derived parameters of
+// each shape are computed with the same formulas and rounding as the reference
+// constructors, so the device kernels see bit-identical constants.
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+
+#include "geometry.h"
+#include "shapes.cuh"
+
+namespace vgb {
+
+static thread_local char g_err[512] = "";
+static thread_local int64_t g_launches = 0;
+
+vgb_status set_error(vgb_status s, const char *fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+  return s;
+}
+
+vgb_status cuda_error(cudaError_t e, const char *what) {
+  if (e == cudaErrorMemoryAllocation)
+    return set_error(VGB_ENOMEM, "%s: %s", what, cudaGetErrorString(e));
+  return set_error(VGB_ECUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+void count_launch(int n) { g_launches += n; }
+
+// ---------------------------------------------------------------------------
+// Transformation3D (source/Transformation3D.cpp)
+// ---------------------------------------------------------------------------
+
+// :138-150 GenerateRotationCode
+static int gen_rot_code(const double *r) {
+  int code = 0;
+  for (int i = 0; i < 9; ++i) code |= (1 << i) * (std::fabs(r[i]) > kTolerance);
+  if (code == 0x111 && (r[0] == 1. && r[4] == 1. && r[8] == 1.)) code = 0x200;
+  return code;
+}
+
+// management/TransformationSpecializations.icc: codes with a specialised
+// placed volume; everything else runs the generic rotation.
+static int specialised_rot(int code) {
+  static const int codes[] = {0x1b1, 0x18e, 0x076, 0x16a, 0x155, 0x0ad, 0x0dc, 0x0e3,
+                              0x11b, 0x0a1, 0x10a, 0x046, 0x062, 0x054, 0x111, 0x200};
+  for (int c : codes)
+    if (c == code) return code;
+  return -1;
+}
+
+static void set_codes(RawXform &x) {
+  // :80-89 SetProperties; source/UnplacedVolume.cpp:23-24
+  const bool has_t = std::fabs(x.t[0]) > kTolerance || std::fabs(x.t[1]) > kTolerance ||
+                     std::fabs(x.t[2]) > kTolerance;
+  x.trans_code = has_t ? -1 : 0;
+  x.rot_code = specialised_rot(gen_rot_code(x.r));
+}
+
+// The effective device transform of one placement.  generic_only mirrors
+// shapes whose placed volumes always take Transform<kGeneric,kGeneric>
+// (source/UnplacedPolyhedron.cpp:321-333).
+static DXform effective(const RawXform &x, bool generic_only) {
+  DXform d;
+  std::memset(&d, 0, sizeof(d));
+  const int tcode = generic_only ? -1 : x.trans_code;
+  const int rcode = generic_only ? -1 : x.rot_code;
+  if (tcode != 0) {
+    d.flags |= kXfHasTrans;
+    for (int i = 0; i < 3; ++i) d.t[i] = x.t[i];
+  }
+  if (rcode != 0x200) {
+    d.flags |= kXfHasRot;
+    for (int i = 0; i < 9; ++i) {
+      const bool keep = (rcode == -1) || ((rcode >> i) & 1);
+      d.r[i] = keep ? x.r[i] : 0.;
+    }
+    if (rcode == 0x16a) d.flags |= kXfQuirk16A;
+  } else {
+    d.r[0] = d.r[4] = d.r[8] = 1.;
+  }
+  return d;
+}
+
+}  // namespace vgb
+
+using namespace vgb;
+
+#define VGB_CHECK_G(g)                                                          \
+  do {                                                                          \
+    if (!(g)) return set_error(VGB_EINVAL, "%s: geometry is NULL", __func__);   \
+  } while (0)
+#define VGB_CHECK_OPEN(g)                                                       \
+  do {                                                                          \
+    VGB_CHECK_G(g);                                                             \
+    if ((g)->closed)                                                            \
+      return set_error(VGB_EINVAL, "%s: geometry is closed", __func__);         \
+  } while (0)
+
+static vgb_status add_unplaced(vgb_geometry *g, int type, const void *rec, size_t bytes,
+                               int32_t extra, int32_t *id) {
+  // 16-byte aligned records in the pool
+  while (g->params.size() % 2) g->params.push_back(0.);
+  const size_t nd = (bytes + sizeof(double) - 1) / sizeof(double);
+  UnplacedRec u;
+  u.type = type;
+  u.param_off = (int32_t)g->params.size();
+  u.param_len = (int32_t)nd;
+  u.extra = extra;
+  g->params.resize(g->params.size() + nd + (nd % 2), 0.);
+  std::memcpy(g->params.data() + u.param_off, rec, bytes);
+  g->unplaced.push_back(u);
+  if (id) *id = (int32_t)g->unplaced.size() - 1;
+  return VGB_OK;
+}
+
+// Depth of the tree below a logical volume (GeoManager::getMaxDepth counts
+// levels from the world, management/GeoManager.h:191).
+static int depth_of(const vgb_geometry *g, int32_t logical, int guard) {
+  if (guard > 64) return -1;
+  int best = 0;
+  for (int32_t d : g->logical_daughters[logical]) {
+    const int sub = depth_of(g, g->placed[d].logical, guard + 1);
+    if (sub < 0) return -1;
+    if (sub > best) best = sub;
+  }
+  return best + 1;
+}
+
+template <class T>
+static vgb_status upload(const std::vector<T> &h, T **d, int64_t *bytes) {
+  const size_t n = h.empty() ? 1 : h.size();
+  cudaError_t e = cudaMalloc((void **)d, n * sizeof(T));
+  if (e != cudaSuccess) return cuda_error(e, "vgb_geometry_close: cudaMalloc");
+  *bytes += (int64_t)(n * sizeof(T));
+  if (!h.empty()) {
+    e = cudaMemcpy(*d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cuda_error(e, "vgb_geometry_close: cudaMemcpy");
+  }
+  return VGB_OK;
+}
+
+extern "C" {
+
+const char *vgb_last_error(void) { return vgb::g_err; }
+const char *vgb_version(void) { return "vgb 0.1 (sm_100a)"; }
+int64_t vgb_launch_count(void) { return vgb::g_launches; }
+void vgb_launch_count_reset(void) { vgb::g_launches = 0; }
+
+vgb_status vgb_geometry_create(vgb_geometry **g) {
+  if (!g) return set_error(VGB_EINVAL, "vgb_geometry_create: out pointer is NULL");
+  *g = new (std::nothrow) vgb_geometry();
+  if (!*g) return set_error(VGB_ENOMEM, "vgb_geometry_create: out of host memory");
+  return VGB_OK;
+}
+
+vgb_status vgb_geometry_destroy(vgb_geometry *g) {
+  if (!g) return VGB_OK;
+  if (g->device >= 0) {
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(g->device);
+    cudaFree(g->dev.params);
+    cudaFree(g->dev.xforms);
+    cudaFree(g->dev.placed);
+    cudaFree(g->dev.logicals);
+    cudaFree(g->dev.daughters);
+    cudaFree(g->staging);
+    if (g->staging_streams[0]) cudaStreamDestroy(g->staging_streams[0]);
+    if (g->staging_streams[1]) cudaStreamDestroy(g->staging_streams[1]);
+    if (g->staging_start) cudaEventDestroy(g->staging_start);
+    cudaSetDevice(prev);
+  }
+  delete g;
+  return VGB_OK;
+}
+
+vgb_status vgb_unplaced_box(vgb_geometry *g, double dx, double dy, double dz, int32_t *id) {
+  VGB_CHECK_OPEN(g);
+  if (!(dx > 0 && dy > 0 && dz > 0))
+    return set_error(VGB_EINVAL, "vgb_unplaced_box: half-lengths must be > 0");
+  BoxP b;
+  b.d[0] = dx;
+  b.d[1] = dy;
+  b.d[2] = dz;
+  return add_unplaced(g, VGB_SHAPE_BOX, &b, sizeof(b), 0, id);
+}
+
+vgb_status vgb_transformation(vgb_geometry *g, double tx, double ty, double tz, double phi,
+                              double theta, double psi, int32_t *id) {
+  VGB_CHECK_OPEN(g);
+  RawXform x;
+  // source/Transformation3D.cpp:93-114 SetRotation(phi, theta, psi), degrees
+  const double sinphi = std::sin(kDegToRad * phi), cosphi = std::cos(kDegToRad * phi);
+  const double sinthe = std::sin(kDegToRad * theta), costhe = std::cos(kDegToRad * theta);
+  const double sinpsi = std::sin(kDegToRad * psi), cospsi = std::cos(kDegToRad * psi);
+  x.t[0] = tx;
+  x.t[1] = ty;
+  x.t[2] = tz;
+  x.r[0] = cospsi * cosphi - costhe * sinphi * sinpsi;
+  x.r[1] = -sinpsi * cosphi - costhe * sinphi * cospsi;
+  x.r[2] = sinthe * sinphi;
+  x.r[3] = cospsi * sinphi + costhe * cosphi * sinpsi;
+  x.r[4] = -sinpsi * sinphi + costhe * cosphi * cospsi;
+  x.r[5] = -sinthe * cosphi;
+  x.r[6] = sinpsi * sinthe;
+  x.r[7] = cospsi * sinthe;
+  x.r[8] = costhe;
+  set_codes(x);
+  g->raw_xforms.push_back(x);
+  if (id) *id = (int32_t)g->raw_xforms.size() - 1;
+  return VGB_OK;
+}
+
+vgb_status vgb_transformation_matrix(vgb_geometry *g, double tx, double ty, double tz,
+                                     const double *r9, int32_t *id) {
+  VGB_CHECK_OPEN(g);
+  if (!r9) return set_error(VGB_EINVAL, "vgb_transformation_matrix: r9 is NULL");
+  RawXform x;
+  x.t[0] = tx;
+  x.t[1] = ty;
+  x.t[2] = tz;
+  for (int i = 0; i < 9; ++i) x.r[i] = r9[i];
+  set_codes(x);
+  g->raw_xforms.push_back(x);
+  if (id) *id = (int32_t)g->raw_xforms.size() - 1;
+  return VGB_OK;
+}
+
+vgb_status vgb_logical_volume(vgb_geometry *g, const char *label, int32_t unplaced,
+                              int32_t *id) {
+  VGB_CHECK_OPEN(g);
+  if (unplaced < 0 || unplaced >= (int32_t)g->unplaced.size())
+    return set_error(VGB_EINVAL, "vgb_logical_volume: unknown unplaced id %d", unplaced);
+  LogicalRec l;
+  l.unplaced = unplaced;
+  l.dfirst = 0;
+  l.dcount = 0;
+  l.pad = 0;
+  g->logicals.push_back(l);
+  g->logical_daughters.emplace_back();
+  g->labels.push_back(label ? label : "");
+  if (id) *id = (int32_t)g->logicals.size() - 1;
+  return VGB_OK;
+}
+
+vgb_status vgb_place(vgb_geometry *g, int32_t logical, int32_t transformation,
+                     int32_t *placed) {
+  VGB_CHECK_OPEN(g);
+  if (logical < 0 || logical >= (int32_t)g->logicals.size())
+    return set_error(VGB_EINVAL, "vgb_place: unknown logical volume %d", logical);
+  if (transformation < 0 || transformation >= (int32_t)g->raw_xforms.size())
+    return set_error(VGB_EINVAL, "vgb_place: unknown transformation %d", transformation);
+  PlacedRec p;
+  p.logical = logical;
+  p.unplaced = g->logicals[logical].unplaced;
+  p.xform = (int32_t)g->xforms.size();
+  p.pad = 0;
+  const int type = g->unplaced[p.unplaced].type;
+  g->xforms.push_back(effective(g->raw_xforms[transformation], type == VGB_SHAPE_POLYHEDRON));
+  g->placed.push_back(p);
+  if (placed) *placed = (int32_t)g->placed.size() - 1;
+  return VGB_OK;
+}
+
+vgb_status vgb_place_daughter(vgb_geometry *g, int32_t mother_logical, int32_t daughter_logical,
+                              int32_t transformation, int32_t *placed) {
+  VGB_CHECK_OPEN(g);
+  if (mother_logical < 0 || mother_logical >= (int32_t)g->logicals.size())
+    return set_error(VGB_EINVAL, "vgb_place_daughter: unknown mother %d", mother_logical);
+  int32_t id = -1;
+  vgb_status s = vgb_place(g, daughter_logical, transformation, &id);
+  if (s != VGB_OK) return s;
+  g->logical_daughters[mother_logical].push_back(id);
+  if (placed) *placed = id;
+  return VGB_OK;
+}
+
+vgb_status vgb_set_world(vgb_geometry *g, int32_t placed) {
+  VGB_CHECK_OPEN(g);
+  if (placed < 0 || placed >= (int32_t)g->placed.size())
+    return set_error(VGB_EINVAL, "vgb_set_world: unknown placed volume %d", placed);
+  g->world = placed;
+  return VGB_OK;
+}
+
+vgb_status vgb_geometry_close(vgb_geometry *g) {
+  VGB_CHECK_OPEN(g);
+  // CSR of daughters in insertion order (source/LogicalVolume.cpp:84-102)
+  g->daughters.clear();
+  for (size_t l = 0; l < g->logicals.size(); ++l) {
+    g->logicals[l].dfirst = (int32_t)g->daughters.size();
+    g->logicals[l].dcount = (int32_t)g->logical_daughters[l].size();
+    for (int32_t d : g->logical_daughters[l]) g->daughters.push_back(d);
+  }
+  if (g->world >= 0) {
+    g->max_depth = depth_of(g, g->placed[g->world].logical, 0);
+    if (g->max_depth < 0)
+      return set_error(VGB_EINVAL, "vgb_geometry_close: volume tree deeper than 64 levels");
+  }
+  // shape records that hold device pointers are fixed up after the pool lands
+  cudaError_t e = cudaGetDevice(&g->device);
+  if (e != cudaSuccess) return cuda_error(e, "vgb_geometry_close: cudaGetDevice");
+  vgb_status s;
+  {
+    // allocate the pool, let shape records that reference other parts of the
+    // pool store device addresses, then copy it
+    const size_t n = g->params.empty() ? 2 : g->params.size();
+    e = cudaMalloc((void **)&g->dev.params, n * sizeof(double));
+    if (e != cudaSuccess) return cuda_error(e, "vgb_geometry_close: cudaMalloc");
+    g->dev.bytes += (int64_t)(n * sizeof(double));
+    if ((s = finalize_shapes(g)) != VGB_OK) return s;
+    if (!g->params.empty()) {
+      e = cudaMemcpy(g->dev.params, g->params.data(), g->params.size() * sizeof(double),
+                     cudaMemcpyHostToDevice);
+      if (e != cudaSuccess) return cuda_error(e, "vgb_geometry_close: cudaMemcpy");
+    }
+  }
+  if ((s = upload(g->xforms, &g->dev.xforms, &g->dev.bytes)) != VGB_OK) return s;
+  if ((s = upload(g->placed, &g->dev.placed, &g->dev.bytes)) != VGB_OK) return s;
+  if ((s = upload(g->logicals, &g->dev.logicals, &g->dev.bytes)) != VGB_OK) return s;
+  if ((s = upload(g->daughters, &g->dev.daughters, &g->dev.bytes)) != VGB_OK) return s;
+  g->closed = true;
+  return VGB_OK;
+}
+
+vgb_status vgb_geometry_max_depth(const vgb_geometry *g, int32_t *depth) {
+  VGB_CHECK_G(g);
+  if (!depth) return set_error(VGB_EINVAL, "vgb_geometry_max_depth: out pointer is NULL");
+  *depth = g->max_depth;
+  return VGB_OK;
+}
+
+vgb_status vgb_geometry_device_bytes(const vgb_geometry *g, int64_t *bytes) {
+  VGB_CHECK_G(g);
+  if (!bytes) return set_error(VGB_EINVAL, "vgb_geometry_device_bytes: out pointer is NULL");
+  *bytes = g->dev.bytes;
+  return VGB_OK;
+}
+
+}  // extern "C"
+
+namespace vgb {
+vgb_status finalize_shapes(vgb_geometry *g) {
+  (void)g;
+  return VGB_OK;
+}
+}  // namespace vgb
+
+// ---------------------------------------------------------------------------
+// shapes not yet uploaded by this build report VGB_ENOTSUP
+// ---------------------------------------------------------------------------
+extern "C" {
+#define VGB_NOTYET(name) return set_error(VGB_ENOTSUP, name ": shape not available yet")
+vgb_status vgb_unplaced_tube(vgb_geometry *, double, double, double, double, double, int32_t *) {
+  VGB_NOTYET("vgb_unplaced_tube");
+}
+vgb_status vgb_unplaced_cone(vgb_geometry *, double, double, double, double, double, double,
+                             double, int32_t *) {
+  VGB_NOTYET("vgb_unplaced_cone");
+}
+vgb_status vgb_unplaced_sphere(vgb_geometry *, double, double, double, double, double, double,
+                               int32_t *) {
+  VGB_NOTYET("vgb_unplaced_sphere");
+}
+vgb_status vgb_unplaced_torus(vgb_geometry *, double, double, double, double, double, int32_t *) {
+  VGB_NOTYET("vgb_unplaced_torus");
+}
+vgb_status vgb_unplaced_polycone(vgb_geometry *, double, double, int32_t, const double *,
+                                 const double *, const double *, int32_t *) {
+  VGB_NOTYET("vgb_unplaced_polycone");
+}
+vgb_status vgb_unplaced_polyhedron(vgb_geometry *, double, double, int32_t, int32_t,
+                                   const double *, const double *, const double *, int32_t *) {
+  VGB_NOTYET("vgb_unplaced_polyhedron");
+}
+vgb_status vgb_unplaced_trd(vgb_geometry *, double, double, double, double, double, int32_t *) {
+  VGB_NOTYET("vgb_unplaced_trd");
+}
+vgb_status vgb_unplaced_boolean(vgb_geometry *, int32_t, int32_t, int32_t, int32_t *) {
+  VGB_NOTYET("vgb_unplaced_boolean");
+}
+#undef VGB_NOTYET
+}

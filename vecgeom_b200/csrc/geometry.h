@@ -1,0 +1,102 @@
+// geometry.h -- host-side geometry registry of libvgb and its device image.
+//
+// The reference keeps an object graph (Unplaced*, LogicalVolume, VPlacedVolume,
+// Transformation3D) and copies it to the GPU object by object with one
+// constructor kernel each (source/CudaManager.cpp:39-322,
+// backend/cuda/Interface.h:24-32).  Here the same graph is recorded in flat
+// tables and vgb_geometry_close() uploads each table with one copy:
+//   params    double pool; each unplaced shape owns a 16-byte aligned record
+//   xforms    DXform per Transformation3D (effective matrix, see vgb_core.cuh)
+//   placed    {unplaced, logical, xform} per placed volume
+//   logicals  {unplaced, first daughter, daughter count} per logical volume
+//   daughters placed ids, CSR over logicals, in insertion order
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/vgb.h"
+#include "vgb_core.cuh"
+
+namespace vgb {
+
+struct UnplacedRec {
+  int32_t type;       // vgb_shape_type
+  int32_t param_off;  // offset in doubles into the param pool (16-byte aligned)
+  int32_t param_len;  // length in doubles
+  int32_t extra;      // shape-specific (e.g. boolean left placed id)
+};
+
+struct PlacedRec {
+  int32_t unplaced;
+  int32_t logical;
+  int32_t xform;
+  int32_t pad;
+};
+
+struct LogicalRec {
+  int32_t unplaced;
+  int32_t dfirst;
+  int32_t dcount;
+  int32_t pad;
+};
+
+struct RawXform {
+  double t[3];
+  double r[9];
+  int trans_code;  // 0 kIdentity, -1 kGeneric
+  int rot_code;    // specialised code, 0x200 identity or -1 generic
+};
+
+struct DeviceImage {
+  double *params = nullptr;
+  DXform *xforms = nullptr;
+  PlacedRec *placed = nullptr;
+  LogicalRec *logicals = nullptr;
+  int32_t *daughters = nullptr;
+  int64_t bytes = 0;
+};
+
+}  // namespace vgb
+
+struct vgb_geometry {
+  std::vector<vgb::UnplacedRec> unplaced;
+  std::vector<double> params;
+  std::vector<vgb::RawXform> raw_xforms;
+  std::vector<vgb::DXform> xforms;  // per (placed volume), effective for its shape
+  std::vector<std::string> labels;
+  std::vector<vgb::LogicalRec> logicals;
+  std::vector<std::vector<int32_t>> logical_daughters;
+  std::vector<vgb::PlacedRec> placed;
+  std::vector<int32_t> daughters;
+  int32_t world = -1;
+  int32_t max_depth = 0;
+  bool closed = false;
+  int device = -1;
+  vgb::DeviceImage dev;
+  // host-pointer calls stage through one device buffer on two internal streams
+  std::mutex staging_mu;  // serialises host-pointer calls that share the buffer
+  void *staging = nullptr;
+  size_t staging_bytes = 0;
+  cudaStream_t staging_streams[2] = {nullptr, nullptr};
+  cudaEvent_t staging_start = nullptr;
+};
+
+namespace vgb {
+// Error reporting (thread-local message, status return).
+vgb_status set_error(vgb_status s, const char *fmt, ...);
+vgb_status cuda_error(cudaError_t e, const char *what);
+void count_launch(int n = 1);
+
+// The host copy of a shape's parameter record (for passing by value).
+inline const void *shape_params(const vgb_geometry *g, int32_t unplaced) {
+  return g->params.data() + g->unplaced[unplaced].param_off;
+}
+// Device address of a shape's parameter record.
+inline const double *shape_params_dev(const vgb_geometry *g, int32_t unplaced) {
+  return g->dev.params + g->unplaced[unplaced].param_off;
+}
+}  // namespace vgb

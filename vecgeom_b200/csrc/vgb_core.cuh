@@ -1,0 +1,137 @@
+// vgb_core.cuh -- constants, small vector type and placement transforms shared by
+// every kernel of libvgb.
+//
+// The FP64 kernels are compiled with -fmad=false: every a*b+c rounds twice, as
+// in the reference Scalar build compiled with -ffp-contract=off, so Inside/
+// Contains and the navigator's next volume come out bit-identical.
+#pragma once
+
+#include <cstdint>
+#include <cfloat>
+#include <cmath>
+
+#ifdef __CUDACC__
+#define VGB_HD __host__ __device__ __forceinline__
+#define VGB_D __device__ __forceinline__
+#else
+#define VGB_HD inline
+#define VGB_D inline
+#endif
+
+namespace vgb {
+
+// base/Global.h:267-302
+constexpr double kPi = 3.14159265358979323846;
+constexpr double kTwoPi = 2. * kPi;
+constexpr double kDegToRad = kPi / 180.;
+constexpr double kTolerance = 1e-9;
+constexpr double kHalfTolerance = 0.5 * kTolerance;
+constexpr double kRadTolerance = 1e-9;
+constexpr double kAngTolerance = 1e-9;
+constexpr double kMinimum = DBL_MIN;
+constexpr double kTiny = 1e-30;
+
+// EnumInside (base/Global.h:196-207)
+constexpr int kInside = 0;
+constexpr int kSurface = 1;
+constexpr int kOutside = 2;
+
+template <class R> struct Lim;
+template <> struct Lim<double> {
+  static VGB_HD double inf() { return HUGE_VAL; }
+  static VGB_HD double minimum() { return DBL_MIN; }
+};
+template <> struct Lim<float> {
+  static VGB_HD float inf() { return HUGE_VALF; }
+  static VGB_HD float minimum() { return FLT_MIN; }
+};
+
+template <class R> struct V3 {
+  R x, y, z;
+  VGB_HD R operator[](int i) const { return i == 0 ? x : (i == 1 ? y : z); }
+};
+
+template <class R> VGB_HD V3<R> mk3(R x, R y, R z) { return V3<R>{x, y, z}; }
+
+// Placement transform as uploaded to the device.  r/t hold the *effective*
+// matrix: the entries a specialised rotation code drops
+// (base/Transformation3D.h:367-480, management/TransformationSpecializations.icc)
+// are zeroed, and t is zero when the translation code is kIdentity.  The generic
+// row-order sum over r then reproduces every specialised DoRotation<code>.
+enum : int32_t {
+  kXfHasTrans = 1,   // translation applied (translation code kGeneric)
+  kXfHasRot = 2,     // rotation applied (rotation code != 0x200)
+  kXfQuirk16A = 4,   // rotation code 0x16A: third row is m2*R5 + m2*R8 (reference typo,
+                     // base/Transformation3D.h:391)
+};
+
+struct alignas(16) DXform {
+  double r[9];
+  double t[3];
+  int32_t flags;
+  int32_t pad;
+};
+
+// base/Transformation3D.h:533-562 Transform<trans_code, rot_code>
+template <class R>
+VGB_HD V3<R> xf_point(const DXform &X, const V3<R> &m) {
+  V3<R> a = m;
+  if (X.flags & kXfHasTrans) {
+    a.x = m.x - (R)X.t[0];
+    a.y = m.y - (R)X.t[1];
+    a.z = m.z - (R)X.t[2];
+  }
+  if (!(X.flags & kXfHasRot)) return a;
+  V3<R> l;
+  l.x = a.x * (R)X.r[0];
+  l.y = a.x * (R)X.r[1];
+  l.z = a.x * (R)X.r[2];
+  l.x = l.x + a.y * (R)X.r[3];
+  l.y = l.y + a.y * (R)X.r[4];
+  l.z = l.z + a.y * (R)X.r[5];
+  l.x = l.x + a.z * (R)X.r[6];
+  l.y = l.y + a.z * (R)X.r[7];
+  l.z = l.z + a.z * (R)X.r[8];
+  if (X.flags & kXfQuirk16A) l.z = a.z * (R)X.r[5] + a.z * (R)X.r[8];
+  return l;
+}
+
+// base/Transformation3D.h:751-767 TransformDirection<rot_code>
+template <class R>
+VGB_HD V3<R> xf_dir(const DXform &X, const V3<R> &m) {
+  if (!(X.flags & kXfHasRot)) return m;
+  V3<R> l;
+  l.x = m.x * (R)X.r[0];
+  l.y = m.x * (R)X.r[1];
+  l.z = m.x * (R)X.r[2];
+  l.x = l.x + m.y * (R)X.r[3];
+  l.y = l.y + m.y * (R)X.r[4];
+  l.z = l.z + m.y * (R)X.r[5];
+  l.x = l.x + m.z * (R)X.r[6];
+  l.y = l.y + m.z * (R)X.r[7];
+  l.z = l.z + m.z * (R)X.r[8];
+  if (X.flags & kXfQuirk16A) l.z = m.z * (R)X.r[5] + m.z * (R)X.r[8];
+  return l;
+}
+
+// base/Transformation3D.h:598-632 InverseTransform (local -> master), used by the
+// navigator to compose paths.
+template <class R>
+VGB_HD V3<R> xf_inverse_point(const DXform &X, const V3<R> &l) {
+  V3<R> m;
+  m.x = (R)X.t[0];
+  m.x = m.x + l.x * (R)X.r[0];
+  m.x = m.x + l.y * (R)X.r[1];
+  m.x = m.x + l.z * (R)X.r[2];
+  m.y = (R)X.t[1];
+  m.y = m.y + l.x * (R)X.r[3];
+  m.y = m.y + l.y * (R)X.r[4];
+  m.y = m.y + l.z * (R)X.r[5];
+  m.z = (R)X.t[2];
+  m.z = m.z + l.x * (R)X.r[6];
+  m.z = m.z + l.y * (R)X.r[7];
+  m.z = m.z + l.z * (R)X.r[8];
+  return m;
+}
+
+}  // namespace vgb

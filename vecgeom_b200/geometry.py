@@ -1,0 +1,276 @@
+"""Host-side mirror of the reference's geometry and VPlacedVolume SOA3D API.
+
+Names, argument order and meaning follow the reference so that call sites read
+alike:
+  - ``Geometry.UnplacedBox(dx, dy, dz)`` ... (volumes/Unplaced*.h constructors)
+  - ``Geometry.Transformation3D(tx, ty, tz, phi, theta, psi)`` (degrees,
+    source/Transformation3D.cpp:36-44)
+  - ``Geometry.LogicalVolume(label, unplaced)``, ``LogicalVolume.Place(t)``,
+    ``LogicalVolume.PlaceDaughter(daughter, t)`` (source/LogicalVolume.cpp:60-102)
+  - ``PlacedVolume.Contains(points, out)``, ``Inside``, ``DistanceToIn(points,
+    dirs, step_max, out)``, ``DistanceToOut``, ``SafetyToIn``, ``SafetyToOut``,
+    ``DistanceToInMinimize``, ``SafetyToInMinimize``, ``SafetyToOutMinimize``
+    (volumes/PlacedVolume.h:145-250)
+Every call goes through libvgb.so's C ABI.  Arrays may be numpy arrays (host
+memory, staged by the library) or torch tensors on the geometry's CUDA device.
+Errors raise VgbError instead of asserting.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib as L
+from ._lib import check
+
+kInside, kSurface, kOutside = 0, 1, 2
+kTolerance = 1e-9
+kInfinity = float("inf")
+
+
+def _addr(a) -> int | None:
+    """Address of a contiguous array (numpy or torch) or None."""
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        if not a.flags["C_CONTIGUOUS"]:
+            raise ValueError("arrays must be contiguous")
+        return a.ctypes.data
+    if hasattr(a, "data_ptr"):
+        if not a.is_contiguous():
+            raise ValueError("tensors must be contiguous")
+        return a.data_ptr()
+    raise TypeError(f"unsupported array type {type(a)!r}")
+
+
+def _check_dtype(a, kind: str) -> None:
+    if a is None:
+        return
+    want = {"f8": ("float64",), "i4": ("int32",), "u1": ("uint8", "bool")}[kind]
+    name = str(a.dtype).replace("torch.", "")
+    if name not in want:
+        raise TypeError(f"expected dtype {want[0]}, got {name}")
+
+
+def _len(a) -> int:
+    return int(a.shape[0])
+
+
+class SOA3D:
+    """Structure-of-arrays batch of 3-vectors (base/SOA3D.h:32-39)."""
+
+    def __init__(self, x, y, z):
+        if not (_len(x) == _len(y) == _len(z)):
+            raise ValueError("SOA3D components must have one length")
+        for a in (x, y, z):
+            _check_dtype(a, "f8")
+        self.x, self.y, self.z = x, y, z
+
+    def size(self) -> int:
+        return _len(self.x)
+
+    def __len__(self) -> int:
+        return self.size()
+
+
+@dataclass
+class LogicalVolume:
+    geometry: "Geometry"
+    id: int
+    label: str
+
+    def Place(self, transformation: int) -> "PlacedVolume":
+        out = ctypes.c_int32()
+        check(L.lib().vgb_place(self.geometry.handle, self.id, transformation, ctypes.byref(out)))
+        return PlacedVolume(self.geometry, out.value, self)
+
+    def PlaceDaughter(self, daughter: "LogicalVolume", transformation: int) -> "PlacedVolume":
+        out = ctypes.c_int32()
+        check(L.lib().vgb_place_daughter(self.geometry.handle, self.id, daughter.id,
+                                         transformation, ctypes.byref(out)))
+        return PlacedVolume(self.geometry, out.value, daughter)
+
+
+class PlacedVolume:
+    """A placed volume; its methods are the VPlacedVolume SOA3D virtuals."""
+
+    def __init__(self, geometry: "Geometry", pid: int, logical: LogicalVolume):
+        self.geometry = geometry
+        self.id = pid
+        self.logical = logical
+
+    # -- generic entry -------------------------------------------------------
+    def batch(self, op: int, points: SOA3D, out, dirs: SOA3D | None = None, step_max=None,
+              aux=None, daughter: int = 0, precision: int = L.PREC_FP64, stream=None) -> None:
+        g = self.geometry
+        g._require_closed()
+        n = points.size()
+        if _len(out) < n:
+            raise ValueError("output shorter than the batch")
+        if dirs is not None and dirs.size() != n:
+            raise ValueError("directions must match the points")
+        if step_max is not None:
+            _check_dtype(step_max, "f8")
+        _check_dtype(aux, "i4")
+        d = dirs
+        s = stream.cuda_stream if hasattr(stream, "cuda_stream") else stream
+        check(L.lib().vgb_batch(
+            g.handle, self.id, op, n, _addr(points.x), _addr(points.y), _addr(points.z),
+            _addr(d.x) if d else None, _addr(d.y) if d else None, _addr(d.z) if d else None,
+            _addr(step_max), _addr(out), _addr(aux), daughter, precision, s))
+
+    # -- the reference's method names ----------------------------------------
+    def Contains(self, points: SOA3D, out, **kw) -> None:
+        _check_dtype(out, "u1")
+        self.batch(L.OP_CONTAINS, points, out, **kw)
+
+    def Inside(self, points: SOA3D, out, **kw) -> None:
+        _check_dtype(out, "i4")
+        self.batch(L.OP_INSIDE, points, out, **kw)
+
+    def DistanceToIn(self, points: SOA3D, dirs: SOA3D, step_max, out, **kw) -> None:
+        _check_dtype(out, "f8")
+        self.batch(L.OP_DISTANCE_TO_IN, points, out, dirs, step_max, **kw)
+
+    def DistanceToInMinimize(self, points: SOA3D, dirs: SOA3D, daughterindex: int, out,
+                             nextnodeids, **kw) -> None:
+        _check_dtype(out, "f8")
+        self.batch(L.OP_DISTANCE_TO_IN_MINIMIZE, points, out, dirs, None, nextnodeids,
+                   daughterindex, **kw)
+
+    def DistanceToOut(self, points: SOA3D, dirs: SOA3D, step_max, out, nextnodeindex=None,
+                      **kw) -> None:
+        _check_dtype(out, "f8")
+        if nextnodeindex is None:
+            self.batch(L.OP_DISTANCE_TO_OUT, points, out, dirs, step_max, **kw)
+        else:
+            self.batch(L.OP_DISTANCE_TO_OUT_NODE, points, out, dirs, step_max, nextnodeindex,
+                       **kw)
+
+    def PlacedDistanceToOut(self, points: SOA3D, dirs: SOA3D, step_max, out, **kw) -> None:
+        _check_dtype(out, "f8")
+        self.batch(L.OP_PLACED_DISTANCE_TO_OUT, points, out, dirs, step_max, **kw)
+
+    def SafetyToIn(self, points: SOA3D, out, **kw) -> None:
+        _check_dtype(out, "f8")
+        self.batch(L.OP_SAFETY_TO_IN, points, out, **kw)
+
+    def SafetyToInMinimize(self, points: SOA3D, safeties, **kw) -> None:
+        _check_dtype(safeties, "f8")
+        self.batch(L.OP_SAFETY_TO_IN_MINIMIZE, points, safeties, **kw)
+
+    def SafetyToOut(self, points: SOA3D, out, **kw) -> None:
+        _check_dtype(out, "f8")
+        self.batch(L.OP_SAFETY_TO_OUT, points, out, **kw)
+
+    def SafetyToOutMinimize(self, points: SOA3D, safeties, **kw) -> None:
+        _check_dtype(safeties, "f8")
+        self.batch(L.OP_SAFETY_TO_OUT_MINIMIZE, points, safeties, **kw)
+
+    def fused(self, ops: int, points: SOA3D, outs: dict, dirs: SOA3D | None = None,
+              step_max=None, dto_inside_only: bool = False, precision: int = L.PREC_FP64,
+              stream=None) -> None:
+        """Several ops over the same points in one pass (vgb_batch_fused)."""
+        g = self.geometry
+        g._require_closed()
+        arr = (ctypes.c_void_p * 6)()
+        for k, v in outs.items():
+            arr[k] = _addr(v)
+        d = dirs
+        s = stream.cuda_stream if hasattr(stream, "cuda_stream") else stream
+        check(L.lib().vgb_batch_fused(
+            g.handle, self.id, ops, points.size(), _addr(points.x), _addr(points.y),
+            _addr(points.z), _addr(d.x) if d else None, _addr(d.y) if d else None,
+            _addr(d.z) if d else None, _addr(step_max), arr,
+            L.FUSED_DTO_INSIDE_ONLY if dto_inside_only else 0, precision, s))
+
+
+class Geometry:
+    """A geometry under construction, then closed and resident on the device."""
+
+    def __init__(self):
+        h = ctypes.c_void_p()
+        check(L.lib().vgb_geometry_create(ctypes.byref(h)))
+        self.handle = h
+        self.closed = False
+        self.world: PlacedVolume | None = None
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h is not None and L._lib is not None:
+            L._lib.vgb_geometry_destroy(h)
+            self.handle = None
+
+    def _id(self, fn, *args) -> int:
+        out = ctypes.c_int32()
+        check(fn(self.handle, *args, ctypes.byref(out)))
+        return out.value
+
+    def _require_closed(self) -> None:
+        if not self.closed:
+            raise L.VgbError(L.EINVAL, "geometry is not closed")
+
+    # -- unplaced shapes (volumes/Unplaced*.h) --------------------------------
+    def UnplacedBox(self, dx, dy, dz) -> int:
+        return self._id(L.lib().vgb_unplaced_box, dx, dy, dz)
+
+    def UnplacedTube(self, rmin, rmax, dz, sphi, dphi) -> int:
+        return self._id(L.lib().vgb_unplaced_tube, rmin, rmax, dz, sphi, dphi)
+
+    def UnplacedCone(self, rmin1, rmax1, rmin2, rmax2, dz, sphi, dphi) -> int:
+        return self._id(L.lib().vgb_unplaced_cone, rmin1, rmax1, rmin2, rmax2, dz, sphi, dphi)
+
+    def UnplacedSphere(self, rmin, rmax, sphi, dphi, stheta, dtheta) -> int:
+        return self._id(L.lib().vgb_unplaced_sphere, rmin, rmax, sphi, dphi, stheta, dtheta)
+
+    def UnplacedTorus(self, rmin, rmax, rtor, sphi, dphi) -> int:
+        return self._id(L.lib().vgb_unplaced_torus, rmin, rmax, rtor, sphi, dphi)
+
+    def UnplacedPolycone(self, sphi, dphi, rmin, rmax, z) -> int:
+        rmin, rmax, z = (np.ascontiguousarray(a, np.float64) for a in (rmin, rmax, z))
+        return self._id(L.lib().vgb_unplaced_polycone, sphi, dphi, len(z), rmin.ctypes.data,
+                        rmax.ctypes.data, z.ctypes.data)
+
+    def UnplacedPolyhedron(self, phi_start_deg, phi_delta_deg, sides, z, rmin, rmax) -> int:
+        rmin, rmax, z = (np.ascontiguousarray(a, np.float64) for a in (rmin, rmax, z))
+        return self._id(L.lib().vgb_unplaced_polyhedron, phi_start_deg, phi_delta_deg, sides,
+                        len(z), z.ctypes.data, rmin.ctypes.data, rmax.ctypes.data)
+
+    def UnplacedTrd(self, dx1, dx2, dy1, dy2, dz) -> int:
+        return self._id(L.lib().vgb_unplaced_trd, dx1, dx2, dy1, dy2, dz)
+
+    def UnplacedBooleanVolume(self, op: int, left: PlacedVolume, right: PlacedVolume) -> int:
+        return self._id(L.lib().vgb_unplaced_boolean, op, left.id, right.id)
+
+    # -- placement -----------------------------------------------------------
+    def Transformation3D(self, tx=0., ty=0., tz=0., phi=0., theta=0., psi=0.) -> int:
+        return self._id(L.lib().vgb_transformation, tx, ty, tz, phi, theta, psi)
+
+    def Transformation3DMatrix(self, tx, ty, tz, r9) -> int:
+        r = np.ascontiguousarray(r9, np.float64)
+        return self._id(L.lib().vgb_transformation_matrix, tx, ty, tz, r.ctypes.data)
+
+    def LogicalVolume(self, label: str, unplaced: int) -> LogicalVolume:
+        lid = self._id(L.lib().vgb_logical_volume, label.encode(), unplaced)
+        return LogicalVolume(self, lid, label)
+
+    def SetWorld(self, placed: PlacedVolume) -> None:
+        check(L.lib().vgb_set_world(self.handle, placed.id))
+        self.world = placed
+
+    def CloseGeometry(self) -> None:
+        """GeoManager::CloseGeometry + CudaManager upload (one copy per table)."""
+        check(L.lib().vgb_geometry_close(self.handle))
+        self.closed = True
+
+    def getMaxDepth(self) -> int:
+        out = ctypes.c_int32()
+        check(L.lib().vgb_geometry_max_depth(self.handle, ctypes.byref(out)))
+        return out.value
+
+    def device_bytes(self) -> int:
+        out = ctypes.c_int64()
+        check(L.lib().vgb_geometry_device_bytes(self.handle, ctypes.byref(out)))
+        return out.value

@@ -1,0 +1,330 @@
+"""Seeded synthetic workloads for the shape and navigation benchmarks.
+
+Plays the role of the reference's point/direction generators
+(volumes/utilities/VolumeUtilities.h:67-452) with our own, seed-stable
+sampling:
+  * directions are isotropic unit vectors (normalised 3-D Gaussians);
+  * "mixed" point sets are 1/3 uniform inside the shape, 1/3 uniform outside it
+    within a bounding box 1.5x the shape's extent, and 1/3 within +-1e-6 mm of
+    the surface (a boundary crossing between an inside and an outside sample,
+    found by bisection, then moved by U(-1e-6, 1e-6) mm along the segment).
+Each ShapeSpec carries an exact (tolerance-free) numpy containment test used
+only to draw inputs; results are always computed by libvgb.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+from typing import Callable
+
+import numpy as np
+
+SEED_BASE = 0x5EED
+
+
+def isotropic(rng: np.random.Generator, n: int):
+    v = rng.standard_normal((3, n))
+    v /= np.sqrt((v * v).sum(axis=0))
+    return v[0].copy(), v[1].copy(), v[2].copy()
+
+
+@dataclass
+class ShapeSpec:
+    """One unplaced shape: constructor arguments plus sampling helpers."""
+    kind: str                       # box, tube, cone, sphere, torus, polycone, polyhedron, boolsub, trd
+    params: dict
+    half: tuple                     # half extents of the axis-aligned bounding box
+    center: tuple = (0., 0., 0.)
+    contains: Callable = field(default=None, repr=False)
+
+    def bbox_sample(self, rng, n, scale=1.0):
+        h = np.asarray(self.half) * scale
+        c = np.asarray(self.center)
+        u = rng.uniform(-1.0, 1.0, (3, n))
+        return (c[0] + u[0] * h[0], c[1] + u[1] * h[1], c[2] + u[2] * h[2])
+
+
+def _phi_in(phi, sphi, dphi):
+    """phi in [sphi, sphi+dphi] (radians), wrap-aware."""
+    if dphi >= 2 * math.pi - 1e-15:
+        return np.ones_like(phi, dtype=bool)
+    d = np.mod(phi - sphi, 2 * math.pi)
+    return d <= dphi
+
+
+def box_spec(dx, dy, dz) -> ShapeSpec:
+    def contains(x, y, z):
+        return (np.abs(x) <= dx) & (np.abs(y) <= dy) & (np.abs(z) <= dz)
+    return ShapeSpec("box", dict(dx=dx, dy=dy, dz=dz), (dx, dy, dz), contains=contains)
+
+
+def tube_spec(rmin, rmax, dz, sphi, dphi) -> ShapeSpec:
+    def contains(x, y, z):
+        r2 = x * x + y * y
+        ok = (np.abs(z) <= dz) & (r2 <= rmax * rmax) & (r2 >= rmin * rmin)
+        return ok & _phi_in(np.arctan2(y, x), sphi, dphi)
+    return ShapeSpec("tube", dict(rmin=rmin, rmax=rmax, dz=dz, sphi=sphi, dphi=dphi),
+                     (rmax, rmax, dz), contains=contains)
+
+
+def cone_spec(rmin1, rmax1, rmin2, rmax2, dz, sphi, dphi) -> ShapeSpec:
+    def contains(x, y, z):
+        t = (z + dz) / (2 * dz)
+        rlo = rmin1 + (rmin2 - rmin1) * t
+        rhi = rmax1 + (rmax2 - rmax1) * t
+        r = np.sqrt(x * x + y * y)
+        ok = (np.abs(z) <= dz) & (r <= rhi) & (r >= rlo)
+        return ok & _phi_in(np.arctan2(y, x), sphi, dphi)
+    R = max(rmax1, rmax2)
+    return ShapeSpec("cone", dict(rmin1=rmin1, rmax1=rmax1, rmin2=rmin2, rmax2=rmax2, dz=dz,
+                                  sphi=sphi, dphi=dphi), (R, R, dz), contains=contains)
+
+
+def sphere_spec(rmin, rmax, sphi, dphi, stheta, dtheta) -> ShapeSpec:
+    def contains(x, y, z):
+        r2 = x * x + y * y + z * z
+        ok = (r2 <= rmax * rmax) & (r2 >= rmin * rmin)
+        th = np.arctan2(np.sqrt(x * x + y * y), z)
+        ok &= (th >= stheta) & (th <= stheta + dtheta)
+        return ok & _phi_in(np.arctan2(y, x), sphi, dphi)
+    return ShapeSpec("sphere", dict(rmin=rmin, rmax=rmax, sphi=sphi, dphi=dphi, stheta=stheta,
+                                    dtheta=dtheta), (rmax, rmax, rmax), contains=contains)
+
+
+def torus_spec(rmin, rmax, rtor, sphi, dphi) -> ShapeSpec:
+    def contains(x, y, z):
+        rho = np.sqrt(x * x + y * y) - rtor
+        d2 = rho * rho + z * z
+        ok = (d2 <= rmax * rmax) & (d2 >= rmin * rmin)
+        return ok & _phi_in(np.arctan2(y, x), sphi, dphi)
+    R = rtor + rmax
+    return ShapeSpec("torus", dict(rmin=rmin, rmax=rmax, rtor=rtor, sphi=sphi, dphi=dphi),
+                     (R, R, rmax), contains=contains)
+
+
+def trd_spec(dx1, dx2, dy1, dy2, dz) -> ShapeSpec:
+    def contains(x, y, z):
+        t = (z + dz) / (2 * dz)
+        hx = dx1 + (dx2 - dx1) * t
+        hy = dy1 + (dy2 - dy1) * t
+        return (np.abs(z) <= dz) & (np.abs(x) <= hx) & (np.abs(y) <= hy)
+    return ShapeSpec("trd", dict(dx1=dx1, dx2=dx2, dy1=dy1, dy2=dy2, dz=dz),
+                     (max(dx1, dx2), max(dy1, dy2), dz), contains=contains)
+
+
+def polycone_spec(sphi, dphi, z, rmin, rmax) -> ShapeSpec:
+    z = np.asarray(z, float)
+    rmin = np.asarray(rmin, float)
+    rmax = np.asarray(rmax, float)
+
+    def contains(x, y, zz):
+        r = np.sqrt(x * x + y * y)
+        ok = np.zeros(x.shape, bool)
+        for k in range(len(z) - 1):
+            if z[k + 1] == z[k]:
+                continue
+            t = (zz - z[k]) / (z[k + 1] - z[k])
+            insec = (zz >= z[k]) & (zz <= z[k + 1])
+            lo = rmin[k] + (rmin[k + 1] - rmin[k]) * t
+            hi = rmax[k] + (rmax[k + 1] - rmax[k]) * t
+            ok |= insec & (r >= lo) & (r <= hi)
+        return ok & _phi_in(np.arctan2(y, x), sphi, dphi)
+    R = float(rmax.max())
+    zc = 0.5 * (z[0] + z[-1])
+    return ShapeSpec("polycone", dict(sphi=sphi, dphi=dphi, z=z, rmin=rmin, rmax=rmax),
+                     (R, R, 0.5 * (z[-1] - z[0])), center=(0., 0., zc), contains=contains)
+
+
+def polyhedron_spec(phi_start_deg, phi_delta_deg, sides, z, rmin, rmax) -> ShapeSpec:
+    """Polyhedron with rmin/rmax as inner/outer apothems (distance to the side
+    planes), as volumes/UnplacedPolyhedron.h takes them."""
+    z = np.asarray(z, float)
+    rmin = np.asarray(rmin, float)
+    rmax = np.asarray(rmax, float)
+    s0 = math.radians(phi_start_deg)
+    dphi = math.radians(phi_delta_deg if phi_delta_deg > 0 else 360.0)
+    sw = dphi / sides
+
+    def contains(x, y, zz):
+        phi = np.arctan2(y, x)
+        rel = np.mod(phi - s0, 2 * math.pi)
+        inphi = rel <= dphi if dphi < 2 * math.pi - 1e-12 else np.ones_like(rel, bool)
+        k = np.minimum(np.floor(rel / sw), sides - 1)
+        mid = s0 + (k + 0.5) * sw
+        a = x * np.cos(mid) + y * np.sin(mid)   # distance along the side normal
+        ok = np.zeros(x.shape, bool)
+        for j in range(len(z) - 1):
+            if z[j + 1] == z[j]:
+                continue
+            t = (zz - z[j]) / (z[j + 1] - z[j])
+            inseg = (zz >= z[j]) & (zz <= z[j + 1])
+            lo = rmin[j] + (rmin[j + 1] - rmin[j]) * t
+            hi = rmax[j] + (rmax[j + 1] - rmax[j]) * t
+            ok |= inseg & (a >= lo) & (a <= hi)
+        return ok & inphi
+    R = float(rmax.max()) / math.cos(math.pi / sides)
+    zc = 0.5 * (z[0] + z[-1])
+    return ShapeSpec("polyhedron", dict(phi_start_deg=phi_start_deg, phi_delta_deg=phi_delta_deg,
+                                        sides=sides, z=z, rmin=rmin, rmax=rmax),
+                     (R, R, 0.5 * (z[-1] - z[0])), center=(0., 0., zc), contains=contains)
+
+
+def boolsub_spec(box_half, tube_rmax, tube_dz) -> ShapeSpec:
+    """Box minus a full solid tube, both at the origin."""
+    bx, by, bz = box_half
+
+    def contains(x, y, z):
+        inbox = (np.abs(x) <= bx) & (np.abs(y) <= by) & (np.abs(z) <= bz)
+        intube = (x * x + y * y <= tube_rmax * tube_rmax) & (np.abs(z) <= tube_dz)
+        return inbox & ~intube
+    return ShapeSpec("boolsub", dict(box_half=box_half, tube_rmax=tube_rmax, tube_dz=tube_dz),
+                     (bx, by, bz), contains=contains)
+
+
+# ---------------------------------------------------------------------------
+# point sets
+# ---------------------------------------------------------------------------
+
+def _rejection(spec: ShapeSpec, rng, n: int, want_inside: bool, scale: float):
+    xs, ys, zs = [], [], []
+    got = 0
+    while got < n:
+        m = max(1024, 2 * (n - got))
+        x, y, z = spec.bbox_sample(rng, m, scale)
+        c = spec.contains(x, y, z)
+        sel = c if want_inside else ~c
+        xs.append(x[sel]); ys.append(y[sel]); zs.append(z[sel])
+        got += int(sel.sum())
+    return (np.concatenate(xs)[:n], np.concatenate(ys)[:n], np.concatenate(zs)[:n])
+
+
+def _near_surface(spec: ShapeSpec, rng, n: int, eps: float = 1e-6):
+    a = np.stack(_rejection(spec, rng, n, True, 1.0))
+    b = np.stack(_rejection(spec, rng, n, False, 1.5))
+    lo, hi = a.copy(), b.copy()            # contains(lo) True, contains(hi) False
+    for _ in range(64):
+        mid = 0.5 * (lo + hi)
+        c = spec.contains(mid[0], mid[1], mid[2])
+        lo = np.where(c, mid, lo)
+        hi = np.where(c, hi, mid)
+    d = b - a
+    d /= np.sqrt((d * d).sum(axis=0))
+    off = rng.uniform(-eps, eps, n)
+    p = 0.5 * (lo + hi) + d * off
+    return p[0].copy(), p[1].copy(), p[2].copy()
+
+
+def mixed_points(spec: ShapeSpec, n: int, seed: int):
+    """1/3 inside, 1/3 outside in the 1.5x box, 1/3 within 1e-6 mm of the surface,
+    interleaved in a seeded random order."""
+    rng = np.random.default_rng(seed)
+    n1 = n // 3
+    n2 = n // 3
+    n3 = n - n1 - n2
+    parts = [_rejection(spec, rng, n1, True, 1.0), _rejection(spec, rng, n2, False, 1.5),
+             _near_surface(spec, rng, n3)]
+    x = np.concatenate([p[0] for p in parts])
+    y = np.concatenate([p[1] for p in parts])
+    z = np.concatenate([p[2] for p in parts])
+    perm = rng.permutation(n)
+    return x[perm].copy(), y[perm].copy(), z[perm].copy()
+
+
+def uniform_points(spec: ShapeSpec, n: int, seed: int, scale: float = 1.5):
+    rng = np.random.default_rng(seed)
+    return spec.bbox_sample(rng, n, scale)
+
+
+@dataclass
+class ShapeWorkload:
+    spec: ShapeSpec
+    x: np.ndarray
+    y: np.ndarray
+    z: np.ndarray
+    dx: np.ndarray
+    dy: np.ndarray
+    dz: np.ndarray
+    step: np.ndarray
+
+    @property
+    def n(self) -> int:
+        return len(self.x)
+
+
+def make_workload(spec: ShapeSpec, n: int, seed: int, mix: str = "mixed",
+                  step_max: float = 1e30) -> ShapeWorkload:
+    if mix == "mixed":
+        x, y, z = mixed_points(spec, n, seed)
+    else:
+        x, y, z = uniform_points(spec, n, seed)
+    dx, dy, dz = isotropic(np.random.default_rng(seed + 7919), n)
+    return ShapeWorkload(spec, x, y, z, dx, dy, dz, np.full(n, step_max))
+
+
+# ---------------------------------------------------------------------------
+# the named benchmark shapes
+# ---------------------------------------------------------------------------
+
+def config1_box() -> ShapeSpec:
+    """Plain FP64 box, half-lengths (10, 20, 30) mm, unrotated at the origin."""
+    return box_spec(10., 20., 30.)
+
+
+def config2_shapes() -> dict:
+    """Tube, cone, sphere of the FP32+refine vs FP64 comparison."""
+    return {
+        "tube": tube_spec(5., 20., 30., 0., 1.5 * math.pi),
+        "cone": cone_spec(0., 10., 5., 20., 25., 0., 2 * math.pi),
+        "sphere": sphere_spec(10., 30., 0., 2 * math.pi, 0., 0.5 * math.pi),
+    }
+
+
+def config3_shapes(seed: int = SEED_BASE + 3) -> dict:
+    """Torus, polycone, polyhedron and box-minus-tube (compute-heavy shapes).
+    Polycone: 10 z-planes from -100 to 100 mm, rmin ~ U(0,20), rmax ~ U(30,60),
+    phi 0-300 deg.  Polyhedron: 8 sides, 6 z-planes evenly spaced in [-100, 100],
+    rmin 10, rmax 40."""
+    rng = np.random.default_rng(seed)
+    zc = np.linspace(-100., 100., 10)
+    return {
+        "torus": torus_spec(0., 5., 50., 0., 2 * math.pi),
+        "polycone": polycone_spec(0., math.radians(300.), zc, rng.uniform(0., 20., 10),
+                                  rng.uniform(30., 60., 10)),
+        "polyhedron": polyhedron_spec(0., 360., 8, np.linspace(-100., 100., 6),
+                                      np.full(6, 10.), np.full(6, 40.)),
+        "boolsub": boolsub_spec((30., 30., 30.), 15., 40.),
+    }
+
+
+def build_unplaced(geom, spec: ShapeSpec) -> int:
+    """Create spec's unplaced shape in a vecgeom_b200.Geometry; returns its id."""
+    p = spec.params
+    k = spec.kind
+    if k == "box":
+        return geom.UnplacedBox(p["dx"], p["dy"], p["dz"])
+    if k == "tube":
+        return geom.UnplacedTube(p["rmin"], p["rmax"], p["dz"], p["sphi"], p["dphi"])
+    if k == "cone":
+        return geom.UnplacedCone(p["rmin1"], p["rmax1"], p["rmin2"], p["rmax2"], p["dz"],
+                                 p["sphi"], p["dphi"])
+    if k == "sphere":
+        return geom.UnplacedSphere(p["rmin"], p["rmax"], p["sphi"], p["dphi"], p["stheta"],
+                                   p["dtheta"])
+    if k == "torus":
+        return geom.UnplacedTorus(p["rmin"], p["rmax"], p["rtor"], p["sphi"], p["dphi"])
+    if k == "trd":
+        return geom.UnplacedTrd(p["dx1"], p["dx2"], p["dy1"], p["dy2"], p["dz"])
+    if k == "polycone":
+        return geom.UnplacedPolycone(p["sphi"], p["dphi"], p["rmin"], p["rmax"], p["z"])
+    if k == "polyhedron":
+        return geom.UnplacedPolyhedron(p["phi_start_deg"], p["phi_delta_deg"], p["sides"],
+                                       p["z"], p["rmin"], p["rmax"])
+    if k == "boolsub":
+        bx, by, bz = p["box_half"]
+        lb = geom.LogicalVolume("sub_box", geom.UnplacedBox(bx, by, bz))
+        lt = geom.LogicalVolume("sub_tube", geom.UnplacedTube(0., p["tube_rmax"], p["tube_dz"],
+                                                              0., 2 * math.pi))
+        left = lb.Place(geom.Transformation3D())
+        right = lt.Place(geom.Transformation3D())
+        return geom.UnplacedBooleanVolume(2, left, right)
+    raise ValueError(k)
