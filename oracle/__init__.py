@@ -58,8 +58,10 @@ class Oracle:
         if not os.path.exists(ORACLE_SO):
             build(with_ref=False)
         L = ctypes.CDLL(ORACLE_SO)
-        L.or_box.restype = _vp
-        L.or_box.argtypes = [_d, _d, _d]
+        for name, argn in (("or_box", 3), ("or_tube", 5)):
+            f = getattr(L, name)
+            f.restype = _vp
+            f.argtypes = [_d] * argn
         L.or_shape_free.argtypes = [_vp]
         L.or_xform_euler.argtypes = [ctypes.POINTER(Xform)] + [_d] * 6
         L.or_xform_matrix.argtypes = [ctypes.POINTER(Xform), _d, _d, _d, _vp]
@@ -201,6 +203,8 @@ def oracle_unplaced(orc: Oracle, spec):
     k = spec.kind
     if k == "box":
         return orc.shape("box", p["dx"], p["dy"], p["dz"])
+    if k == "tube":
+        return orc.shape("tube", p["rmin"], p["rmax"], p["dz"], p["sphi"], p["dphi"])
     raise NotImplementedError(k)
 
 

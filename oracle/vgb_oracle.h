@@ -73,6 +73,7 @@ void or_transform_dir(const or_xform *x, const double m[3], double l[3]);
  * them (volumes/Unplaced*.h). */
 typedef struct or_shape_s or_shape_t;
 or_shape_t *or_box(double dx, double dy, double dz);
+or_shape_t *or_tube(double rmin, double rmax, double dz, double sphi, double dphi);
 void or_shape_free(or_shape_t *s);
 
 /* Batch call over SOA arrays, the VPlacedVolume SOA3D virtuals

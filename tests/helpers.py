@@ -67,4 +67,8 @@ def shape_specs() -> dict:
     s.update(W.config2_shapes())
     s.update(W.config3_shapes())
     s["trd"] = W.trd_spec(10., 20., 15., 25., 30.)
+    # variants that reach the phi-section and rmin branches
+    s["tubesector"] = W.tube_spec(0., 20., 30., 0.3, 1.0)
+    s["conesector"] = W.cone_spec(2., 10., 5., 20., 25., 0.5, 4.0)
+    s["conesmall"] = W.cone_spec(0., 10., 0., 20., 25., -0.5, 1.2)
     return s

@@ -1,0 +1,59 @@
+// hostcheck.cu -- test infrastructure: the device shape arithmetic of libvgb
+// (vecgeom_b200/csrc/*.cuh, all __host__ __device__) compiled for the host, so
+// the parity tests can check every shape's math against the reference on a
+// machine without a GPU.  The product never loads this library; on a GPU the
+// tests check the real kernels through libvgb.so.
+//
+// Built with -ffp-contract=off, like the FP64 kernels (-fmad=false), so the
+// host results round like the device results (transcendentals aside).
+#include "../../vecgeom_b200/csrc/batch.cuh"
+#include "../../vecgeom_b200/csrc/geometry.h"
+
+using namespace vgb;
+
+namespace {
+
+template <class Ops, class P>
+int run(const P &prm, const DXform &X, int op, int64_t n, const double *x, const double *y,
+        const double *z, const double *dx, const double *dy, const double *dz, const double *st,
+        void *out) {
+  for (int64_t i = 0; i < n; ++i) {
+    const V3<double> m = {x[i], y[i], z[i]};
+    V3<double> d = {0, 0, 0};
+    if (dx) d = {dx[i], dy[i], dz[i]};
+    switch (op) {
+    case VGB_OP_CONTAINS: static_cast<uint8_t *>(out)[i] = Ops::contains(prm, xf_point(X, m)); break;
+    case VGB_OP_INSIDE: static_cast<int32_t *>(out)[i] = Ops::inside(prm, xf_point(X, m)); break;
+    case VGB_OP_DISTANCE_TO_IN:
+      static_cast<double *>(out)[i] = Ops::distance_to_in(prm, xf_point(X, m), xf_dir(X, d), st[i]);
+      break;
+    case VGB_OP_DISTANCE_TO_OUT:
+      static_cast<double *>(out)[i] = Ops::distance_to_out(prm, m, d, st[i]);
+      break;
+    case VGB_OP_SAFETY_TO_IN: static_cast<double *>(out)[i] = Ops::safety_to_in(prm, xf_point(X, m)); break;
+    case VGB_OP_SAFETY_TO_OUT: static_cast<double *>(out)[i] = Ops::safety_to_out(prm, m); break;
+    default: return -1;
+    }
+  }
+  return 0;
+}
+
+}  // namespace
+
+extern "C" int hc_batch(const vgb_geometry *g, int32_t placed, int32_t op, int64_t n,
+                        const double *x, const double *y, const double *z, const double *dx,
+                        const double *dy, const double *dz, const double *st, void *out) {
+  const PlacedRec &pr = g->placed[placed];
+  const DXform &X = g->xforms[pr.xform];
+  const int type = g->unplaced[pr.unplaced].type;
+  const void *prm = shape_params(g, pr.unplaced);
+  switch (type) {
+#define VGB_SHAPE_CASE(TYPE, OPS, P) \
+  case TYPE:                         \
+    return run<OPS<double>>(*static_cast<const P *>(prm), X, op, n, x, y, z, dx, dy, dz, st, out);
+    VGB_FOR_EACH_SHAPE(VGB_SHAPE_CASE)
+#undef VGB_SHAPE_CASE
+  default:
+    return -2;
+  }
+}

@@ -1,0 +1,77 @@
+"""CPU: libvgb's shape arithmetic, compiled for the host, against the reference.
+
+The kernels' per-point functions are __host__ __device__; tests/hostcheck builds
+them for the host (test-only library, never loaded by the product).  These
+tests run the golden cases (reference Scalar outputs) through that build, so
+every shape's math is pinned to the reference before it runs on a GPU.  The
+GPU tests then check the same functions as device code through libvgb.so.
+"""
+import ctypes
+import glob
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from helpers import PLACEMENTS, assert_distances, assert_exact
+from test_oracle_golden import load_case, spec_from_meta
+from vecgeom_b200 import _lib
+from vecgeom_b200 import workloads as W
+from vecgeom_b200.geometry import Geometry
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+SO = os.path.join(ROOT, "_build", "hostcheck", "libvgb_hostcheck.so")
+GOLDEN = sorted(glob.glob(os.path.join(HERE, "golden", "*.npz")))
+HOST_SHAPES = {"box", "tube", "cone"}
+
+
+@pytest.fixture(scope="module")
+def hc():
+    subprocess.run(["make", "-C", os.path.join(HERE, "hostcheck")], check=True,
+                   stdout=subprocess.DEVNULL)
+    L = ctypes.CDLL(SO)
+    for name, (res, args) in _lib.SIGNATURES.items():
+        f = getattr(L, name, None)
+        if f is not None:
+            f.restype = res
+            f.argtypes = args
+    vp = ctypes.c_void_p
+    L.hc_batch.restype = ctypes.c_int
+    L.hc_batch.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int64] + [vp] * 8
+    return L
+
+
+def host_run(L, geom, pv, op, pts, dirs=None, step=None):
+    n = len(pts[0])
+    out = np.zeros(n, {0: np.uint8, 1: np.int32}.get(op, np.float64))
+    p = [np.ascontiguousarray(a) for a in pts]
+    d = [np.ascontiguousarray(a) for a in dirs] if dirs is not None else [None] * 3
+    addr = lambda a: None if a is None else a.ctypes.data  # noqa: E731
+    rc = L.hc_batch(geom.handle, pv.id, op, n, *(addr(a) for a in p), *(addr(a) for a in d),
+                    addr(step), out.ctypes.data)
+    assert rc == 0, f"hc_batch rc={rc}"
+    return out
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p)[:-4] for p in GOLDEN])
+def test_host_build_matches_reference(hc, path):
+    d, meta = load_case(path)
+    if meta["kind"] not in HOST_SHAPES:
+        pytest.skip(f"{meta['kind']} not in this build")
+    spec = spec_from_meta(meta)
+    g = Geometry(library=hc)
+    lv = g.LogicalVolume(spec.kind, W.build_unplaced(g, spec))
+    pv = lv.Place(g.Transformation3D(*PLACEMENTS[str(d["placement"])]))
+    pm = (d["mx"], d["my"], d["mz"])
+    dm = (d["mdx"], d["mdy"], d["mdz"])
+    pl = (d["lx"], d["ly"], d["lz"])
+    dl = (d["ldx"], d["ldy"], d["ldz"])
+    step = np.ascontiguousarray(d["step"])
+    assert_exact(host_run(hc, g, pv, 0, pm), d["contains"], "Contains")
+    assert_exact(host_run(hc, g, pv, 1, pm), d["inside"], "Inside")
+    assert_distances(host_run(hc, g, pv, 4, pm), d["safety_to_in"], "SafetyToIn")
+    assert_distances(host_run(hc, g, pv, 5, pl), d["safety_to_out"], "SafetyToOut")
+    assert_distances(host_run(hc, g, pv, 2, pm, dm, step), d["distance_to_in"], "DistanceToIn")
+    assert_distances(host_run(hc, g, pv, 3, pl, dl, step), d["distance_to_out"], "DistanceToOut")

@@ -18,7 +18,7 @@ from vecgeom_b200 import workloads as W
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 GOLDEN = sorted(glob.glob(os.path.join(HERE, "golden", "*.npz")))
-ORACLE_SHAPES = {"box"}
+ORACLE_SHAPES = {"box", "tube"}
 
 
 def load_case(path):

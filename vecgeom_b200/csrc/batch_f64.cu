@@ -63,8 +63,11 @@ vgb_status launch_batch_f64(const vgb_geometry *g, int32_t placed, int op, const
   const int type = g->unplaced[pr.unplaced].type;
   const void *prm = shape_params(g, pr.unplaced);
   switch (type) {
-  case VGB_SHAPE_BOX:
-    return launch_ops<BoxOps<double>>(*static_cast<const BoxP *>(prm), X, op, io, s);
+#define VGB_SHAPE_CASE(TYPE, OPS, P) \
+  case TYPE:                         \
+    return launch_ops<OPS<double>>(*static_cast<const P *>(prm), X, op, io, s);
+    VGB_FOR_EACH_SHAPE(VGB_SHAPE_CASE)
+#undef VGB_SHAPE_CASE
   default:
     return set_error(VGB_ENOTSUP, "vgb_batch: shape type %d not supported", type);
   }
@@ -77,8 +80,11 @@ vgb_status launch_fused_f64(const vgb_geometry *g, int32_t placed, const FusedIO
   const int type = g->unplaced[pr.unplaced].type;
   const void *prm = shape_params(g, pr.unplaced);
   switch (type) {
-  case VGB_SHAPE_BOX:
-    return launch_fused<BoxOps<double>>(*static_cast<const BoxP *>(prm), X, io, s);
+#define VGB_SHAPE_CASE(TYPE, OPS, P) \
+  case TYPE:                         \
+    return launch_fused<OPS<double>>(*static_cast<const P *>(prm), X, io, s);
+    VGB_FOR_EACH_SHAPE(VGB_SHAPE_CASE)
+#undef VGB_SHAPE_CASE
   default:
     return set_error(VGB_ENOTSUP, "vgb_batch_fused: shape type %d not supported", type);
   }

@@ -92,19 +92,8 @@ static DXform effective(const RawXform &x, bool generic_only) {
 
 using namespace vgb;
 
-#define VGB_CHECK_G(g)                                                          \
-  do {                                                                          \
-    if (!(g)) return set_error(VGB_EINVAL, "%s: geometry is NULL", __func__);   \
-  } while (0)
-#define VGB_CHECK_OPEN(g)                                                       \
-  do {                                                                          \
-    VGB_CHECK_G(g);                                                             \
-    if ((g)->closed)                                                            \
-      return set_error(VGB_EINVAL, "%s: geometry is closed", __func__);         \
-  } while (0)
-
-static vgb_status add_unplaced(vgb_geometry *g, int type, const void *rec, size_t bytes,
-                               int32_t extra, int32_t *id) {
+vgb_status vgb::add_unplaced(vgb_geometry *g, int type, const void *rec, size_t bytes,
+                             int32_t extra, int32_t *id) {
   // 16-byte aligned records in the pool
   while (g->params.size() % 2) g->params.push_back(0.);
   const size_t nd = (bytes + sizeof(double) - 1) / sizeof(double);
@@ -179,17 +168,6 @@ vgb_status vgb_geometry_destroy(vgb_geometry *g) {
   }
   delete g;
   return VGB_OK;
-}
-
-vgb_status vgb_unplaced_box(vgb_geometry *g, double dx, double dy, double dz, int32_t *id) {
-  VGB_CHECK_OPEN(g);
-  if (!(dx > 0 && dy > 0 && dz > 0))
-    return set_error(VGB_EINVAL, "vgb_unplaced_box: half-lengths must be > 0");
-  BoxP b;
-  b.d[0] = dx;
-  b.d[1] = dy;
-  b.d[2] = dz;
-  return add_unplaced(g, VGB_SHAPE_BOX, &b, sizeof(b), 0, id);
 }
 
 vgb_status vgb_transformation(vgb_geometry *g, double tx, double ty, double tz, double phi,
@@ -353,38 +331,3 @@ vgb_status finalize_shapes(vgb_geometry *g) {
 }
 }  // namespace vgb
 
-// ---------------------------------------------------------------------------
-// shapes not yet uploaded by this build report VGB_ENOTSUP
-// ---------------------------------------------------------------------------
-extern "C" {
-#define VGB_NOTYET(name) return set_error(VGB_ENOTSUP, name ": shape not available yet")
-vgb_status vgb_unplaced_tube(vgb_geometry *, double, double, double, double, double, int32_t *) {
-  VGB_NOTYET("vgb_unplaced_tube");
-}
-vgb_status vgb_unplaced_cone(vgb_geometry *, double, double, double, double, double, double,
-                             double, int32_t *) {
-  VGB_NOTYET("vgb_unplaced_cone");
-}
-vgb_status vgb_unplaced_sphere(vgb_geometry *, double, double, double, double, double, double,
-                               int32_t *) {
-  VGB_NOTYET("vgb_unplaced_sphere");
-}
-vgb_status vgb_unplaced_torus(vgb_geometry *, double, double, double, double, double, int32_t *) {
-  VGB_NOTYET("vgb_unplaced_torus");
-}
-vgb_status vgb_unplaced_polycone(vgb_geometry *, double, double, int32_t, const double *,
-                                 const double *, const double *, int32_t *) {
-  VGB_NOTYET("vgb_unplaced_polycone");
-}
-vgb_status vgb_unplaced_polyhedron(vgb_geometry *, double, double, int32_t, int32_t,
-                                   const double *, const double *, const double *, int32_t *) {
-  VGB_NOTYET("vgb_unplaced_polyhedron");
-}
-vgb_status vgb_unplaced_trd(vgb_geometry *, double, double, double, double, double, int32_t *) {
-  VGB_NOTYET("vgb_unplaced_trd");
-}
-vgb_status vgb_unplaced_boolean(vgb_geometry *, int32_t, int32_t, int32_t, int32_t *) {
-  VGB_NOTYET("vgb_unplaced_boolean");
-}
-#undef VGB_NOTYET
-}

@@ -90,6 +90,9 @@ namespace vgb {
 vgb_status set_error(vgb_status s, const char *fmt, ...);
 vgb_status cuda_error(cudaError_t e, const char *what);
 void count_launch(int n = 1);
+// Appends a shape record to the parameter pool (16-byte aligned).
+vgb_status add_unplaced(vgb_geometry *g, int type, const void *rec, size_t bytes, int32_t extra,
+                        int32_t *id);
 
 // The host copy of a shape's parameter record (for passing by value).
 inline const void *shape_params(const vgb_geometry *g, int32_t unplaced) {
@@ -100,3 +103,14 @@ inline const double *shape_params_dev(const vgb_geometry *g, int32_t unplaced) {
   return g->dev.params + g->unplaced[unplaced].param_off;
 }
 }  // namespace vgb
+
+#define VGB_CHECK_G(g)                                                          \
+  do {                                                                          \
+    if (!(g)) return vgb::set_error(VGB_EINVAL, "%s: geometry is NULL", __func__);   \
+  } while (0)
+#define VGB_CHECK_OPEN(g)                                                       \
+  do {                                                                          \
+    VGB_CHECK_G(g);                                                             \
+    if ((g)->closed)                                                            \
+      return vgb::set_error(VGB_EINVAL, "%s: geometry is closed", __func__);         \
+  } while (0)

@@ -2,8 +2,16 @@
 #pragma once
 #include "../../include/vgb.h"
 #include "box.cuh"
+#include "tube.cuh"
+#include "cone.cuh"
 
 struct vgb_geometry;
+
+// (type, ops template, parameter record) of every shape with batch kernels
+#define VGB_FOR_EACH_SHAPE(X)            \
+  X(VGB_SHAPE_BOX, vgb::BoxOps, vgb::BoxP) \
+  X(VGB_SHAPE_TUBE, vgb::TubeOps, vgb::TubeP) \
+  X(VGB_SHAPE_CONE, vgb::ConeOps, vgb::ConeP)
 
 namespace vgb {
 // Called by vgb_geometry_close() once the device parameter pool is allocated:

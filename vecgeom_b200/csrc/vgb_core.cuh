@@ -46,6 +46,12 @@ template <> struct Lim<float> {
   static VGB_HD float minimum() { return FLT_MIN; }
 };
 
+// Min/Max of the reference Scalar backend (backend/scalar/Backend.h:146-163) are
+// std::min/std::max: min(a,b) = b < a ? b : a, max(a,b) = a < b ? b : a.  The
+// same selects keep NaN and signed-zero results identical.
+template <class R> VGB_HD R vmin(R a, R b) { return b < a ? b : a; }
+template <class R> VGB_HD R vmax(R a, R b) { return a < b ? b : a; }
+
 template <class R> struct V3 {
   R x, y, z;
   VGB_HD R operator[](int i) const { return i == 0 ? x : (i == 1 ? y : z); }

@@ -83,12 +83,12 @@ class LogicalVolume:
 
     def Place(self, transformation: int) -> "PlacedVolume":
         out = ctypes.c_int32()
-        check(L.lib().vgb_place(self.geometry.handle, self.id, transformation, ctypes.byref(out)))
+        check(self.geometry.L.vgb_place(self.geometry.handle, self.id, transformation, ctypes.byref(out)))
         return PlacedVolume(self.geometry, out.value, self)
 
     def PlaceDaughter(self, daughter: "LogicalVolume", transformation: int) -> "PlacedVolume":
         out = ctypes.c_int32()
-        check(L.lib().vgb_place_daughter(self.geometry.handle, self.id, daughter.id,
+        check(self.geometry.L.vgb_place_daughter(self.geometry.handle, self.id, daughter.id,
                                          transformation, ctypes.byref(out)))
         return PlacedVolume(self.geometry, out.value, daughter)
 
@@ -116,7 +116,7 @@ class PlacedVolume:
         _check_dtype(aux, "i4")
         d = dirs
         s = stream.cuda_stream if hasattr(stream, "cuda_stream") else stream
-        check(L.lib().vgb_batch(
+        check(g.L.vgb_batch(
             g.handle, self.id, op, n, _addr(points.x), _addr(points.y), _addr(points.z),
             _addr(d.x) if d else None, _addr(d.y) if d else None, _addr(d.z) if d else None,
             _addr(step_max), _addr(out), _addr(aux), daughter, precision, s))
@@ -180,7 +180,7 @@ class PlacedVolume:
             arr[k] = _addr(v)
         d = dirs
         s = stream.cuda_stream if hasattr(stream, "cuda_stream") else stream
-        check(L.lib().vgb_batch_fused(
+        check(g.L.vgb_batch_fused(
             g.handle, self.id, ops, points.size(), _addr(points.x), _addr(points.y),
             _addr(points.z), _addr(d.x) if d else None, _addr(d.y) if d else None,
             _addr(d.z) if d else None, _addr(step_max), arr,
@@ -190,17 +190,20 @@ class PlacedVolume:
 class Geometry:
     """A geometry under construction, then closed and resident on the device."""
 
-    def __init__(self):
+    def __init__(self, library=None):
+        # library: an already configured ctypes handle exposing the vgb_* ABI
+        # (defaults to libvgb.so)
+        self.L = library if library is not None else L.lib()
         h = ctypes.c_void_p()
-        check(L.lib().vgb_geometry_create(ctypes.byref(h)))
+        check(self.L.vgb_geometry_create(ctypes.byref(h)))
         self.handle = h
         self.closed = False
         self.world: PlacedVolume | None = None
 
     def __del__(self):
         h = getattr(self, "handle", None)
-        if h is not None and L._lib is not None:
-            L._lib.vgb_geometry_destroy(h)
+        if h is not None and getattr(self, "L", None) is not None:
+            self.L.vgb_geometry_destroy(h)
             self.handle = None
 
     def _id(self, fn, *args) -> int:
@@ -214,63 +217,63 @@ class Geometry:
 
     # -- unplaced shapes (volumes/Unplaced*.h) --------------------------------
     def UnplacedBox(self, dx, dy, dz) -> int:
-        return self._id(L.lib().vgb_unplaced_box, dx, dy, dz)
+        return self._id(self.L.vgb_unplaced_box, dx, dy, dz)
 
     def UnplacedTube(self, rmin, rmax, dz, sphi, dphi) -> int:
-        return self._id(L.lib().vgb_unplaced_tube, rmin, rmax, dz, sphi, dphi)
+        return self._id(self.L.vgb_unplaced_tube, rmin, rmax, dz, sphi, dphi)
 
     def UnplacedCone(self, rmin1, rmax1, rmin2, rmax2, dz, sphi, dphi) -> int:
-        return self._id(L.lib().vgb_unplaced_cone, rmin1, rmax1, rmin2, rmax2, dz, sphi, dphi)
+        return self._id(self.L.vgb_unplaced_cone, rmin1, rmax1, rmin2, rmax2, dz, sphi, dphi)
 
     def UnplacedSphere(self, rmin, rmax, sphi, dphi, stheta, dtheta) -> int:
-        return self._id(L.lib().vgb_unplaced_sphere, rmin, rmax, sphi, dphi, stheta, dtheta)
+        return self._id(self.L.vgb_unplaced_sphere, rmin, rmax, sphi, dphi, stheta, dtheta)
 
     def UnplacedTorus(self, rmin, rmax, rtor, sphi, dphi) -> int:
-        return self._id(L.lib().vgb_unplaced_torus, rmin, rmax, rtor, sphi, dphi)
+        return self._id(self.L.vgb_unplaced_torus, rmin, rmax, rtor, sphi, dphi)
 
     def UnplacedPolycone(self, sphi, dphi, rmin, rmax, z) -> int:
         rmin, rmax, z = (np.ascontiguousarray(a, np.float64) for a in (rmin, rmax, z))
-        return self._id(L.lib().vgb_unplaced_polycone, sphi, dphi, len(z), rmin.ctypes.data,
+        return self._id(self.L.vgb_unplaced_polycone, sphi, dphi, len(z), rmin.ctypes.data,
                         rmax.ctypes.data, z.ctypes.data)
 
     def UnplacedPolyhedron(self, phi_start_deg, phi_delta_deg, sides, z, rmin, rmax) -> int:
         rmin, rmax, z = (np.ascontiguousarray(a, np.float64) for a in (rmin, rmax, z))
-        return self._id(L.lib().vgb_unplaced_polyhedron, phi_start_deg, phi_delta_deg, sides,
+        return self._id(self.L.vgb_unplaced_polyhedron, phi_start_deg, phi_delta_deg, sides,
                         len(z), z.ctypes.data, rmin.ctypes.data, rmax.ctypes.data)
 
     def UnplacedTrd(self, dx1, dx2, dy1, dy2, dz) -> int:
-        return self._id(L.lib().vgb_unplaced_trd, dx1, dx2, dy1, dy2, dz)
+        return self._id(self.L.vgb_unplaced_trd, dx1, dx2, dy1, dy2, dz)
 
     def UnplacedBooleanVolume(self, op: int, left: PlacedVolume, right: PlacedVolume) -> int:
-        return self._id(L.lib().vgb_unplaced_boolean, op, left.id, right.id)
+        return self._id(self.L.vgb_unplaced_boolean, op, left.id, right.id)
 
     # -- placement -----------------------------------------------------------
     def Transformation3D(self, tx=0., ty=0., tz=0., phi=0., theta=0., psi=0.) -> int:
-        return self._id(L.lib().vgb_transformation, tx, ty, tz, phi, theta, psi)
+        return self._id(self.L.vgb_transformation, tx, ty, tz, phi, theta, psi)
 
     def Transformation3DMatrix(self, tx, ty, tz, r9) -> int:
         r = np.ascontiguousarray(r9, np.float64)
-        return self._id(L.lib().vgb_transformation_matrix, tx, ty, tz, r.ctypes.data)
+        return self._id(self.L.vgb_transformation_matrix, tx, ty, tz, r.ctypes.data)
 
     def LogicalVolume(self, label: str, unplaced: int) -> LogicalVolume:
-        lid = self._id(L.lib().vgb_logical_volume, label.encode(), unplaced)
+        lid = self._id(self.L.vgb_logical_volume, label.encode(), unplaced)
         return LogicalVolume(self, lid, label)
 
     def SetWorld(self, placed: PlacedVolume) -> None:
-        check(L.lib().vgb_set_world(self.handle, placed.id))
+        check(self.L.vgb_set_world(self.handle, placed.id))
         self.world = placed
 
     def CloseGeometry(self) -> None:
         """GeoManager::CloseGeometry + CudaManager upload (one copy per table)."""
-        check(L.lib().vgb_geometry_close(self.handle))
+        check(self.L.vgb_geometry_close(self.handle))
         self.closed = True
 
     def getMaxDepth(self) -> int:
         out = ctypes.c_int32()
-        check(L.lib().vgb_geometry_max_depth(self.handle, ctypes.byref(out)))
+        check(self.L.vgb_geometry_max_depth(self.handle, ctypes.byref(out)))
         return out.value
 
     def device_bytes(self) -> int:
         out = ctypes.c_int64()
-        check(L.lib().vgb_geometry_device_bytes(self.handle, ctypes.byref(out)))
+        check(self.L.vgb_geometry_device_bytes(self.handle, ctypes.byref(out)))
         return out.value
