@@ -137,13 +137,43 @@ class RefLib:
         L.vgref_nav_trace.argtypes = [_i64] + [_vp] * 6 + [_d, _i] + [_vp] * 4 + [_i]
         L.vgref_locate.restype = _i
         L.vgref_locate.argtypes = [_d, _d, _d, _vp]
+        L.vgref_usphere_distance_to_in.restype = _i
+        L.vgref_usphere_distance_to_in.argtypes = [_d] * 6 + [_vp, _i64] + [_vp] * 7
         self.L = L
         self._keep = []
+        self.last_transform = None
 
     def placed(self, unplaced, tx=0., ty=0., tz=0., phi=0., theta=0., psi=0., label="v"):
         t = self.L.vgref_transform_euler(tx, ty, tz, phi, theta, psi)
+        self.last_transform = t
         lv = self.L.vgref_logical(label.encode(), unplaced)
         return self.L.vgref_place(lv, t)
+
+    def usphere_distance_to_in(self, p: dict, transform, pts, dirs, nthreads: int = 1):
+        """USolids USphere::DistanceToIn (USolids/src/USphere.cc:630), the
+        in-tree definition of the sphere DistanceToIn the reference stubs out."""
+        import threading
+        x, y, z = (np.ascontiguousarray(a, np.float64) for a in pts)
+        dx, dy, dz = (np.ascontiguousarray(a, np.float64) for a in dirs)
+        n = len(x)
+        out = np.zeros(n, np.float64)
+        args = (p["rmin"], p["rmax"], p["sphi"], p["dphi"], p["stheta"], p["dtheta"], transform)
+
+        def run(b, e):
+            self.L.vgref_usphere_distance_to_in(*args, e - b, x[b:].ctypes.data, y[b:].ctypes.data,
+                                                z[b:].ctypes.data, dx[b:].ctypes.data,
+                                                dy[b:].ctypes.data, dz[b:].ctypes.data,
+                                                out[b:].ctypes.data)
+        if nthreads <= 1 or n < 4096:
+            run(0, n)
+        else:
+            ch = (n + nthreads - 1) // nthreads
+            ts = [threading.Thread(target=run, args=(b, min(n, b + ch))) for b in range(0, n, ch)]
+            for t in ts:
+                t.start()
+            for t in ts:
+                t.join()
+        return out
 
     def batch(self, placed, op: int, pts, dirs=None, step=None, nthreads: int = 1,
               out=None, aux=None, daughter: int = 0) -> np.ndarray:

@@ -71,6 +71,12 @@ def make_case(ref, name: str, spec, placement: str, seed: int) -> dict:
         use_dir = op in (oracle.DISTANCE_TO_IN, oracle.DISTANCE_TO_OUT)
         out[opname] = ref.batch(pv, op, pts, dirs if use_dir else None,
                                 wl.step if use_dir else None)
+    if spec.kind == "sphere":
+        # the reference's sphere DistanceToIn is a stub returning kInfinity
+        # (volumes/kernel/SphereImplementation.h:84-93); pin it to USolids'
+        # USphere::DistanceToIn (USolids/src/USphere.cc:630) instead
+        out["distance_to_in_vecgeom_stub"] = out["distance_to_in"]
+        out["distance_to_in"] = ref.usphere_distance_to_in(spec.params, t, pts_m, dirs_m)
     return out
 
 

@@ -29,9 +29,10 @@ def distances_match(a: np.ndarray, b: np.ndarray) -> np.ndarray:
     b = np.asarray(b, np.float64)
     both_nan = np.isnan(a) & np.isnan(b)
     same_inf = np.isinf(a) & np.isinf(b) & (np.sign(a) == np.sign(b))
+    finite = np.isfinite(a) & np.isfinite(b)
     with np.errstate(invalid="ignore"):
         d = np.abs(a - b)
-        ok = (d <= ABS_TOL) | (d <= REL_TOL * np.abs(b))
+        ok = finite & ((d <= ABS_TOL) | (d <= REL_TOL * np.abs(b)))
     return ok | both_nan | same_inf
 
 
@@ -71,4 +72,6 @@ def shape_specs() -> dict:
     s["tubesector"] = W.tube_spec(0., 20., 30., 0.3, 1.0)
     s["conesector"] = W.cone_spec(2., 10., 5., 20., 25., 0.5, 4.0)
     s["conesmall"] = W.cone_spec(0., 10., 0., 20., 25., -0.5, 1.2)
+    s["spheresector"] = W.sphere_spec(5., 30., 0.3, 4.0, 0.4, 1.9)
+    s["spherefull"] = W.sphere_spec(0., 25., 0., 2 * math.pi, 0., math.pi)
     return s

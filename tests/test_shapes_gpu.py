@@ -133,6 +133,9 @@ def reference_outputs(spec, placement, pts, dirs, step):
     want["safety_to_in"] = call(oracle.SAFETY_TO_IN, pts)
     want["safety_to_out"] = call(oracle.SAFETY_TO_OUT, pts)
     want["distance_to_in"] = call(oracle.DISTANCE_TO_IN, pts, dirs, step)
+    if spec.kind == "sphere" and oracle.RefLib.available():
+        want["distance_to_in"] = ref.usphere_distance_to_in(spec.params, ref.last_transform, pts,
+                                                            dirs)
     want["distance_to_out"] = call(oracle.DISTANCE_TO_OUT, pts, dirs, step)
     return want
 

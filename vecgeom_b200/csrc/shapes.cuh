@@ -4,6 +4,7 @@
 #include "box.cuh"
 #include "tube.cuh"
 #include "cone.cuh"
+#include "sphere.cuh"
 
 struct vgb_geometry;
 
@@ -11,7 +12,8 @@ struct vgb_geometry;
 #define VGB_FOR_EACH_SHAPE(X)            \
   X(VGB_SHAPE_BOX, vgb::BoxOps, vgb::BoxP) \
   X(VGB_SHAPE_TUBE, vgb::TubeOps, vgb::TubeP) \
-  X(VGB_SHAPE_CONE, vgb::ConeOps, vgb::ConeP)
+  X(VGB_SHAPE_CONE, vgb::ConeOps, vgb::ConeP) \
+  X(VGB_SHAPE_SPHERE, vgb::SphereOps, vgb::SphereP)
 
 namespace vgb {
 // Called by vgb_geometry_close() once the device parameter pool is allocated:

@@ -3,6 +3,7 @@
 // Each computes the shape's cached values with the reference constructor's
 // formulas (host code, -ffp-contract=off, glibc cos/sin as in the reference),
 // so the device kernels see bit-identical constants.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 
@@ -103,9 +104,92 @@ ConeP make_cone(double rmin1, double rmax1, double rmin2, double rmax2, double d
   return c;
 }
 
+// UnplacedSphere constructor (source/UnplacedSphere.cpp:24-95 with
+// CheckPhiAngles/CheckThetaAngles, volumes/UnplacedSphere.h:56-210); USphere
+// (USolids/src/USphere.cc:30-55) computes the same values.
+SphereP make_sphere(double rmin, double rmax, double sphi, double dphi, double stheta,
+                    double dtheta) {
+  SphereP s;
+  std::memset(&s, 0, sizeof(s));
+  const double kAngTol = 1e-9, kRadTol = 1e-9, fEpsilon = 2.e-11;
+  s.rmin = rmin;
+  s.rmax = rmax;
+  s.rminTolerance = (rmin != 0) ? std::max(kRadTol, fEpsilon * rmin) : 0;
+  s.mkTolerance = std::max(kRadTol, fEpsilon * rmax);
+  bool fullPhi = true, fullTheta = true, full = true;
+  // CheckPhiAngles -> CheckDPhiAngle, CheckSPhiAngle
+  double fSPhi = 0, fDPhi = 0;
+  if (dphi >= 2 * kPi - kAngTol * 0.5) {
+    fDPhi = 2 * kPi;
+    fSPhi = 0;
+  } else {
+    fullPhi = false;
+    if (dphi > 0) fDPhi = dphi;
+  }
+  if (!fullPhi) {
+    if (sphi < 0)
+      fSPhi = 2 * kPi - std::fmod(std::fabs(sphi), 2 * kPi);
+    else
+      fSPhi = std::fmod(sphi, 2 * kPi);
+    if (fSPhi + fDPhi > 2 * kPi) fSPhi -= 2 * kPi;
+  }
+  full = fullPhi && fullTheta;
+  s.sphi = fSPhi;
+  s.dphi = fDPhi;
+  s.hDPhi = 0.5 * fDPhi;
+  s.cPhi = fSPhi + s.hDPhi;
+  s.ePhi = fSPhi + fDPhi;
+  s.sinCPhi = std::sin(s.cPhi);
+  s.cosCPhi = std::cos(s.cPhi);
+  s.cosHDPhiIT = std::cos(s.hDPhi - 0.5 * kAngTol);
+  s.cosHDPhiOT = std::cos(s.hDPhi + 0.5 * kAngTol);
+  s.sinSPhi = std::sin(fSPhi);
+  s.cosSPhi = std::cos(fSPhi);
+  s.sinEPhi = std::sin(s.ePhi);
+  s.cosEPhi = std::cos(s.ePhi);
+  // CheckThetaAngles
+  double fSTheta = 0, fDTheta = 0;
+  if (!((stheta < 0) || (stheta > kPi))) fSTheta = stheta;
+  if (dtheta + stheta >= kPi)
+    fDTheta = kPi - stheta;
+  else if (dtheta > 0)
+    fDTheta = dtheta;
+  fullTheta = !(fDTheta - fSTheta < kPi);
+  full = fullPhi && fullTheta;
+  s.stheta = fSTheta;
+  s.dtheta = fDTheta;
+  s.eTheta = fSTheta + fDTheta;
+  s.sinSTheta = std::sin(fSTheta);
+  s.cosSTheta = std::cos(fSTheta);
+  s.sinETheta = std::sin(s.eTheta);
+  s.cosETheta = std::cos(s.eTheta);
+  const double tanS = std::tan(fSTheta), tanE = std::tan(s.eTheta);
+  s.tanSTheta2 = tanS * tanS;
+  s.tanETheta2 = tanE * tanE;
+  // evaluated per point by the reference kernels; constant per shape
+  s.cosHDPhi = std::cos(s.hDPhi);
+  const double phim = 0.5 * (fSPhi + s.ePhi);
+  s.sinPhim = std::sin(phim);
+  s.cosPhim = std::cos(phim);
+  s.fullPhi = fullPhi;
+  s.fullTheta = fullTheta;
+  s.full = full;
+  return s;
+}
+
 }  // namespace vgb
 
 extern "C" {
+
+vgb_status vgb_unplaced_sphere(vgb_geometry *g, double rmin, double rmax, double sphi,
+                               double dphi, double stheta, double dtheta, int32_t *id) {
+  VGB_CHECK_OPEN(g);
+  if (!(rmin >= 0 && rmax > rmin && rmax >= 1.1 * kRadTolerance && dphi > 0 && dtheta > 0 &&
+        stheta >= 0 && stheta <= kPi))
+    return set_error(VGB_EINVAL, "vgb_unplaced_sphere: invalid radii or angles");
+  SphereP s = make_sphere(rmin, rmax, sphi, dphi, stheta, dtheta);
+  return add_unplaced(g, VGB_SHAPE_SPHERE, &s, sizeof(s), 0, id);
+}
 
 vgb_status vgb_unplaced_cone(vgb_geometry *g, double rmin1, double rmax1, double rmin2,
                              double rmax2, double dz, double sphi, double dphi, int32_t *id) {
@@ -140,10 +224,6 @@ vgb_status vgb_unplaced_tube(vgb_geometry *g, double rmin, double rmax, double d
 // shapes not yet uploaded by this build report VGB_ENOTSUP
 // ---------------------------------------------------------------------------
 #define VGB_NOTYET(name) return set_error(VGB_ENOTSUP, name ": shape not available yet")
-vgb_status vgb_unplaced_sphere(vgb_geometry *, double, double, double, double, double, double,
-                               int32_t *) {
-  VGB_NOTYET("vgb_unplaced_sphere");
-}
 vgb_status vgb_unplaced_torus(vgb_geometry *, double, double, double, double, double, int32_t *) {
   VGB_NOTYET("vgb_unplaced_torus");
 }
