@@ -52,6 +52,7 @@ def parse():
     ap.add_argument("--n", type=int, default=0, help="points per shape (0 = workload default)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--shapes", default="", help="comma list restricting the workload's shapes")
     return ap.parse_args()
 
 
@@ -77,56 +78,59 @@ def workload_desc(name, n, precision):
 # ---------------------------------------------------------------------------
 
 class ClockSampler:
-    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    """Samples SM clock and clock-event (throttle) reasons through NVML every
+    few milliseconds while running (reads only; changes no GPU setting)."""
 
-    def __init__(self, index: int):
+    REASONS = {"hw_slowdown": "nvmlClocksEventReasonHwSlowdown",
+               "hw_thermal_slowdown": "nvmlClocksEventReasonHwThermalSlowdown",
+               "sw_thermal_slowdown": "nvmlClocksEventReasonSwThermalSlowdown",
+               "sw_power_cap": "nvmlClocksEventReasonSwPowerCap",
+               "hw_power_brake": "nvmlClocksEventReasonHwPowerBrakeSlowdown"}
+
+    def __init__(self, index: int, period_s: float = 0.005):
         self.index = index
-        self.proc = None
-        self.lines = []
+        self.period = period_s
+        self.samples = []
+        self.reasons = set()
+        self.max_mhz = None
+        self._stop = threading.Event()
+        self._thread = None
+        self.err = None
 
     def start(self):
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.QUERY}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
-                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.thread = threading.Thread(target=self._read, daemon=True)
-            self.thread.start()
-        except (OSError, FileNotFoundError):
-            self.proc = None
+            import pynvml as N
+            N.nvmlInit()
+            h = N.nvmlDeviceGetHandleByIndex(self.index)
+            self.max_mhz = float(N.nvmlDeviceGetMaxClockInfo(h, N.NVML_CLOCK_SM))
+        except Exception as e:  # noqa: BLE001
+            self.err = f"nvml unavailable: {e}"
+            return
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
+        def loop():
+            while not self._stop.is_set():
+                try:
+                    self.samples.append(float(N.nvmlDeviceGetClockInfo(h, N.NVML_CLOCK_SM)))
+                    r = N.nvmlDeviceGetCurrentClocksEventReasons(h)
+                    for name, attr in self.REASONS.items():
+                        if r & getattr(N, attr, 0):
+                            self.reasons.add(name)
+                except Exception as e:  # noqa: BLE001
+                    self.err = str(e)
+                    return
+                time.sleep(self.period)
+        self._thread = threading.Thread(target=loop, daemon=True)
+        self._thread.start()
 
     def stop(self) -> dict:
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
-        self.thread.join(timeout=2)
-        sm, smax, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            f = [x.strip() for x in ln.split(",")]
-            if len(f) < 9:
-                continue
-            try:
-                sm.append(float(f[1]))
-                smax.append(float(f[2]))
-            except ValueError:
-                continue
-            for nm, v in zip(names, f[5:9]):
-                if v.lower() == "active":
-                    reasons.add(nm)
-        return {"sm_mhz": float(np.median(sm)) if sm else None,
-                "sm_max_mhz": float(max(smax)) if smax else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        self._stop.set()
+        if self._thread is not None:
+            self._thread.join(timeout=2)
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz,
+                    "reasons": [self.err or "no samples"], "samples": 0}
+        return {"sm_mhz": float(np.median(self.samples)), "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(self.reasons), "samples": len(self.samples)}
 
 
 # ---------------------------------------------------------------------------
@@ -156,7 +160,13 @@ def cpu_rate(shapes: dict, n_total: int, seed: int, budget_s: float = 12.0) -> d
         dirs = (wl.dx, wl.dy, wl.dz)
         if use_ref:
             pv = ref.placed(ref_unplaced(ref, spec))
-            run = lambda op, p, d, s: ref.batch(pv, op, p, d, s, nthreads=threads)  # noqa
+            tr = ref.last_transform
+
+            def run(op, p, d, s, pv=pv, tr=tr, spec=spec):
+                if spec.kind == "sphere" and op == oracle.DISTANCE_TO_IN:
+                    # the reference's sphere DistanceToIn is a stub; time USolids'
+                    return ref.usphere_distance_to_in(spec.params, tr, p, d, nthreads=threads)
+                return ref.batch(pv, op, p, d, s, nthreads=threads)
         else:
             sh = oracle_unplaced(orc, spec)
             xf = orc.xform()
@@ -239,6 +249,9 @@ def main():
     prec = V.PREC_FP64 if args.precision == "fp64" else V.PREC_FP32_REFINE
 
     shapes, n, mix = workload_shapes(args.workload)
+    if args.shapes:
+        keep = set(args.shapes.split(","))
+        shapes = {k: v for k, v in shapes.items() if k in keep}
     if args.n:
         n = args.n
     stream = torch.cuda.current_stream()
