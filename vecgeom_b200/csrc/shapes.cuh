@@ -5,6 +5,7 @@
 #include "tube.cuh"
 #include "cone.cuh"
 #include "sphere.cuh"
+#include "trd.cuh"
 
 struct vgb_geometry;
 
@@ -13,7 +14,8 @@ struct vgb_geometry;
   X(VGB_SHAPE_BOX, vgb::BoxOps, vgb::BoxP) \
   X(VGB_SHAPE_TUBE, vgb::TubeOps, vgb::TubeP) \
   X(VGB_SHAPE_CONE, vgb::ConeOps, vgb::ConeP) \
-  X(VGB_SHAPE_SPHERE, vgb::SphereOps, vgb::SphereP)
+  X(VGB_SHAPE_SPHERE, vgb::SphereOps, vgb::SphereP) \
+  X(VGB_SHAPE_TRD, vgb::TrdOps, vgb::TrdP)
 
 namespace vgb {
 // Called by vgb_geometry_close() once the device parameter pool is allocated:

@@ -177,9 +177,41 @@ SphereP make_sphere(double rmin, double rmax, double sphi, double dphi, double s
   return s;
 }
 
+// UnplacedTrd::calculateCached (volumes/UnplacedTrd.h:38-51)
+TrdP make_trd(double dx1, double dx2, double dy1, double dy2, double dz) {
+  TrdP t;
+  std::memset(&t, 0, sizeof(t));
+  t.dx1 = dx1;
+  t.dx2 = dx2;
+  t.dy1 = dy1;
+  t.dy2 = dy2;
+  t.dz = dz;
+  t.x2minusx1 = dx2 - dx1;
+  t.y2minusy1 = dy2 - dy1;
+  t.halfx1plusx2 = 0.5 * (dx1 + dx2);
+  t.halfy1plusy2 = 0.5 * (dy1 + dy2);
+  t.dztimes2 = dz * 2;
+  t.fx = 0.5 * (dx1 - dx2) / dz;
+  t.fy = 0.5 * (dy1 - dy2) / dz;
+  t.calfx = 1. / std::sqrt(1.0 + t.fx * t.fx);
+  t.calfy = 1. / std::sqrt(1.0 + t.fy * t.fy);
+  t.varying_y = dy1 != dy2;
+  return t;
+}
+
 }  // namespace vgb
 
 extern "C" {
+
+vgb_status vgb_unplaced_trd(vgb_geometry *g, double dx1, double dx2, double dy1, double dy2,
+                            double dz, int32_t *id) {
+  VGB_CHECK_OPEN(g);
+  if (!(dx1 >= 0 && dx2 >= 0 && dy1 >= 0 && dy2 >= 0 && dz > 0 && (dx1 > 0 || dx2 > 0) &&
+        (dy1 > 0 || dy2 > 0)))
+    return set_error(VGB_EINVAL, "vgb_unplaced_trd: invalid half-lengths");
+  TrdP t = make_trd(dx1, dx2, dy1, dy2, dz);
+  return add_unplaced(g, VGB_SHAPE_TRD, &t, sizeof(t), 0, id);
+}
 
 vgb_status vgb_unplaced_sphere(vgb_geometry *g, double rmin, double rmax, double sphi,
                                double dphi, double stheta, double dtheta, int32_t *id) {
@@ -234,9 +266,6 @@ vgb_status vgb_unplaced_polycone(vgb_geometry *, double, double, int32_t, const 
 vgb_status vgb_unplaced_polyhedron(vgb_geometry *, double, double, int32_t, int32_t,
                                    const double *, const double *, const double *, int32_t *) {
   VGB_NOTYET("vgb_unplaced_polyhedron");
-}
-vgb_status vgb_unplaced_trd(vgb_geometry *, double, double, double, double, double, int32_t *) {
-  VGB_NOTYET("vgb_unplaced_trd");
 }
 vgb_status vgb_unplaced_boolean(vgb_geometry *, int32_t, int32_t, int32_t, int32_t *) {
   VGB_NOTYET("vgb_unplaced_boolean");
