@@ -316,13 +316,16 @@ def main():
             d2h_bytes += m * out_d.element_size()
             tasks.append((name, opname, m, run_d, run_h))
 
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")   # > 126 MB L2
+    # L2 flush: a read sweep over 256 MB (> 126 MB L2); reading leaves clean lines,
+    # so the next kernel pays no write-back for the flush itself
+    flush = torch.ones(64 << 20, dtype=torch.float32, device="cuda")
+    flush_sink = torch.empty((), dtype=torch.float32, device="cuda")
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
           for _ in tasks]
 
     def one_step(timed: bool):
         for k, t in enumerate(tasks):
-            flush.zero_()
+            torch.sum(flush, out=flush_sink)
             if timed:
                 ev[k][0].record(stream)
             t[3]()
@@ -410,7 +413,7 @@ def main():
             "dtype": "f64" if args.precision == "fp64" else "f32+f64",
             "data": "synthetic (seeded)",
             "config": dict(workload_desc(args.workload, n, args.precision),
-                           l2="flushed (256 MB write) before every op, outside the events"),
+                           l2="flushed (256 MB read sweep) before every op, outside the events"),
             "per_op_mpoints_s": per_op, "roofline": roof, "e2e": e2e,
             "gpu_launches": launches, "clocks": clk}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

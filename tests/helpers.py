@@ -75,4 +75,5 @@ def shape_specs() -> dict:
     s["spheresector"] = W.sphere_spec(5., 30., 0.3, 4.0, 0.4, 1.9)
     s["spherefull"] = W.sphere_spec(0., 25., 0., 2 * math.pi, 0., math.pi)
     s["trd1"] = W.trd_spec(10., 20., 15., 15., 30.)
+    s["torussector"] = W.torus_spec(2., 6., 40., 0.4, 4.5)
     return s

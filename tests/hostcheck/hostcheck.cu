@@ -25,7 +25,7 @@ int run(const P &prm, const DXform &X, int op, int64_t n, const double *x, const
     case VGB_OP_CONTAINS: static_cast<uint8_t *>(out)[i] = Ops::contains(prm, xf_point(X, m)); break;
     case VGB_OP_INSIDE: static_cast<int32_t *>(out)[i] = Ops::inside(prm, xf_point(X, m)); break;
     case VGB_OP_DISTANCE_TO_IN:
-      static_cast<double *>(out)[i] = Ops::distance_to_in(prm, xf_point(X, m), xf_dir(X, d), st[i]);
+      static_cast<double *>(out)[i] = Ops::distance_to_in(prm, xf_point(X, m), dti_dir<Ops>(X, d), st[i]);
       break;
     case VGB_OP_DISTANCE_TO_OUT:
       static_cast<double *>(out)[i] = Ops::distance_to_out(prm, m, d, st[i]);

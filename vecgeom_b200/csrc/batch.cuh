@@ -8,6 +8,8 @@
 // which make a device virtual call per point, with shape and op resolved at
 // compile time.
 #pragma once
+#include <type_traits>
+
 #include "shapes.cuh"
 
 namespace vgb {
@@ -38,6 +40,21 @@ struct FusedIO {
 
 template <class T> VGB_D T ldg(const T *p) { return __ldg(p); }
 
+// Shapes whose reference DistanceToIn moves the direction with the point
+// transform (TorusImplementation.h:906) declare kDirectionAsPoint.
+template <class Ops, class = void> struct DirAsPoint : std::false_type {};
+template <class Ops>
+struct DirAsPoint<Ops, std::void_t<decltype(Ops::kDirectionAsPoint)>>
+    : std::integral_constant<bool, Ops::kDirectionAsPoint> {};
+
+template <class Ops, class R>
+VGB_HD V3<R> dti_dir(const DXform &X, const V3<R> &d) {
+  if constexpr (DirAsPoint<Ops>::value)
+    return xf_point(X, d);
+  else
+    return xf_dir(X, d);
+}
+
 template <class Ops, class P, int OP>
 __device__ __forceinline__ void batch_point(const P &prm, const DXform &X, const BatchIO &io,
                                             int64_t i) {
@@ -67,7 +84,7 @@ __device__ __forceinline__ void batch_point(const P &prm, const DXform &X, const
     const V3<R> d = {ldg(io.dx + i), ldg(io.dy + i), ldg(io.dz + i)};
     if constexpr (OP == VGB_OP_DISTANCE_TO_IN) {
       static_cast<double *>(io.out)[i] =
-          Ops::distance_to_in(prm, xf_point(X, m), xf_dir(X, d), ldg(io.step + i));
+          Ops::distance_to_in(prm, xf_point(X, m), dti_dir<Ops>(X, d), ldg(io.step + i));
     } else if constexpr (OP == VGB_OP_DISTANCE_TO_OUT) {
       static_cast<double *>(io.out)[i] = Ops::distance_to_out(prm, m, d, ldg(io.step + i));
     } else if constexpr (OP == VGB_OP_DISTANCE_TO_OUT_NODE) {
@@ -85,7 +102,7 @@ __device__ __forceinline__ void batch_point(const P &prm, const DXform &X, const
       // distance is the step limit; update only on a strictly smaller result.
       double *o = static_cast<double *>(io.out);
       const R cur = o[i];
-      const R r = Ops::distance_to_in(prm, xf_point(X, m), xf_dir(X, d), cur);
+      const R r = Ops::distance_to_in(prm, xf_point(X, m), dti_dir<Ops>(X, d), cur);
       if (r < cur) {
         o[i] = r;
         io.aux[i] = io.daughter;
@@ -128,7 +145,7 @@ __global__ void __launch_bounds__(kBatchBlock) k_fused(const P prm, const DXform
       static_cast<double *>(io.out[VGB_OP_SAFETY_TO_OUT])[i] = Ops::safety_to_out(prm, m);
     if (ops & (1u << VGB_OP_DISTANCE_TO_IN))
       static_cast<double *>(io.out[VGB_OP_DISTANCE_TO_IN])[i] =
-          Ops::distance_to_in(prm, l, xf_dir(X, d), ldg(io.step + i));
+          Ops::distance_to_in(prm, l, dti_dir<Ops>(X, d), ldg(io.step + i));
     if (ops & (1u << VGB_OP_DISTANCE_TO_OUT)) {
       R r = Lim<R>::inf();
       if (!(io.flags & VGB_FUSED_DTO_INSIDE_ONLY) || c)

@@ -6,6 +6,7 @@
 #include "cone.cuh"
 #include "sphere.cuh"
 #include "trd.cuh"
+#include "torus.cuh"
 
 struct vgb_geometry;
 
@@ -15,7 +16,8 @@ struct vgb_geometry;
   X(VGB_SHAPE_TUBE, vgb::TubeOps, vgb::TubeP) \
   X(VGB_SHAPE_CONE, vgb::ConeOps, vgb::ConeP) \
   X(VGB_SHAPE_SPHERE, vgb::SphereOps, vgb::SphereP) \
-  X(VGB_SHAPE_TRD, vgb::TrdOps, vgb::TrdP)
+  X(VGB_SHAPE_TRD, vgb::TrdOps, vgb::TrdP) \
+  X(VGB_SHAPE_TORUS, vgb::TorusOps, vgb::TorusP)
 
 namespace vgb {
 // Called by vgb_geometry_close() once the device parameter pool is allocated:

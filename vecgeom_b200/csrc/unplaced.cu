@@ -199,9 +199,41 @@ TrdP make_trd(double dx1, double dx2, double dy1, double dy2, double dz) {
   return t;
 }
 
+// UnplacedTorus constructor (volumes/UnplacedTorus.h:40-70): cached squares,
+// phi wedge and the bounding tube (rtor-rmax-kTolerance, rtor+rmax+kTolerance,
+// rmax, sphi, dphi), which DistanceToIn runs as TubeTypes::HollowTube
+// (TorusImplementation.h:908-923): rmin always checked, phi never.
+TorusP make_torus(double rmin, double rmax, double rtor, double sphi, double dphi) {
+  TorusP t;
+  std::memset(&t, 0, sizeof(t));
+  t.rmin = rmin;
+  t.rmax = rmax;
+  t.rtor = rtor;
+  t.sphi = sphi;
+  t.dphi = dphi;
+  t.rmin2 = rmin * rmin;
+  t.rmax2 = rmax * rmax;
+  t.rtor2 = rtor * rtor;
+  t.wedge = make_wedge(dphi, sphi);
+  t.btube = make_tube(rtor - rmax - kTolerance, rtor + rmax + kTolerance, rmax, sphi, dphi);
+  t.btube.has_rmin = 1;
+  t.btube.has_phi = 0;
+  t.has_phi = dphi < kTwoPi;
+  return t;
+}
+
 }  // namespace vgb
 
 extern "C" {
+
+vgb_status vgb_unplaced_torus(vgb_geometry *g, double rmin, double rmax, double rtor, double sphi,
+                              double dphi, int32_t *id) {
+  VGB_CHECK_OPEN(g);
+  if (!(rmin >= 0 && rmax > rmin && rtor > rmax && dphi > 0))
+    return set_error(VGB_EINVAL, "vgb_unplaced_torus: need 0 <= rmin < rmax < rtor, dphi > 0");
+  TorusP t = make_torus(rmin, rmax, rtor, sphi, dphi);
+  return add_unplaced(g, VGB_SHAPE_TORUS, &t, sizeof(t), 0, id);
+}
 
 vgb_status vgb_unplaced_trd(vgb_geometry *g, double dx1, double dx2, double dy1, double dy2,
                             double dz, int32_t *id) {
@@ -256,9 +288,6 @@ vgb_status vgb_unplaced_tube(vgb_geometry *g, double rmin, double rmax, double d
 // shapes not yet uploaded by this build report VGB_ENOTSUP
 // ---------------------------------------------------------------------------
 #define VGB_NOTYET(name) return set_error(VGB_ENOTSUP, name ": shape not available yet")
-vgb_status vgb_unplaced_torus(vgb_geometry *, double, double, double, double, double, int32_t *) {
-  VGB_NOTYET("vgb_unplaced_torus");
-}
 vgb_status vgb_unplaced_polycone(vgb_geometry *, double, double, int32_t, const double *,
                                  const double *, const double *, int32_t *) {
   VGB_NOTYET("vgb_unplaced_polycone");
