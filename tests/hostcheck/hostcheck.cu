@@ -50,7 +50,9 @@ extern "C" int hc_batch(const vgb_geometry *g, int32_t placed, int32_t op, int64
   switch (type) {
 #define VGB_SHAPE_CASE(TYPE, OPS, P) \
   case TYPE:                         \
-    return run<OPS<double>>(*static_cast<const P *>(prm), X, op, n, x, y, z, dx, dy, dz, st, out);
+    return run<OPS<double>>(bind_params(*static_cast<const P *>(prm),                    \
+                                        static_cast<const double *>(prm)),                \
+                            X, op, n, x, y, z, dx, dy, dz, st, out);
     VGB_FOR_EACH_SHAPE(VGB_SHAPE_CASE)
 #undef VGB_SHAPE_CASE
   default:

@@ -65,7 +65,8 @@ vgb_status launch_batch_f64(const vgb_geometry *g, int32_t placed, int op, const
   switch (type) {
 #define VGB_SHAPE_CASE(TYPE, OPS, P) \
   case TYPE:                         \
-    return launch_ops<OPS<double>>(*static_cast<const P *>(prm), X, op, io, s);
+    return launch_ops<OPS<double>>(                                                     \
+        bind_params(*static_cast<const P *>(prm), shape_params_dev(g, pr.unplaced)), X, op, io, s);
     VGB_FOR_EACH_SHAPE(VGB_SHAPE_CASE)
 #undef VGB_SHAPE_CASE
   default:
@@ -82,7 +83,8 @@ vgb_status launch_fused_f64(const vgb_geometry *g, int32_t placed, const FusedIO
   switch (type) {
 #define VGB_SHAPE_CASE(TYPE, OPS, P) \
   case TYPE:                         \
-    return launch_fused<OPS<double>>(*static_cast<const P *>(prm), X, io, s);
+    return launch_fused<OPS<double>>(                                                   \
+        bind_params(*static_cast<const P *>(prm), shape_params_dev(g, pr.unplaced)), X, io, s);
     VGB_FOR_EACH_SHAPE(VGB_SHAPE_CASE)
 #undef VGB_SHAPE_CASE
   default:

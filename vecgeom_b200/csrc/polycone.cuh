@@ -1,0 +1,197 @@
+// polycone.cuh -- Polycone shape arithmetic (device), templated on the arithmetic type.
+//
+// A polycone is a z-ordered stack of cone sections (volumes/UnplacedPolycone.h:32-124,
+// source/UnplacedPolycone.cpp:22-165); every operation walks the sections as
+// volumes/kernel/PolyconeImplementation.h does, calling the cone arithmetic of
+// cone.cuh on the point shifted into the section frame.  The section table sits
+// in the geometry's parameter pool right after this header; `base` is bound to
+// the record's address when the kernel is launched.
+#pragma once
+#include "cone.cuh"
+
+namespace vgb {
+
+struct PolySec {
+  ConeP cone;    // UnplacedCone(prevRmin, prevRmax, rMin, rMax, dz, phiStart, phiTotal)
+  double shift;  // fShift: z of the section centre
+  double pad;
+};
+
+struct PolyconeP {
+  int32_t nsec;
+  int32_t sec_off;  // doubles from the record start to the PolySec array
+  int32_t zs_off;   // doubles from the record start to fZs (nsec + 1 values)
+  int32_t pad;
+  const double *base;  // record address, bound at launch (device) or by host callers
+};
+
+template <class R> struct PolyconeOps {
+  using C = ConeOps<R>;
+
+  static VGB_HD const PolySec &sec(const PolyconeP &p, int i) {
+    return reinterpret_cast<const PolySec *>(p.base + p.sec_off)[i];
+  }
+  static VGB_HD R zs(const PolyconeP &p, int i) { return (R)p.base[p.zs_off + i]; }
+
+  // UnplacedPolycone::GetSectionIndex (volumes/UnplacedPolycone.h:113-124)
+  static VGB_HD int section_index(const PolyconeP &p, R z) {
+    if (z < zs(p, 0)) return -1;
+    for (int i = 0; i < p.nsec; ++i)
+      if (z >= zs(p, i) && z <= zs(p, i + 1)) return i;
+    return -2;
+  }
+
+  static VGB_HD V3<R> shifted(const V3<R> &q, const PolySec &s) {
+    return {q.x - (R)0, q.y - (R)0, q.z - (R)s.shift};
+  }
+
+  // ContainsKernel (:52-72)
+  static VGB_HD bool contains(const PolyconeP &p, const V3<R> &q) {
+    if (q.z < zs(p, 0) || q.z > zs(p, p.nsec)) return false;
+    const PolySec &s = sec(p, section_index(p, q.z));
+    return C::contains(s.cone, shifted(q, s));
+  }
+
+  // InsideKernel (:74-88): kInside or kOutside only
+  static VGB_HD int inside(const PolyconeP &p, const V3<R> &q) {
+    return contains(p, q) ? kInside : kOutside;
+  }
+
+  // DistanceToIn (:125-165)
+  static VGB_HD R distance_to_in(const PolyconeP &p, const V3<R> &q, const V3<R> &v, R smax) {
+    R distance = Lim<R>::inf();
+    int increment = (v.z > 0) ? 1 : -1;
+    if (fabs(v.z) < (R)kTolerance) increment = 0;
+    int index = section_index(p, q.z);
+    if (index == -1) index = 0;
+    if (index == -2) index = p.nsec - 1;
+    do {
+      const PolySec &s = sec(p, index);
+      distance = C::distance_to_in(s.cone, shifted(q, s), v, smax);
+      if (distance < Lim<R>::inf() || !increment) break;
+      index += increment;
+    } while (index >= 0 && index < p.nsec);
+    return distance;
+  }
+
+  // DistanceToOut (:167-292)
+  static VGB_HD R distance_to_out(const PolyconeP &p, const V3<R> &q, const V3<R> &v, R smax) {
+    if (p.nsec == 1) {
+      const PolySec &s = sec(p, 0);
+      return C::distance_to_out(s.cone, shifted(q, s), v, smax);
+    }
+    const int indexLow = section_index(p, q.z - (R)kTolerance);
+    const int indexHigh = section_index(p, q.z + (R)kTolerance);
+    int index;
+    if (indexLow != indexHigh && (indexLow >= 0)) {
+      const PolySec &s = sec(p, indexLow);
+      index = C::contains(s.cone, shifted(q, s)) ? indexLow : indexHigh;
+    } else {
+      index = indexLow;
+      if (index < 0) index = section_index(p, q.z);
+    }
+    if (index < 0) return (R)0.;
+    R totalDistance = 0.;
+    R dist;
+    int increment = (v.z > 0) ? 1 : -1;
+    if (fabs(v.z) < (R)kTolerance) increment = 0;
+    int istep = 0;
+    V3<R> pn = q;
+    do {
+      const PolySec &s = sec(p, index);
+      if ((totalDistance != 0) || (istep < 2)) {
+        pn = {q.x + totalDistance * v.x, q.y + totalDistance * v.y, q.z + totalDistance * v.z};
+        pn.z = pn.z - (R)s.shift;
+        if (C::inside(s.cone, pn) == kOutside) break;
+      } else {
+        pn.z = pn.z - (R)s.shift;
+      }
+      istep++;
+      dist = C::distance_to_out(s.cone, pn, v, smax);
+      if (fabs(dist) < (R)0.5 * (R)kTolerance) {
+        int index1 = index;
+        if ((index > 0) && (index < p.nsec - 1)) {
+          index1 += increment;
+        } else {
+          if ((index == 0) && (increment > 0)) index1 += increment;
+          if ((index == p.nsec - 1) && (increment < 0)) index1 += increment;
+        }
+        const R td = totalDistance + dist;
+        V3<R> pte = {q.x + td * v.x, q.y + td * v.y, q.z + td * v.z};
+        const PolySec &s1 = sec(p, index1);
+        pte.z = pte.z - (R)s1.shift;
+        if (!C::contains(s1.cone, pte)) break;
+      }
+      totalDistance += dist;
+      index += increment;
+    } while (increment != 0 && index >= 0 && index < p.nsec);
+    return totalDistance;
+  }
+
+  // SafetyToIn (:336-408)
+  static VGB_HD R safety_to_in(const PolyconeP &p, const V3<R> &q) {
+    int index = section_index(p, q.z);
+    bool needZ = false;
+    if (index < 0) {
+      needZ = true;
+      if (index == -1) index = 0;
+      if (index == -2) index = p.nsec - 1;
+    }
+    const PolySec &s = sec(p, index);
+    if (needZ) return C::template safety_to_in_impl<false>(s.cone, shifted(q, s));
+    R safety = C::template safety_to_in_impl<true>(s.cone, shifted(q, s));
+    if (safety < (R)kTolerance) return safety;
+    R minSafety = safety;
+    R zbase = zs(p, index + 1);
+    for (int i = index + 1; i < p.nsec; ++i) {
+      const R dz = zs(p, i) - zbase;
+      if (dz >= minSafety) break;
+      const PolySec &si = sec(p, i);
+      safety = C::template safety_to_in_impl<false>(si.cone, shifted(q, si));
+      if (safety < minSafety) minSafety = safety;
+    }
+    if (index > 0) {  // the reference reads fZs[index-1] unconditionally; unused when index == 0
+      zbase = zs(p, index - 1);
+      for (int i = index - 1; i >= 0; --i) {
+        const R dz = zbase - zs(p, i);
+        if (dz >= minSafety) break;
+        const PolySec &si = sec(p, i);
+        safety = C::template safety_to_in_impl<false>(si.cone, shifted(q, si));
+        if (safety < minSafety) minSafety = safety;
+      }
+    }
+    return minSafety;
+  }
+
+  // SafetyToOut (:431-476)
+  static VGB_HD R safety_to_out(const PolyconeP &p, const V3<R> &q) {
+    const int index = section_index(p, q.z);
+    if (index < 0) return (R)0;
+    const PolySec &s = sec(p, index);
+    R safety = C::template safety_to_out_impl<false>(s.cone, shifted(q, s));
+    R minSafety = safety;
+    if (minSafety == Lim<R>::inf()) return (R)0.;
+    if (minSafety < (R)kTolerance) return (R)0.;
+    R zbase = zs(p, index + 1);
+    for (int i = index + 1; i < p.nsec; ++i) {
+      const R dz = zs(p, i) - zbase;
+      if (dz >= minSafety) break;
+      const PolySec &si = sec(p, i);
+      safety = C::template safety_to_in_impl<false>(si.cone, shifted(q, si));
+      if (safety < minSafety) minSafety = safety;
+    }
+    if (index > 0) {
+      zbase = zs(p, index - 1);
+      for (int i = index - 1; i >= 0; --i) {
+        const R dz = zbase - zs(p, i);
+        if (dz >= minSafety) break;
+        const PolySec &si = sec(p, i);
+        safety = C::template safety_to_in_impl<false>(si.cone, shifted(q, si));
+        if (safety < minSafety) minSafety = safety;
+      }
+    }
+    return minSafety;
+  }
+};
+
+}  // namespace vgb

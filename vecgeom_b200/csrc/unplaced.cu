@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <vector>
 
 #include "geometry.h"
 #include "shapes.cuh"
@@ -222,9 +223,71 @@ TorusP make_torus(double rmin, double rmax, double rtor, double sphi, double dph
   return t;
 }
 
+// UnplacedPolycone::Init (source/UnplacedPolycone.cpp:22-165): one cone section
+// per pair of consecutive, increasing z planes; equal z planes add no section.
+// Returns the record (header, sections, fZs) as a double blob.
+std::vector<double> make_polycone(double sphi, double dphi, int nz, const double *rmin,
+                                  const double *rmax, const double *z) {
+  std::vector<PolySec> secs;
+  std::vector<double> zsv;
+  double prevZ = z[0], prevRmax = 0, prevRmin = 0;
+  int dirZ = 1;
+  if (nz > 1 && z[1] < z[0]) dirZ = -1;
+  for (int i = 0; i < nz; ++i) {
+    const double rMin = rmin[i], rMax = rmax[i], zi = z[i];
+    if (i > 0) {
+      if (((zi > prevZ) && (dirZ > 0)) || ((zi < prevZ) && (dirZ < 0))) {
+        const double dz = (zi - prevZ) / 2;
+        PolySec s;
+        std::memset(&s, 0, sizeof(s));
+        s.cone = make_cone(prevRmin, prevRmax, rMin, rMax, dz, sphi, dphi);
+        zsv.push_back(zi);
+        const size_t k = zsv.size() - 1;
+        s.shift = zsv[k - 1] + 0.5 * (zsv[k] - zsv[k - 1]);
+        secs.push_back(s);
+      }
+    } else {
+      zsv.push_back(zi);
+    }
+    prevZ = zi;
+    prevRmin = rMin;
+    prevRmax = rMax;
+  }
+  PolyconeP h;
+  std::memset(&h, 0, sizeof(h));
+  const int hdr = (int)((sizeof(PolyconeP) + 15) / 16 * 2);
+  const int secd = (int)(sizeof(PolySec) / sizeof(double));
+  h.nsec = (int32_t)secs.size();
+  h.sec_off = hdr;
+  h.zs_off = hdr + h.nsec * secd;
+  std::vector<double> blob(h.zs_off + zsv.size() + 1, 0.);
+  std::memcpy(blob.data(), &h, sizeof(h));
+  if (!secs.empty()) std::memcpy(blob.data() + h.sec_off, secs.data(), secs.size() * sizeof(PolySec));
+  std::memcpy(blob.data() + h.zs_off, zsv.data(), zsv.size() * sizeof(double));
+  return blob;
+}
+
 }  // namespace vgb
 
 extern "C" {
+
+vgb_status vgb_unplaced_polycone(vgb_geometry *g, double sphi, double dphi, int32_t nz,
+                                 const double *rmin, const double *rmax, const double *z,
+                                 int32_t *id) {
+  VGB_CHECK_OPEN(g);
+  if (nz < 2 || !rmin || !rmax || !z)
+    return set_error(VGB_EINVAL, "vgb_unplaced_polycone: need nz >= 2 and the three arrays");
+  for (int i = 0; i < nz; ++i)
+    if (rmin[i] < 0 || rmax[i] < rmin[i])
+      return set_error(VGB_EINVAL, "vgb_unplaced_polycone: rmin[%d] > rmax[%d]", i, i);
+  for (int i = 1; i < nz; ++i)
+    if (z[i] < z[i - 1])
+      return set_error(VGB_EINVAL, "vgb_unplaced_polycone: z planes must not decrease");
+  std::vector<double> blob = make_polycone(sphi, dphi, nz, rmin, rmax, z);
+  if (reinterpret_cast<const PolyconeP *>(blob.data())->nsec < 1)
+    return set_error(VGB_EINVAL, "vgb_unplaced_polycone: no section (all z planes equal)");
+  return add_unplaced(g, VGB_SHAPE_POLYCONE, blob.data(), blob.size() * sizeof(double), 0, id);
+}
 
 vgb_status vgb_unplaced_torus(vgb_geometry *g, double rmin, double rmax, double rtor, double sphi,
                               double dphi, int32_t *id) {
@@ -288,10 +351,6 @@ vgb_status vgb_unplaced_tube(vgb_geometry *g, double rmin, double rmax, double d
 // shapes not yet uploaded by this build report VGB_ENOTSUP
 // ---------------------------------------------------------------------------
 #define VGB_NOTYET(name) return set_error(VGB_ENOTSUP, name ": shape not available yet")
-vgb_status vgb_unplaced_polycone(vgb_geometry *, double, double, int32_t, const double *,
-                                 const double *, const double *, int32_t *) {
-  VGB_NOTYET("vgb_unplaced_polycone");
-}
 vgb_status vgb_unplaced_polyhedron(vgb_geometry *, double, double, int32_t, int32_t,
                                    const double *, const double *, const double *, int32_t *) {
   VGB_NOTYET("vgb_unplaced_polyhedron");
