@@ -325,7 +325,7 @@ def main():
 
     def one_step(timed: bool):
         for k, t in enumerate(tasks):
-            torch.sum(flush, out=flush_sink)
+            torch.sum(flush, dim=0, out=flush_sink)
             if timed:
                 ev[k][0].record(stream)
             t[3]()

@@ -76,6 +76,9 @@ def shape_specs() -> dict:
     s["spherefull"] = W.sphere_spec(0., 25., 0., 2 * math.pi, 0., math.pi)
     s["trd1"] = W.trd_spec(10., 20., 15., 15., 30.)
     s["torussector"] = W.torus_spec(2., 6., 40., 0.4, 4.5)
+    s["polyhedroncut"] = W.polyhedron_spec(30., 270., 6, [-40., -10., 20., 45.],
+                                           [0., 8., 12., 5.], [25., 30., 35., 28.])
+    s["polyhedronlarge"] = W.polyhedron_spec(-20., 120., 3, [-30., 30.], [5., 10.], [20., 30.])
     s["polyconefull"] = W.polycone_spec(0., 2 * math.pi, [-50., -20., -20., 10., 40.],
                                         [0., 5., 8., 0., 12.], [20., 25., 30., 18., 30.])
     return s

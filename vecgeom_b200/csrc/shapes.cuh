@@ -8,6 +8,7 @@
 #include "trd.cuh"
 #include "torus.cuh"
 #include "polycone.cuh"
+#include "polyhedron.cuh"
 
 struct vgb_geometry;
 
@@ -19,7 +20,8 @@ struct vgb_geometry;
   X(VGB_SHAPE_SPHERE, vgb::SphereOps, vgb::SphereP)           \
   X(VGB_SHAPE_TRD, vgb::TrdOps, vgb::TrdP)                    \
   X(VGB_SHAPE_TORUS, vgb::TorusOps, vgb::TorusP)              \
-  X(VGB_SHAPE_POLYCONE, vgb::PolyconeOps, vgb::PolyconeP)
+  X(VGB_SHAPE_POLYCONE, vgb::PolyconeOps, vgb::PolyconeP)    \
+  X(VGB_SHAPE_POLYHEDRON, vgb::PolyhedronOps, vgb::PolyhedronP)
 
 namespace vgb {
 
@@ -28,6 +30,10 @@ namespace vgb {
 // device copy of the parameter pool, or the host copy for host-side callers.
 template <class P> VGB_HD P bind_params(P p, const double *) { return p; }
 VGB_HD PolyconeP bind_params(PolyconeP p, const double *rec) {
+  p.base = rec;
+  return p;
+}
+VGB_HD PolyhedronP bind_params(PolyhedronP p, const double *rec) {
   p.base = rec;
   return p;
 }

@@ -267,9 +267,250 @@ std::vector<double> make_polycone(double sphi, double dphi, int nz, const double
   return blob;
 }
 
+// ---- polyhedron construction (source/UnplacedPolyhedron.cpp:20-175) --------
+
+namespace {
+struct HV {
+  double x, y, z;
+};
+HV hv(double x, double y, double z) { return HV{x, y, z}; }
+bool operator==(const HV &a, const HV &b) { return a.x == b.x && a.y == b.y && a.z == b.z; }
+HV sub(const HV &a, const HV &b) { return hv(a.x - b.x, a.y - b.y, a.z - b.z); }
+double dot(const HV &a, const HV &b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+double length(const HV &a) { return std::sqrt(dot(a, a)); }
+HV scale(const HV &a, double s) { return hv(a.x * s, a.y * s, a.z * s); }
+// Vector3D::Normalized (base/Vector3D.h:236-238): multiply by 1/Length
+HV normalized(const HV &a) { return scale(a, 1. / length(a)); }
+// Vector3D::FixZeroes (base/Vector3D.h:344-349)
+HV fix_zeroes(HV a) {
+  if (std::fabs(a.x) < kTolerance) a.x = 0.;
+  if (std::fabs(a.y) < kTolerance) a.y = 0.;
+  if (std::fabs(a.z) < kTolerance) a.z = 0.;
+  return a;
+}
+// Vector3D::Cross (base/Vector3D.h:266-272)
+HV cross(const HV &l, const HV &r) {
+  return hv(l.y * r.z - l.z * r.y, l.z * r.x - l.x * r.z, l.x * r.y - l.y * r.x);
+}
+HV from_cylindrical(double r, double phi, double z) {
+  return hv(r * std::cos(phi), r * std::sin(phi), z);
+}
+// NormalizeAngle (volumes/kernel/GenericKernels.h:106-110)
+double normalize_angle(double a) { return a + kTwoPi * ((a < 0) - int(a / kTwoPi)); }
+
+void set_quad_corner(PhQuad &q, int k, const HV &c) {
+  q.c[k][0] = c.x;
+  q.c[k][1] = c.y;
+  q.c[k][2] = c.z;
+}
+HV quad_corner(const PhQuad &q, int k) { return hv(q.c[k][0], q.c[k][1], q.c[k][2]); }
+
+// Quadrilaterals::Set (source/Quadrilaterals.cpp:38-104)
+void quad_set(PhQuad &q, const HV &c0, const HV &c1, const HV &c2, const HV &c3) {
+  std::memset(&q, 0, sizeof(q));
+  set_quad_corner(q, 0, c0);
+  set_quad_corner(q, 1, c1);
+  set_quad_corner(q, 2, c2);
+  set_quad_corner(q, 3, c3);
+  HV chosen[4];
+  chosen[0] = quad_corner(q, 0);
+  int assigned = 1, tested = 1;
+  while (tested <= 4) {
+    do {
+      chosen[assigned] = tested < 4 ? quad_corner(q, tested) : chosen[assigned - 1];
+      tested++;
+    } while ((chosen[assigned] == chosen[assigned - 1]) && tested < 4);
+    assigned++;
+    if (assigned == 3) break;
+  }
+  const HV &a0 = chosen[0], &a1 = chosen[1], &a2 = chosen[2];
+  const double a = a0.y * (a1.z - a2.z) + a1.y * (a2.z - a0.z) + a2.y * (a0.z - a1.z);
+  const double b = a0.z * (a1.x - a2.x) + a1.z * (a2.x - a0.x) + a2.z * (a0.x - a1.x);
+  const double c = a0.x * (a1.y - a2.y) + a1.x * (a2.y - a0.y) + a2.x * (a0.y - a1.y);
+  double d = -a0.x * (a1.y * a2.z - a2.y * a1.z) - a1.x * (a2.y * a0.z - a0.y * a2.z) -
+             a2.x * (a0.y * a1.z - a1.y * a0.z);
+  HV normal = hv(a, b, c);
+  const double inv = 1. / length(normal);
+  normal = scale(normal, inv);
+  d *= inv;
+  normal = fix_zeroes(normal);
+  q.n[0] = normal.x;
+  q.n[1] = normal.y;
+  q.n[2] = normal.z;
+  q.d = d;
+  // ComputeSideVector + Planes::Set(index, normal, origin) (source/Planes.cpp:30-39)
+  const HV cs[4] = {c0, c1, c2, c3};
+  for (int j = 0; j < 4; ++j) {
+    const HV &s0 = cs[j], &s1 = cs[(j + 1) % 4];
+    if (!(s1 == s0)) {
+      const HV sv = normalized(cross(normal, sub(s1, s0)));
+      const HV fixed = fix_zeroes(sv);
+      const double il = 1. / length(fixed);
+      const HV nn = scale(fixed, il);
+      q.sn[j][0] = nn.x;
+      q.sn[j][1] = nn.y;
+      q.sn[j][2] = nn.z;
+      q.sd[j] = il * -dot(fixed, s0);
+    } else {
+      q.sn[j][0] = q.sn[j][1] = q.sn[j][2] = 0.;
+      q.sd[j] = 0.;
+    }
+  }
+}
+
+// Quadrilaterals::FlipSign -> Planes::FlipSign (source/Planes.cpp:48-51)
+void quad_flip(PhQuad &q) {
+  q.n[0] = -q.n[0];
+  q.n[1] = -q.n[1];
+  q.n[2] = -q.n[2];
+  q.d = -q.d;
+}
+HV quad_normal(const PhQuad &q) { return hv(q.n[0], q.n[1], q.n[2]); }
+}  // namespace
+
+std::vector<double> make_polyhedron(double phiStart, double phiDelta, int sides, int nz,
+                                    const double *zPlanes, const double *rMin, const double *rMax) {
+  const bool hasPhiCutout = phiDelta < 360;
+  const bool largePhiCutout = phiDelta < 180;
+  bool hasInnerRadii = false;
+  const int nseg = nz - 1;
+  std::vector<PhSeg> segs(nseg);
+  std::vector<PhQuad> quads;
+  std::vector<int> outer_n(nseg), inner_n(nseg), phi_n(nseg), has_inner(nseg);
+  for (int i = 0; i < nseg; ++i) {
+    has_inner[i] = rMin[i] > 0 || rMin[i + 1] > 0;
+    outer_n[i] = sides * ((zPlanes[i] == zPlanes[i + 1] && rMax[i] == rMax[i + 1]) ? 0 : 1);
+    phi_n[i] = hasPhiCutout ? 2 * ((zPlanes[i] == zPlanes[i + 1]) ? 0 : 1) : 0;
+    const int mult = (zPlanes[i] == zPlanes[i + 1] && rMin[i] == rMin[i + 1]) ? 0 : 1;
+    inner_n[i] = 0;
+    if (has_inner[i]) {
+      inner_n[i] = sides * mult;
+      hasInnerRadii = true;
+    }
+  }
+  phiStart = normalize_angle(kDegToRad * phiStart);
+  phiDelta *= kDegToRad;
+  if (phiDelta > kTwoPi) phiDelta = kTwoPi;
+  const double sidePhi = phiDelta / sides;
+  std::vector<double> vphi(sides + 1);
+  std::vector<HV> phisec(sides + 1);
+  for (int i = 0; i < sides + 1; ++i) {
+    vphi[i] = normalize_angle(phiStart + i * sidePhi);
+    const HV cv = fix_zeroes(normalized(from_cylindrical(1., vphi[i], 0)));
+    phisec[i] = cross(normalized(cv), hv(0, 0, -1));
+  }
+  if (!hasPhiCutout) vphi[sides] = vphi[0];
+  const double cosHalfDeltaPhi = std::cos(0.5 * sidePhi);
+  double innerRadius = HUGE_VAL, outerRadius = -HUGE_VAL;
+  for (int i = 0; i < nz; ++i) {
+    if (rMin[i] < innerRadius) innerRadius = rMin[i];
+    if (rMax[i] > outerRadius) outerRadius = rMax[i];
+  }
+  outerRadius /= cosHalfDeltaPhi;
+  const double boundingTubeZ = zPlanes[nz - 1] - zPlanes[0] + 2. * kTolerance;
+  const double boundsPhiStart = !hasPhiCutout ? 0 : phiStart;
+  const double boundsPhiDelta = !hasPhiCutout ? kTwoPi : phiDelta;
+
+  const int nv = nz * (sides + 1);
+  std::vector<HV> ov(nv), iv(nv);
+  auto vi = [&](int plane, int corner) { return plane * (sides + 1) + corner; };
+  for (int i = 0; i < nz; ++i) {
+    for (int j = 0, jMax = sides + (hasPhiCutout ? 1 : 0); j < jMax; ++j) {
+      ov[vi(i, j)] = fix_zeroes(from_cylindrical(rMax[i] / cosHalfDeltaPhi, vphi[j], zPlanes[i]));
+      iv[vi(i, j)] = fix_zeroes(from_cylindrical(rMin[i] / cosHalfDeltaPhi, vphi[j], zPlanes[i]));
+    }
+    if (!hasPhiCutout) {
+      ov[vi(i, sides)] = ov[vi(i, 0)];
+      iv[vi(i, sides)] = iv[vi(i, 0)];
+    }
+  }
+  auto wrong_normal = [](const HV &n, const HV &c) { return n.x * c.x + n.y * c.y < 0; };
+  for (int p = 0; p < nseg; ++p) {
+    PhSeg &s = segs[p];
+    std::memset(&s, 0, sizeof(s));
+    s.has_inner = has_inner[p];
+    s.outer_off = (int32_t)quads.size();
+    s.outer_n = outer_n[p];
+    for (int k = 0; k < outer_n[p]; ++k) {
+      PhQuad q;
+      quad_set(q, ov[vi(p, k)], ov[vi(p, k + 1)], ov[vi(p + 1, k + 1)], ov[vi(p + 1, k)]);
+      if (wrong_normal(quad_normal(q), ov[vi(p, k)])) quad_flip(q);
+      quads.push_back(q);
+    }
+    s.inner_off = (int32_t)quads.size();
+    s.inner_n = inner_n[p];
+    for (int k = 0; k < inner_n[p]; ++k) {
+      PhQuad q;
+      quad_set(q, iv[vi(p, k)], iv[vi(p, k + 1)], iv[vi(p + 1, k + 1)], iv[vi(p + 1, k)]);
+      if (wrong_normal(quad_normal(q), iv[vi(p, k)])) quad_flip(q);
+      quads.push_back(q);
+    }
+    s.phi_off = (int32_t)quads.size();
+    s.phi_n = phi_n[p];
+    if (hasPhiCutout && phi_n[p] == 2) {
+      PhQuad q0, q1;
+      quad_set(q0, iv[vi(p, 0)], iv[vi(p + 1, 0)], ov[vi(p + 1, 0)], ov[vi(p, 0)]);
+      if (dot(quad_normal(q0), phisec[0]) > 0) quad_flip(q0);
+      quad_set(q1, ov[vi(p, sides)], ov[vi(p + 1, sides)], iv[vi(p + 1, sides)], iv[vi(p, sides)]);
+      if (dot(quad_normal(q1), phisec[sides]) < 0) quad_flip(q1);
+      quads.push_back(q0);
+      quads.push_back(q1);
+    }
+  }
+
+  PolyhedronP h;
+  std::memset(&h, 0, sizeof(h));
+  h.sides = sides;
+  h.nseg = nseg;
+  h.has_inner_radii = hasInnerRadii;
+  h.has_phi_cutout = hasPhiCutout;
+  h.large_phi_cutout = largePhiCutout;
+  h.btube = make_tube(innerRadius - kTolerance, outerRadius + kTolerance, 0.5 * boundingTubeZ,
+                      boundsPhiStart, boundsPhiDelta);
+  // HasInnerRadiiTraits (PolyhedronImplementation.h:150-160): HollowTube or
+  // NonHollowTube kernels, neither with phi treatment
+  h.btube.has_rmin = hasInnerRadii;
+  h.btube.has_phi = 0;
+  h.btube_offset = zPlanes[0] + 0.5 * boundingTubeZ;
+  const int hdr = (int)((sizeof(PolyhedronP) + 15) / 16 * 2);
+  h.seg_off = hdr;
+  h.quad_off = h.seg_off + (int)((nseg * sizeof(PhSeg) + 15) / 16 * 2);
+  h.zp_off = h.quad_off + (int)(quads.size() * sizeof(PhQuad) / sizeof(double));
+  h.phisec_off = h.zp_off + nz + (nz % 2);
+  std::vector<double> blob(h.phisec_off + 3 * (sides + 1) + 1, 0.);
+  std::memcpy(blob.data(), &h, sizeof(h));
+  std::memcpy(blob.data() + h.seg_off, segs.data(), nseg * sizeof(PhSeg));
+  if (!quads.empty())
+    std::memcpy(blob.data() + h.quad_off, quads.data(), quads.size() * sizeof(PhQuad));
+  for (int i = 0; i < nz; ++i) blob[h.zp_off + i] = zPlanes[i];
+  for (int i = 0; i < sides + 1; ++i) {
+    blob[h.phisec_off + 3 * i] = phisec[i].x;
+    blob[h.phisec_off + 3 * i + 1] = phisec[i].y;
+    blob[h.phisec_off + 3 * i + 2] = phisec[i].z;
+  }
+  return blob;
+}
+
 }  // namespace vgb
 
 extern "C" {
+
+vgb_status vgb_unplaced_polyhedron(vgb_geometry *g, double phi_start_deg, double phi_delta_deg,
+                                   int32_t sides, int32_t nz, const double *z,
+                                   const double *rmin, const double *rmax, int32_t *id) {
+  VGB_CHECK_OPEN(g);
+  if (nz < 2 || sides < 1 || !z || !rmin || !rmax || !(phi_delta_deg > 0))
+    return set_error(VGB_EINVAL, "vgb_unplaced_polyhedron: need nz >= 2, sides >= 1, phi delta > 0");
+  for (int i = 0; i < nz; ++i)
+    if (rmin[i] < 0 || !(rmax[i] > 0) || rmin[i] > rmax[i])
+      return set_error(VGB_EINVAL, "vgb_unplaced_polyhedron: invalid radii at plane %d", i);
+  for (int i = 1; i < nz; ++i)
+    if (z[i] < z[i - 1])
+      return set_error(VGB_EINVAL, "vgb_unplaced_polyhedron: z planes must not decrease");
+  std::vector<double> blob =
+      make_polyhedron(phi_start_deg, phi_delta_deg, sides, nz, z, rmin, rmax);
+  return add_unplaced(g, VGB_SHAPE_POLYHEDRON, blob.data(), blob.size() * sizeof(double), 0, id);
+}
 
 vgb_status vgb_unplaced_polycone(vgb_geometry *g, double sphi, double dphi, int32_t nz,
                                  const double *rmin, const double *rmax, const double *z,
@@ -351,10 +592,6 @@ vgb_status vgb_unplaced_tube(vgb_geometry *g, double rmin, double rmax, double d
 // shapes not yet uploaded by this build report VGB_ENOTSUP
 // ---------------------------------------------------------------------------
 #define VGB_NOTYET(name) return set_error(VGB_ENOTSUP, name ": shape not available yet")
-vgb_status vgb_unplaced_polyhedron(vgb_geometry *, double, double, int32_t, int32_t,
-                                   const double *, const double *, const double *, int32_t *) {
-  VGB_NOTYET("vgb_unplaced_polyhedron");
-}
 vgb_status vgb_unplaced_boolean(vgb_geometry *, int32_t, int32_t, int32_t, int32_t *) {
   VGB_NOTYET("vgb_unplaced_boolean");
 }
