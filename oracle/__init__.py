@@ -220,9 +220,10 @@ def ref_unplaced(ref: RefLib, spec):
                                   z.ctypes.data, rmin.ctypes.data, rmax.ctypes.data)
     if k == "boolsub":
         bx, by, bz = p["box_half"]
-        left = ref.placed(L.vgref_box(bx, by, bz), label="sub_box")
+        ident = (0., 0., 0., 0., 0., 0.)
+        left = ref.placed(L.vgref_box(bx, by, bz), *p.get("left_place", ident), label="sub_box")
         right = ref.placed(L.vgref_tube(0., p["tube_rmax"], p["tube_dz"], 0., 2 * math.pi),
-                           label="sub_tube")
+                           *p.get("right_place", ident), label="sub_tube")
         return L.vgref_boolean(2, left, right)
     raise ValueError(k)
 

@@ -13,12 +13,13 @@ import numpy as np
 import pytest
 
 import oracle
-from helpers import PLACEMENTS, assert_distances, assert_exact, vgb_unplaced
+from helpers import (PLACEMENTS, assert_distances, assert_exact, assert_torus_distances,
+                     vgb_unplaced)
 from test_oracle_golden import load_case, spec_from_meta
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 GOLDEN = sorted(glob.glob(os.path.join(HERE, "golden", "*.npz")))
-VGB_SHAPES = {"box", "tube", "cone", "sphere", "trd", "torus"}
+VGB_SHAPES = {"box", "tube", "cone", "sphere", "trd", "torus", "polycone", "polyhedron", "boolsub"}
 
 pytestmark = pytest.mark.gpu
 
@@ -79,10 +80,19 @@ def run_all_ops(pv, pm, dm, pl, dl, step, on_device=True):
     return out
 
 
-def check_against(res, want, what):
+def check_against(res, want, what, spec=None, local=None):
+    """local = (points, directions) of DistanceToOut, for the torus bar."""
     assert_exact(res["contains"], want["contains"], f"{what} Contains")
     assert_exact(res["inside"], want["inside"], f"{what} Inside")
-    for k in ("safety_to_in", "safety_to_out", "distance_to_in", "distance_to_out"):
+    for k in ("safety_to_in", "safety_to_out"):
+        assert_distances(res[k], want[k], f"{what} {k}")
+    if spec is not None and spec.kind == "torus":
+        assert_torus_distances(res["distance_to_in"], want["distance_to_in"], spec.params,
+                               what=f"{what} distance_to_in")
+        assert_torus_distances(res["distance_to_out"], want["distance_to_out"], spec.params,
+                               *local, what=f"{what} distance_to_out")
+        return
+    for k in ("distance_to_in", "distance_to_out"):
         assert_distances(res[k], want[k], f"{what} {k}")
 
 
@@ -97,7 +107,8 @@ def test_golden_parity(path, on_device):
     res = run_all_ops(pv, (d["mx"], d["my"], d["mz"]), (d["mdx"], d["mdy"], d["mdz"]),
                       (d["lx"], d["ly"], d["lz"]), (d["ldx"], d["ldy"], d["ldz"]), d["step"],
                       on_device)
-    check_against(res, d, os.path.basename(path))
+    check_against(res, d, os.path.basename(path), spec,
+                  ((d["lx"], d["ly"], d["lz"]), (d["ldx"], d["ldy"], d["ldz"])))
 
 
 @pytest.mark.parametrize("kind", sorted(VGB_SHAPES))
@@ -113,7 +124,7 @@ def test_large_seeded_vs_reference(kind):
     dirs = (wl.dx, wl.dy, wl.dz)
     res = run_all_ops(pv, pts, dirs, pts, dirs, wl.step)
     want = reference_outputs(spec, "generic", pts, dirs, wl.step)
-    check_against(res, want, kind)
+    check_against(res, want, kind, spec, (pts, dirs))
 
 
 def reference_outputs(spec, placement, pts, dirs, step):

@@ -8,8 +8,6 @@
 // which make a device virtual call per point, with shape and op resolved at
 // compile time.
 #pragma once
-#include <type_traits>
-
 #include "shapes.cuh"
 
 namespace vgb {
@@ -39,21 +37,6 @@ struct FusedIO {
 };
 
 template <class T> VGB_D T ldg(const T *p) { return __ldg(p); }
-
-// Shapes whose reference DistanceToIn moves the direction with the point
-// transform (TorusImplementation.h:906) declare kDirectionAsPoint.
-template <class Ops, class = void> struct DirAsPoint : std::false_type {};
-template <class Ops>
-struct DirAsPoint<Ops, std::void_t<decltype(Ops::kDirectionAsPoint)>>
-    : std::integral_constant<bool, Ops::kDirectionAsPoint> {};
-
-template <class Ops, class R>
-VGB_HD V3<R> dti_dir(const DXform &X, const V3<R> &d) {
-  if constexpr (DirAsPoint<Ops>::value)
-    return xf_point(X, d);
-  else
-    return xf_dir(X, d);
-}
 
 template <class Ops, class P, int OP>
 __device__ __forceinline__ void batch_point(const P &prm, const DXform &X, const BatchIO &io,

@@ -56,12 +56,30 @@ static vgb_status launch_fused(const P &prm, const DXform &X, const FusedIO &io,
   return VGB_OK;
 }
 
+// Boolean subtraction: compile-time components for the common pairs, the
+// switch over primitive shapes for every other pair.
+template <class F> static vgb_status with_boolean_ops(const BooleanP &b, F &&f) {
+  const int lt = b.left.type, rt = b.right.type;
+  if (lt == VGB_SHAPE_BOX && rt == VGB_SHAPE_TUBE) return f(BoolSubBoxTube<double>{});
+  if (lt == VGB_SHAPE_BOX && rt == VGB_SHAPE_BOX) return f(BoolSubBoxBox<double>{});
+  return f(BoolSubOps<double>{});
+}
+
+static BooleanP boolean_params(const vgb_geometry *g, int32_t unplaced) {
+  return bind_params(*static_cast<const BooleanP *>(shape_params(g, unplaced)),
+                     shape_params_dev(g, unplaced));
+}
+
 vgb_status launch_batch_f64(const vgb_geometry *g, int32_t placed, int op, const BatchIO &io,
                             cudaStream_t s) {
   const PlacedRec &pr = g->placed[placed];
   const DXform &X = g->xforms[pr.xform];
   const int type = g->unplaced[pr.unplaced].type;
   const void *prm = shape_params(g, pr.unplaced);
+  if (type == VGB_SHAPE_BOOLEAN) {
+    const BooleanP b = boolean_params(g, pr.unplaced);
+    return with_boolean_ops(b, [&](auto o) { return launch_ops<decltype(o)>(b, X, op, io, s); });
+  }
   switch (type) {
 #define VGB_SHAPE_CASE(TYPE, OPS, P) \
   case TYPE:                         \
@@ -80,6 +98,10 @@ vgb_status launch_fused_f64(const vgb_geometry *g, int32_t placed, const FusedIO
   const DXform &X = g->xforms[pr.xform];
   const int type = g->unplaced[pr.unplaced].type;
   const void *prm = shape_params(g, pr.unplaced);
+  if (type == VGB_SHAPE_BOOLEAN) {
+    const BooleanP b = boolean_params(g, pr.unplaced);
+    return with_boolean_ops(b, [&](auto o) { return launch_fused<decltype(o)>(b, X, io, s); });
+  }
   switch (type) {
 #define VGB_SHAPE_CASE(TYPE, OPS, P) \
   case TYPE:                         \

@@ -66,7 +66,7 @@ static void set_codes(RawXform &x) {
 // The effective device transform of one placement.  generic_only mirrors
 // shapes whose placed volumes always take Transform<kGeneric,kGeneric>
 // (source/UnplacedPolyhedron.cpp:321-333).
-static DXform effective(const RawXform &x, bool generic_only) {
+DXform effective_xform(const RawXform &x, bool generic_only) {
   DXform d;
   std::memset(&d, 0, sizeof(d));
   const int tcode = generic_only ? -1 : x.trans_code;
@@ -239,9 +239,10 @@ vgb_status vgb_place(vgb_geometry *g, int32_t logical, int32_t transformation,
   p.logical = logical;
   p.unplaced = g->logicals[logical].unplaced;
   p.xform = (int32_t)g->xforms.size();
-  p.pad = 0;
+  p.raw_xform = transformation;
   const int type = g->unplaced[p.unplaced].type;
-  g->xforms.push_back(effective(g->raw_xforms[transformation], type == VGB_SHAPE_POLYHEDRON));
+  g->xforms.push_back(
+      effective_xform(g->raw_xforms[transformation], type == VGB_SHAPE_POLYHEDRON));
   g->placed.push_back(p);
   if (placed) *placed = (int32_t)g->placed.size() - 1;
   return VGB_OK;

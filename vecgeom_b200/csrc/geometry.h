@@ -33,8 +33,8 @@ struct UnplacedRec {
 struct PlacedRec {
   int32_t unplaced;
   int32_t logical;
-  int32_t xform;
-  int32_t pad;
+  int32_t xform;      // index of the placement's effective DXform
+  int32_t raw_xform;  // the Transformation3D it was placed with
 };
 
 struct LogicalRec {
@@ -90,6 +90,9 @@ namespace vgb {
 vgb_status set_error(vgb_status s, const char *fmt, ...);
 vgb_status cuda_error(cudaError_t e, const char *what);
 void count_launch(int n = 1);
+// The device transform of a placement: the specialised form the reference
+// picks for it, or Transform<kGeneric,kGeneric> when generic_only is set.
+DXform effective_xform(const RawXform &x, bool generic_only);
 // Appends a shape record to the parameter pool (16-byte aligned).
 vgb_status add_unplaced(vgb_geometry *g, int type, const void *rec, size_t bytes, int32_t extra,
                         int32_t *id);

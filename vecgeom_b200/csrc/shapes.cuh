@@ -1,5 +1,7 @@
 // shapes.cuh -- every shape's parameter record and device arithmetic.
 #pragma once
+#include <type_traits>
+
 #include "../../include/vgb.h"
 #include "box.cuh"
 #include "tube.cuh"
@@ -11,17 +13,6 @@
 #include "polyhedron.cuh"
 
 struct vgb_geometry;
-
-// (type, ops template, parameter record) of every shape with batch kernels
-#define VGB_FOR_EACH_SHAPE(X)                                 \
-  X(VGB_SHAPE_BOX, vgb::BoxOps, vgb::BoxP)                    \
-  X(VGB_SHAPE_TUBE, vgb::TubeOps, vgb::TubeP)                 \
-  X(VGB_SHAPE_CONE, vgb::ConeOps, vgb::ConeP)                 \
-  X(VGB_SHAPE_SPHERE, vgb::SphereOps, vgb::SphereP)           \
-  X(VGB_SHAPE_TRD, vgb::TrdOps, vgb::TrdP)                    \
-  X(VGB_SHAPE_TORUS, vgb::TorusOps, vgb::TorusP)              \
-  X(VGB_SHAPE_POLYCONE, vgb::PolyconeOps, vgb::PolyconeP)    \
-  X(VGB_SHAPE_POLYHEDRON, vgb::PolyhedronOps, vgb::PolyhedronP)
 
 namespace vgb {
 
@@ -38,6 +29,36 @@ VGB_HD PolyhedronP bind_params(PolyhedronP p, const double *rec) {
   return p;
 }
 
+// Shapes whose reference DistanceToIn moves the direction with the point
+// transform (TorusImplementation.h:906) declare kDirectionAsPoint.
+template <class Ops, class = void> struct DirAsPoint : std::false_type {};
+template <class Ops>
+struct DirAsPoint<Ops, std::void_t<decltype(Ops::kDirectionAsPoint)>>
+    : std::integral_constant<bool, Ops::kDirectionAsPoint> {};
+
+template <class Ops, class R>
+VGB_HD V3<R> dti_dir(const DXform &X, const V3<R> &d) {
+  if constexpr (DirAsPoint<Ops>::value)
+    return xf_point(X, d);
+  else
+    return xf_dir(X, d);
+}
+
+}  // namespace vgb
+
+#include "boolean.cuh"
+
+namespace vgb {
+VGB_HD BooleanP bind_params(BooleanP p, const double *rec) {
+  p.base = rec;
+  return p;
+}
+
 // Called by vgb_geometry_close() once the device parameter pool is allocated.
 vgb_status finalize_shapes(vgb_geometry *g);
 }  // namespace vgb
+
+// (type, ops template, parameter record) of every shape with batch kernels
+#define VGB_FOR_EACH_SHAPE(X)                                 \
+  VGB_FOR_EACH_PRIMITIVE(X)                                   \
+  X(VGB_SHAPE_BOOLEAN, vgb::BoolSubOps, vgb::BooleanP)

@@ -591,10 +591,40 @@ vgb_status vgb_unplaced_tube(vgb_geometry *g, double rmin, double rmax, double d
 // ---------------------------------------------------------------------------
 // shapes not yet uploaded by this build report VGB_ENOTSUP
 // ---------------------------------------------------------------------------
-#define VGB_NOTYET(name) return set_error(VGB_ENOTSUP, name ": shape not available yet")
-vgb_status vgb_unplaced_boolean(vgb_geometry *, int32_t, int32_t, int32_t, int32_t *) {
-  VGB_NOTYET("vgb_unplaced_boolean");
+// UnplacedBooleanVolume(op, left, right) (volumes/UnplacedBooleanVolume.h:46-51):
+// the components are placed volumes whose transforms and shape records the
+// boolean record carries (offsets relative to the record, since the pool
+// moves to the device as one block).
+vgb_status vgb_unplaced_boolean(vgb_geometry *g, int32_t op, int32_t left_placed,
+                                int32_t right_placed, int32_t *id) {
+  VGB_CHECK_OPEN(g);
+  if (op != VGB_BOOL_SUBTRACTION)
+    return set_error(VGB_ENOTSUP, "vgb_unplaced_boolean: only subtraction (op %d) is available",
+                     (int)VGB_BOOL_SUBTRACTION);
+  const int32_t np = (int32_t)g->placed.size();
+  if (left_placed < 0 || left_placed >= np || right_placed < 0 || right_placed >= np)
+    return set_error(VGB_EINVAL, "vgb_unplaced_boolean: unknown placed volume");
+  const PlacedRec &pl = g->placed[left_placed], &pr = g->placed[right_placed];
+  const int lt = g->unplaced[pl.unplaced].type, rt = g->unplaced[pr.unplaced].type;
+  if (lt == VGB_SHAPE_BOOLEAN || rt == VGB_SHAPE_BOOLEAN)
+    return set_error(VGB_ENOTSUP, "vgb_unplaced_boolean: components must be primitive shapes");
+  BooleanP b;
+  std::memset(&b, 0, sizeof(b));
+  b.op = op;
+  b.left.xf = g->xforms[pl.xform];
+  b.left.type = lt;
+  b.right.xf = g->xforms[pr.xform];
+  b.right.type = rt;
+  b.right_generic = effective_xform(g->raw_xforms[pr.raw_xform], true);
+  int32_t uid = -1;
+  vgb_status s = add_unplaced(g, VGB_SHAPE_BOOLEAN, &b, sizeof(b), left_placed, &uid);
+  if (s != VGB_OK) return s;
+  const int32_t off = g->unplaced[uid].param_off;
+  BooleanP *rec = reinterpret_cast<BooleanP *>(g->params.data() + off);
+  rec->left.rec_off = g->unplaced[pl.unplaced].param_off - off;
+  rec->right.rec_off = g->unplaced[pr.unplaced].param_off - off;
+  if (id) *id = uid;
+  return VGB_OK;
 }
-#undef VGB_NOTYET
 
 }  // extern "C"

@@ -13,9 +13,11 @@
 #ifdef __CUDACC__
 #define VGB_HD __host__ __device__ __forceinline__
 #define VGB_D __device__ __forceinline__
+#define VGB_HD_NOINLINE inline __host__ __device__ __noinline__
 #else
 #define VGB_HD inline
 #define VGB_D inline
+#define VGB_HD_NOINLINE inline __attribute__((noinline))
 #endif
 
 namespace vgb {
@@ -40,10 +42,12 @@ template <class R> struct Lim;
 template <> struct Lim<double> {
   static VGB_HD double inf() { return HUGE_VAL; }
   static VGB_HD double minimum() { return DBL_MIN; }
+  static VGB_HD double quiet_nan() { return (double)NAN; }
 };
 template <> struct Lim<float> {
   static VGB_HD float inf() { return HUGE_VALF; }
   static VGB_HD float minimum() { return FLT_MIN; }
+  static VGB_HD float quiet_nan() { return NAN; }
 };
 
 // Min/Max of the reference Scalar backend (backend/scalar/Backend.h:146-163) are

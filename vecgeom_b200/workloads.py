@@ -169,16 +169,49 @@ def polyhedron_spec(phi_start_deg, phi_delta_deg, sides, z, rmin, rmax) -> Shape
                      (R, R, 0.5 * (z[-1] - z[0])), center=(0., 0., zc), contains=contains)
 
 
-def boolsub_spec(box_half, tube_rmax, tube_dz) -> ShapeSpec:
-    """Box minus a full solid tube, both at the origin."""
+def euler_rotation(phi, theta, psi) -> np.ndarray:
+    """Row-major rotation of Transformation3D(tx,ty,tz, phi,theta,psi), angles in
+    degrees (source/Transformation3D.cpp:93-114).  The master-to-local transform
+    is local = R^T (master - t)."""
+    d = math.pi / 180.
+    sf, cf = math.sin(d * phi), math.cos(d * phi)
+    st, ct = math.sin(d * theta), math.cos(d * theta)
+    sp, cp = math.sin(d * psi), math.cos(d * psi)
+    return np.array([[cp * cf - ct * sf * sp, -sp * cf - ct * sf * cp, st * sf],
+                     [cp * sf + ct * cf * sp, -sp * sf + ct * cf * cp, -st * cf],
+                     [sp * st, cp * st, ct]])
+
+
+def to_local(place, x, y, z):
+    """Mother-frame points in the frame of a placement (tx,ty,tz,phi,theta,psi)."""
+    R = euler_rotation(*place[3:])
+    a = np.stack([np.asarray(x) - place[0], np.asarray(y) - place[1], np.asarray(z) - place[2]])
+    loc = R.T @ a.reshape(3, -1)
+    return (loc[0].reshape(np.shape(x)), loc[1].reshape(np.shape(x)), loc[2].reshape(np.shape(x)))
+
+
+IDENTITY_PLACE = (0., 0., 0., 0., 0., 0.)
+
+
+def boolsub_spec(box_half, tube_rmax, tube_dz, left_place=IDENTITY_PLACE,
+                 right_place=IDENTITY_PLACE) -> ShapeSpec:
+    """Box minus a full solid tube, each component at its own placement
+    (tx,ty,tz, Euler phi,theta,psi in degrees) in the boolean's frame."""
     bx, by, bz = box_half
 
     def contains(x, y, z):
-        inbox = (np.abs(x) <= bx) & (np.abs(y) <= by) & (np.abs(z) <= bz)
-        intube = (x * x + y * y <= tube_rmax * tube_rmax) & (np.abs(z) <= tube_dz)
+        lx, ly, lz = to_local(left_place, x, y, z)
+        inbox = (np.abs(lx) <= bx) & (np.abs(ly) <= by) & (np.abs(lz) <= bz)
+        rx, ry, rz = to_local(right_place, x, y, z)
+        intube = (rx * rx + ry * ry <= tube_rmax * tube_rmax) & (np.abs(rz) <= tube_dz)
         return inbox & ~intube
-    return ShapeSpec("boolsub", dict(box_half=box_half, tube_rmax=tube_rmax, tube_dz=tube_dz),
-                     (bx, by, bz), contains=contains)
+    params = dict(box_half=box_half, tube_rmax=tube_rmax, tube_dz=tube_dz)
+    extent = (bx, by, bz)
+    if tuple(left_place) != IDENTITY_PLACE or tuple(right_place) != IDENTITY_PLACE:
+        params.update(left_place=list(left_place), right_place=list(right_place))
+        e = float(np.linalg.norm(box_half)) + float(np.linalg.norm(left_place[:3]))
+        extent = (e, e, e)
+    return ShapeSpec("boolsub", params, extent, contains=contains)
 
 
 # ---------------------------------------------------------------------------
@@ -324,7 +357,7 @@ def build_unplaced(geom, spec: ShapeSpec) -> int:
         lb = geom.LogicalVolume("sub_box", geom.UnplacedBox(bx, by, bz))
         lt = geom.LogicalVolume("sub_tube", geom.UnplacedTube(0., p["tube_rmax"], p["tube_dz"],
                                                               0., 2 * math.pi))
-        left = lb.Place(geom.Transformation3D())
-        right = lt.Place(geom.Transformation3D())
+        left = lb.Place(geom.Transformation3D(*p.get("left_place", IDENTITY_PLACE)))
+        right = lt.Place(geom.Transformation3D(*p.get("right_place", IDENTITY_PLACE)))
         return geom.UnplacedBooleanVolume(2, left, right)
     raise ValueError(k)
