@@ -212,6 +212,70 @@ vgb_status vgb_batch_fused(const vgb_geometry *g, int32_t placed, uint32_t ops, 
                            const double *dy, const double *dz, const double *step_max,
                            void *const *outs, uint32_t flags, int32_t precision, void *stream);
 
+/* ---------------------------------------------------------------------------
+ * Navigation (navigation/SimpleNavigator.h, NavigationState.h, NavStatePool.h).
+ *
+ * A pool holds n NavigationStates in device memory in the reference's field
+ * layout (navigation/NavigationState.h:45-66): int32 level at byte 0, onBoundary
+ * at byte 4, the {selfAlloc:1, N:31} word at byte 8 and N = max_depth + 1 path
+ * slots of 8 bytes from byte 16; the stride is 16 + 8 N bytes (56 at depth 4).
+ * A slot holds the placed-volume id (int64, -1 when empty) where the reference
+ * holds a VPlacedVolume pointer, which is the translation the reference makes
+ * when it copies a pool to the GPU (NavStatePool::CopyToGpu,
+ * navigation/NavStatePool.h:110-152).
+ *
+ * The navigation calls take device pointers and are asynchronous on `stream`.
+ * A track whose path would exceed 16 levels is not stepped; such tracks raise
+ * VGB_NAV_ERR_DEPTH in the geometry's navigation flags, which
+ * vgb_nav_error_flags() returns (after synchronising the device) and clears.
+ * ------------------------------------------------------------------------- */
+typedef struct vgb_navpool vgb_navpool;
+enum { VGB_NAV_ERR_DEPTH = 1 };
+
+/* NavStatePool(size, depth) (navigation/NavStatePool.h:46-60) for a closed geometry */
+vgb_status vgb_navpool_create(const vgb_geometry *g, int64_t n, vgb_navpool **pool);
+vgb_status vgb_navpool_destroy(vgb_navpool *pool);
+/* device address, state stride in bytes and capacity */
+vgb_status vgb_navpool_info(const vgb_navpool *pool, void **device, int64_t *stride, int64_t *n);
+/* NavStatePool::CopyToGpu / CopyFromGpu (:110-152): n states from / to a host
+ * buffer in the same layout (slots hold placed-volume ids) */
+vgb_status vgb_navpool_upload(vgb_navpool *pool, const void *host, int64_t n, void *stream);
+vgb_status vgb_navpool_download(const vgb_navpool *pool, void *host, int64_t n, void *stream);
+
+/* SimpleNavigator::LocatePoint(world, point, state, true)
+ * (navigation/SimpleNavigator.h:204-240) for n global points into states[0..n) */
+vgb_status vgb_nav_locate(const vgb_geometry *g, int64_t n, const double *x, const double *y,
+                          const double *z, vgb_navpool *states, void *stream);
+
+/* SimpleNavigator::FindNextBoundaryAndStep (:340-470) for n tracks: global
+ * points and directions, current states `cur`, proposed steps pstep[i]; writes
+ * the new states into `next` and the steps into step[i].  If safety is not
+ * NULL, safety[i] receives SimpleNavigator::GetSafety (:572-596) at the point
+ * in the current state.  cur and next must be different pools. */
+vgb_status vgb_nav_find_next_boundary_and_step(const vgb_geometry *g, int64_t n, const double *x,
+                                               const double *y, const double *z,
+                                               const double *dx, const double *dy,
+                                               const double *dz, const vgb_navpool *cur,
+                                               vgb_navpool *next, const double *pstep,
+                                               double *step, double *safety, void *stream);
+
+/* Transport of n straight tracks from their start points to the world exit:
+ * LocatePoint from the world, then per step GetSafety, FindNextBoundaryAndStep
+ * and point += direction * step, until the state is outside or max_steps steps
+ * were taken.  Per track i and step k < nsteps[i] (records at i * max_steps + k):
+ * next_ids = placed id of the new state's Top() (-1 once outside), steps, and
+ * safeties (at the step's start point).  next_ids, steps and safeties may be
+ * NULL; nsteps may not.  A client loop over the reference's calls (which
+ * source/benchmarking/NavigationBenchmarker.cpp:48-110 times one step at a time);
+ * it has no counterpart of its own in the reference. */
+vgb_status vgb_nav_trace(const vgb_geometry *g, int64_t n, const double *x, const double *y,
+                         const double *z, const double *dx, const double *dy, const double *dz,
+                         double pstep, int32_t max_steps, int32_t *next_ids, double *steps,
+                         double *safeties, int32_t *nsteps, void *stream);
+
+/* Navigation error flags (VGB_NAV_ERR_*) raised since the last call; clears them. */
+vgb_status vgb_nav_error_flags(const vgb_geometry *g, uint32_t *flags);
+
 #ifdef __cplusplus
 }
 #endif

@@ -190,6 +190,61 @@ class RefLib:
         return out.view(np.uint8) if op == CONTAINS else out
 
 
+class RefBuilder:
+    """Detector-builder adapter over the reference (same methods as
+    vecgeom_b200.workloads.VgbBuilder), for building one geometry in both."""
+
+    def __init__(self, ref: RefLib):
+        self.ref = ref
+        self.L = ref.L
+
+    def box(self, dx, dy, dz):
+        return self.L.vgref_box(dx, dy, dz)
+
+    def tube(self, rmin, rmax, dz, sphi, dphi):
+        return self.L.vgref_tube(rmin, rmax, dz, sphi, dphi)
+
+    def trd(self, dx1, dx2, dy1, dy2, dz):
+        return self.L.vgref_trd(dx1, dx2, dy1, dy2, dz)
+
+    def transform(self, tx=0., ty=0., tz=0., phi=0., theta=0., psi=0.):
+        return self.L.vgref_transform_euler(tx, ty, tz, phi, theta, psi)
+
+    def logical(self, label, unplaced):
+        return self.L.vgref_logical(label.encode(), unplaced)
+
+    def place(self, logical, transform):
+        return self.L.vgref_place(logical, transform)
+
+    def place_daughter(self, mother, daughter, transform):
+        return self.L.vgref_place_daughter(mother, daughter, transform)
+
+    def set_world(self, placed):
+        self.L.vgref_set_world(placed)
+
+    def close(self):
+        self.L.vgref_close_geometry()
+
+    def ids(self, placed) -> np.ndarray:
+        return np.array([self.L.vgref_placed_id(p) for p in placed], np.int64)
+
+
+def ref_nav_trace(ref: RefLib, pts, dirs, pstep: float, max_steps: int, nthreads: int = 1):
+    """SimpleNavigator trace of the current reference world (see ref_driver.cpp):
+    returns (next reference ids, steps, safeties, nsteps), records per track
+    at i * max_steps."""
+    x, y, z = (np.ascontiguousarray(a, np.float64) for a in pts)
+    dx, dy, dz = (np.ascontiguousarray(a, np.float64) for a in dirs)
+    n = len(x)
+    ids = np.full(n * max_steps, -7, np.int32)
+    steps = np.zeros(n * max_steps)
+    saf = np.zeros(n * max_steps)
+    nst = np.zeros(n, np.int32)
+    ref.L.vgref_nav_trace(n, _p(x), _p(y), _p(z), _p(dx), _p(dy), _p(dz), pstep, max_steps,
+                          _p(ids), _p(steps), _p(saf), _p(nst), nthreads)
+    return ids, steps, saf, nst
+
+
 def ref_unplaced(ref: RefLib, spec):
     """Create spec's unplaced shape with the reference's own constructors."""
     import math

@@ -8,6 +8,7 @@
 // host results round like the device results (transcendentals aside).
 #include "../../vecgeom_b200/csrc/batch.cuh"
 #include "../../vecgeom_b200/csrc/geometry.h"
+#include "../../vecgeom_b200/csrc/navigation.cuh"
 
 using namespace vgb;
 
@@ -58,4 +59,42 @@ extern "C" int hc_batch(const vgb_geometry *g, int32_t placed, int32_t op, int64
   default:
     return -2;
   }
+}
+
+// The navigator of navigation.cuh with a single lane, over the host tables of an
+// (unclosed) geometry: the same loop as vgb_nav_trace's kernel.
+extern "C" int hc_nav_trace(vgb_geometry *g, int64_t n, const double *x, const double *y,
+                            const double *z, const double *dx, const double *dy,
+                            const double *dz, double pstep, int32_t max_steps, int32_t *next_ids,
+                            double *steps, double *safeties, int32_t *nsteps) {
+  if (prepare_tables(g) != VGB_OK) return -1;
+  const NavGeom G = {g->params.data(),   g->unplaced.data(), g->placed.data(),
+                     g->xforms.data(),   g->nav_raw.data(),  g->logicals.data(),
+                     g->daughters.data(), g->world,          g->max_depth};
+  using Nav = Navigator<OneLane, kNavMaskAll>;
+  for (int64_t i = 0; i < n; ++i) {
+    V3<double> p = {x[i], y[i], z[i]};
+    const V3<double> d = {dx[i], dy[i], dz[i]};
+    NavPath cur, nxt;
+    bool ok = Nav::locate_from_world(G, cur, p);
+    int32_t k = 0;
+    while (ok && cur.level > 0 && k < max_steps) {
+      const DXform m = nav_top_matrix(G, cur);
+      const V3<double> lp = xf_point(m, p);
+      const V3<double> ld = xf_dir(m, d);
+      const double sf = Nav::safety(G, cur, lp);
+      double st = 0.;
+      ok = Nav::step(G, cur, nxt, lp, ld, pstep, st);
+      if (!ok) break;
+      const int64_t r = i * (int64_t)max_steps + k;
+      next_ids[r] = nxt.top();
+      steps[r] = st;
+      safeties[r] = sf;
+      p = {p.x + d.x * st, p.y + d.y * st, p.z + d.z * st};
+      cur = nxt;
+      ++k;
+    }
+    nsteps[i] = ok ? k : -1;
+  }
+  return 0;
 }

@@ -84,7 +84,18 @@ SIGNATURES = {
     "vgb_DistanceToOut": (ctypes.c_int, [_vp, _i32, _i64] + [_vp] * 9),
     "vgb_SafetyToIn": (ctypes.c_int, [_vp, _i32, _i64, _vp, _vp, _vp, _vp, _vp]),
     "vgb_SafetyToOut": (ctypes.c_int, [_vp, _i32, _i64, _vp, _vp, _vp, _vp, _vp]),
+    "vgb_navpool_create": (ctypes.c_int, [_vp, _i64, ctypes.POINTER(_vp)]),
+    "vgb_navpool_destroy": (ctypes.c_int, [_vp]),
+    "vgb_navpool_info": (ctypes.c_int, [_vp, ctypes.POINTER(_vp), _pi64, _pi64]),
+    "vgb_navpool_upload": (ctypes.c_int, [_vp, _vp, _i64, _vp]),
+    "vgb_navpool_download": (ctypes.c_int, [_vp, _vp, _i64, _vp]),
+    "vgb_nav_locate": (ctypes.c_int, [_vp, _i64, _vp, _vp, _vp, _vp, _vp]),
+    "vgb_nav_find_next_boundary_and_step": (ctypes.c_int, [_vp, _i64] + [_vp] * 13),
+    "vgb_nav_trace": (ctypes.c_int, [_vp, _i64] + [_vp] * 6 + [_dbl, _i32] + [_vp] * 5),
+    "vgb_nav_error_flags": (ctypes.c_int, [_vp, ctypes.POINTER(_u32)]),
 }
+
+NAV_ERR_DEPTH = 1
 
 
 def lib():

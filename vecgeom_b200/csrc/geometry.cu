@@ -156,7 +156,10 @@ vgb_status vgb_geometry_destroy(vgb_geometry *g) {
     cudaGetDevice(&prev);
     cudaSetDevice(g->device);
     cudaFree(g->dev.params);
+    cudaFree(g->dev.unplaced);
     cudaFree(g->dev.xforms);
+    cudaFree(g->dev.raw);
+    cudaFree(g->dev.nav_flags);
     cudaFree(g->dev.placed);
     cudaFree(g->dev.logicals);
     cudaFree(g->dev.daughters);
@@ -269,8 +272,9 @@ vgb_status vgb_set_world(vgb_geometry *g, int32_t placed) {
   return VGB_OK;
 }
 
-vgb_status vgb_geometry_close(vgb_geometry *g) {
-  VGB_CHECK_OPEN(g);
+}  // extern "C"
+
+vgb_status vgb::prepare_tables(vgb_geometry *g) {
   // CSR of daughters in insertion order (source/LogicalVolume.cpp:84-102)
   g->daughters.clear();
   for (size_t l = 0; l < g->logicals.size(); ++l) {
@@ -283,6 +287,28 @@ vgb_status vgb_geometry_close(vgb_geometry *g) {
     if (g->max_depth < 0)
       return set_error(VGB_EINVAL, "vgb_geometry_close: volume tree deeper than 64 levels");
   }
+  g->nav_raw.resize(g->raw_xforms.size());
+  for (size_t i = 0; i < g->raw_xforms.size(); ++i) {
+    const RawXform &x = g->raw_xforms[i];
+    NavXform &n = g->nav_raw[i];
+    std::memset(&n, 0, sizeof(n));
+    for (int k = 0; k < 3; ++k) n.t[k] = x.t[k];
+    for (int k = 0; k < 9; ++k) n.r[k] = x.r[k];
+    const bool has_t = x.trans_code != 0, has_r = x.rot_code != 0x200;
+    n.flags = (has_t ? kNavHasTrans : 0u) | (has_r ? kNavHasRot : 0u) |
+              ((!has_t && !has_r) ? kNavIdentity : 0u);
+  }
+  g->type_mask = 0;
+  for (const UnplacedRec &u : g->unplaced) g->type_mask |= 1u << u.type;
+  return VGB_OK;
+}
+
+extern "C" {
+
+vgb_status vgb_geometry_close(vgb_geometry *g) {
+  VGB_CHECK_OPEN(g);
+  vgb_status s0 = prepare_tables(g);
+  if (s0 != VGB_OK) return s0;
   // shape records that hold device pointers are fixed up after the pool lands
   cudaError_t e = cudaGetDevice(&g->device);
   if (e != cudaSuccess) return cuda_error(e, "vgb_geometry_close: cudaGetDevice");
@@ -301,10 +327,16 @@ vgb_status vgb_geometry_close(vgb_geometry *g) {
       if (e != cudaSuccess) return cuda_error(e, "vgb_geometry_close: cudaMemcpy");
     }
   }
+  if ((s = upload(g->unplaced, &g->dev.unplaced, &g->dev.bytes)) != VGB_OK) return s;
   if ((s = upload(g->xforms, &g->dev.xforms, &g->dev.bytes)) != VGB_OK) return s;
+  if ((s = upload(g->nav_raw, &g->dev.raw, &g->dev.bytes)) != VGB_OK) return s;
   if ((s = upload(g->placed, &g->dev.placed, &g->dev.bytes)) != VGB_OK) return s;
   if ((s = upload(g->logicals, &g->dev.logicals, &g->dev.bytes)) != VGB_OK) return s;
   if ((s = upload(g->daughters, &g->dev.daughters, &g->dev.bytes)) != VGB_OK) return s;
+  {
+    const std::vector<uint32_t> zero(1, 0u);
+    if ((s = upload(zero, &g->dev.nav_flags, &g->dev.bytes)) != VGB_OK) return s;
+  }
   g->closed = true;
   return VGB_OK;
 }

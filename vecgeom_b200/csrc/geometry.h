@@ -51,12 +51,26 @@ struct RawXform {
   int rot_code;    // specialised code, 0x200 identity or -1 generic
 };
 
+// Transformation3D with its property flags, as the navigator composes it
+// (base/Transformation3D.h:674-743 MultiplyFromRight, :598-632 InverseTransform;
+// flags from SetProperties, source/Transformation3D.cpp:81-90).
+enum : uint32_t { kNavHasTrans = 1, kNavHasRot = 2, kNavIdentity = 4 };
+struct NavXform {
+  double t[3];
+  double r[9];
+  uint32_t flags;
+  uint32_t pad;
+};
+
 struct DeviceImage {
   double *params = nullptr;
+  UnplacedRec *unplaced = nullptr;
   DXform *xforms = nullptr;
+  NavXform *raw = nullptr;
   PlacedRec *placed = nullptr;
   LogicalRec *logicals = nullptr;
   int32_t *daughters = nullptr;
+  uint32_t *nav_flags = nullptr;  // navigation error bits (VGB_NAV_ERR_*)
   int64_t bytes = 0;
 };
 
@@ -72,6 +86,8 @@ struct vgb_geometry {
   std::vector<std::vector<int32_t>> logical_daughters;
   std::vector<vgb::PlacedRec> placed;
   std::vector<int32_t> daughters;
+  std::vector<vgb::NavXform> nav_raw;  // per Transformation3D, for the navigator
+  uint32_t type_mask = 0;              // bit t set when a shape of type t exists
   int32_t world = -1;
   int32_t max_depth = 0;
   bool closed = false;
@@ -93,6 +109,9 @@ void count_launch(int n = 1);
 // The device transform of a placement: the specialised form the reference
 // picks for it, or Transform<kGeneric,kGeneric> when generic_only is set.
 DXform effective_xform(const RawXform &x, bool generic_only);
+// Host tables derived at close: daughters CSR, depth, navigator transforms and
+// the shape-type mask.  No device work.
+vgb_status prepare_tables(vgb_geometry *g);
 // Appends a shape record to the parameter pool (16-byte aligned).
 vgb_status add_unplaced(vgb_geometry *g, int type, const void *rec, size_t bytes, int32_t extra,
                         int32_t *id);

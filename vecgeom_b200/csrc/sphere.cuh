@@ -80,7 +80,10 @@ template <class R> struct SphereOps {
     return (x * (R)s.cosCPhi + y * (R)s.sinCPhi) / rho >= (R)limit;
   }
 
-  static VGB_HD R dti_core(const SphereP &s, const V3<R> &p, const V3<R> &v, int depth) {
+  // Depth 1 is the re-entry after a long distance was split (:685-689); it
+  // does not split again.
+  template <int Depth>
+  static VGB_HD R dti_core(const SphereP &s, const V3<R> &p, const V3<R> &v) {
     const R inf = Lim<R>::inf();
     R snxt = inf;
     R tolSTheta = 0, tolETheta = 0;
@@ -120,11 +123,13 @@ template <class R> struct SphereOps {
       if (d2 >= 0) {
         sd = -pDotV3d - sqrt(d2);
         if (sd >= 0) {
-          if (sd > dRmax && depth == 0) {
-            // :685-689 split long distances and recompute
-            const R fTerm = sd - fmod(sd, dRmax);
-            const V3<R> q = {p.x + fTerm * v.x, p.y + fTerm * v.y, p.z + fTerm * v.z};
-            sd = fTerm + dti_core(s, q, v, 1);
+          if constexpr (Depth == 0) {
+            if (sd > dRmax) {
+              // :685-689 split long distances and recompute
+              const R fTerm = sd - fmod(sd, dRmax);
+              const V3<R> q = {p.x + fTerm * v.x, p.y + fTerm * v.y, p.z + fTerm * v.z};
+              sd = fTerm + dti_core<1>(s, q, v);
+            }
           }
           xi = p.x + sd * v.x;
           yi = p.y + sd * v.y;
@@ -415,7 +420,7 @@ template <class R> struct SphereOps {
   }
 
   static VGB_HD R distance_to_in(const SphereP &s, const V3<R> &p, const V3<R> &v, R) {
-    return dti_core(s, p, v, 0);
+    return dti_core<0>(s, p, v);
   }
 
   // ---- DistanceToOut: SphereImplementation.h:1267-1510 and its helpers -----

@@ -277,3 +277,102 @@ class Geometry:
         out = ctypes.c_int64()
         check(self.L.vgb_geometry_device_bytes(self.handle, ctypes.byref(out)))
         return out.value
+
+
+# ---------------------------------------------------------------------------
+# navigation (navigation/NavStatePool.h, navigation/SimpleNavigator.h)
+# ---------------------------------------------------------------------------
+def _stream(stream):
+    return stream.cuda_stream if hasattr(stream, "cuda_stream") else stream
+
+
+class NavStatePool:
+    """NavStatePool(size, depth) on the geometry's device (navigation/NavStatePool.h:46-60).
+
+    States keep the reference's field layout; ``to_numpy()`` returns them as a
+    structured array (level, onBoundary, header, path slots holding placed ids)."""
+
+    def __init__(self, geometry: "Geometry", n: int):
+        geometry._require_closed()
+        self.geometry = geometry
+        h = ctypes.c_void_p()
+        check(geometry.L.vgb_navpool_create(geometry.handle, n, ctypes.byref(h)))
+        self.handle = h
+        dev, stride, cap = ctypes.c_void_p(), ctypes.c_int64(), ctypes.c_int64()
+        check(geometry.L.vgb_navpool_info(h, ctypes.byref(dev), ctypes.byref(stride),
+                                          ctypes.byref(cap)))
+        self.stride = stride.value
+        self.n = cap.value
+        self.depth = geometry.getMaxDepth()
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h is not None:
+            self.geometry.L.vgb_navpool_destroy(h)
+            self.handle = None
+
+    def dtype(self) -> np.dtype:
+        return np.dtype({"names": ["level", "onBoundary", "header", "path"],
+                         "formats": ["<i4", "u1", "<u4", ("<i8", (self.depth + 1,))],
+                         "offsets": [0, 4, 8, 16], "itemsize": self.stride})
+
+    def to_numpy(self, n: int | None = None, stream=None) -> np.ndarray:
+        n = self.n if n is None else n
+        out = np.zeros(n, self.dtype())
+        check(self.geometry.L.vgb_navpool_download(self.handle, out.ctypes.data, n,
+                                                   _stream(stream)))
+        return out
+
+    def from_numpy(self, states: np.ndarray, stream=None) -> None:
+        states = np.ascontiguousarray(states, self.dtype())
+        check(self.geometry.L.vgb_navpool_upload(self.handle, states.ctypes.data, len(states),
+                                                 _stream(stream)))
+
+    def tops(self, n: int | None = None) -> np.ndarray:
+        """Placed id of Top() per state (-1 when outside)."""
+        st = self.to_numpy(n)
+        lvl = st["level"].astype(np.int64)
+        top = np.full(len(st), -1, np.int64)
+        ok = lvl > 0
+        top[ok] = st["path"][np.flatnonzero(ok), lvl[ok] - 1]
+        return top
+
+
+class SimpleNavigator:
+    """navigation/SimpleNavigator.h over device batches (torch CUDA tensors)."""
+
+    def __init__(self, geometry: "Geometry"):
+        geometry._require_closed()
+        self.geometry = geometry
+
+    def LocatePoint(self, points: SOA3D, states: NavStatePool, stream=None) -> None:
+        g = self.geometry
+        check(g.L.vgb_nav_locate(g.handle, points.size(), _addr(points.x), _addr(points.y),
+                                 _addr(points.z), states.handle, _stream(stream)))
+
+    def FindNextBoundaryAndStep(self, points: SOA3D, dirs: SOA3D, cur: NavStatePool,
+                                nxt: NavStatePool, pstep, step, safety=None,
+                                stream=None) -> None:
+        g = self.geometry
+        for a in (pstep, step, safety):
+            _check_dtype(a, "f8")
+        check(g.L.vgb_nav_find_next_boundary_and_step(
+            g.handle, points.size(), _addr(points.x), _addr(points.y), _addr(points.z),
+            _addr(dirs.x), _addr(dirs.y), _addr(dirs.z), cur.handle, nxt.handle, _addr(pstep),
+            _addr(step), _addr(safety), _stream(stream)))
+
+    def Trace(self, points: SOA3D, dirs: SOA3D, pstep: float, max_steps: int, nsteps,
+              next_ids=None, steps=None, safeties=None, stream=None) -> None:
+        """Steps every track to the world exit (see vgb_nav_trace)."""
+        g = self.geometry
+        _check_dtype(nsteps, "i4")
+        _check_dtype(next_ids, "i4")
+        check(g.L.vgb_nav_trace(
+            g.handle, points.size(), _addr(points.x), _addr(points.y), _addr(points.z),
+            _addr(dirs.x), _addr(dirs.y), _addr(dirs.z), float(pstep), int(max_steps),
+            _addr(next_ids), _addr(steps), _addr(safeties), _addr(nsteps), _stream(stream)))
+
+    def error_flags(self) -> int:
+        out = ctypes.c_uint32()
+        check(self.geometry.L.vgb_nav_error_flags(self.geometry.handle, ctypes.byref(out)))
+        return out.value

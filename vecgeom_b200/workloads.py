@@ -361,3 +361,117 @@ def build_unplaced(geom, spec: ShapeSpec) -> int:
         right = lt.Place(geom.Transformation3D(*p.get("right_place", IDENTITY_PLACE)))
         return geom.UnplacedBooleanVolume(2, left, right)
     raise ValueError(k)
+
+
+# ---------------------------------------------------------------------------
+# Layered cylindrical detector of the navigation benchmark
+# ---------------------------------------------------------------------------
+@dataclass
+class DetectorSpec:
+    """World box (half 2000 mm) with 10 concentric tube layers (inner radius
+    100 + 100 k mm, 20 mm thick, dz 1200 mm).  Layer k holds 64 + 48 k box
+    modules of half-lengths (10, 40, 600) mm at radius r_k + 10, each rotated
+    about z to face the axis (Euler phi = 360 j / N_k degrees).  Every module
+    holds 4 Trd sensors (dx 8 -> 6, dy 30 -> 25, dz 140 mm) at z = -450, -150,
+    150, 450 mm.  Every module has its own logical volume (all share one
+    unplaced box), so 1 + 10 + 2800 + 11200 = 14011 placed volumes, 4 levels.
+    (The modules overlap their neighbours and stick out of their layer at the
+    corners; navigation stays deterministic under the reference's rules.)"""
+    world_half: float = 2000.
+    n_layers: int = 10
+    r0: float = 100.
+    dr: float = 100.
+    thickness: float = 20.
+    layer_dz: float = 1200.
+    module_half: tuple = (10., 40., 600.)
+    modules0: int = 64
+    modules_step: int = 48
+    sensor_trd: tuple = (8., 6., 30., 25., 140.)
+    sensor_z: tuple = (-450., -150., 150., 450.)
+
+    def modules_in_layer(self, k: int) -> int:
+        return self.modules0 + self.modules_step * k
+
+    def placed_count(self) -> int:
+        nm = sum(self.modules_in_layer(k) for k in range(self.n_layers))
+        return 1 + self.n_layers + nm + nm * len(self.sensor_z)
+
+
+class VgbBuilder:
+    """Detector-builder adapter over this library's Geometry (close=False leaves
+    the geometry open, for host-only use of its tables)."""
+
+    def __init__(self, geom, close: bool = True):
+        self.g = geom
+        self._close = close
+
+    def box(self, dx, dy, dz):
+        return self.g.UnplacedBox(dx, dy, dz)
+
+    def tube(self, rmin, rmax, dz, sphi, dphi):
+        return self.g.UnplacedTube(rmin, rmax, dz, sphi, dphi)
+
+    def trd(self, dx1, dx2, dy1, dy2, dz):
+        return self.g.UnplacedTrd(dx1, dx2, dy1, dy2, dz)
+
+    def transform(self, tx=0., ty=0., tz=0., phi=0., theta=0., psi=0.):
+        return self.g.Transformation3D(tx, ty, tz, phi, theta, psi)
+
+    def logical(self, label, unplaced):
+        return self.g.LogicalVolume(label, unplaced)
+
+    def place(self, logical, transform):
+        return logical.Place(transform)
+
+    def place_daughter(self, mother, daughter, transform):
+        return mother.PlaceDaughter(daughter, transform)
+
+    def set_world(self, placed):
+        self.g.SetWorld(placed)
+
+    def close(self):
+        if self._close:
+            self.g.CloseGeometry()
+
+
+def build_detector(b, spec: DetectorSpec | None = None) -> list:
+    """Builds the detector through a builder adapter (this library's or the
+    reference's) in one fixed order; returns the placed volumes in creation
+    order, which is also the order of their ids."""
+    spec = spec or DetectorSpec()
+    placed = []
+    world_lv = b.logical("world", b.box(spec.world_half, spec.world_half, spec.world_half))
+    world = b.place(world_lv, b.transform())
+    placed.append(world)
+    module_box = b.box(*spec.module_half)
+    sensor_lv = b.logical("sensor", b.trd(*spec.sensor_trd))
+    sensor_t = [b.transform(0., 0., z) for z in spec.sensor_z]
+    for k in range(spec.n_layers):
+        rin = spec.r0 + spec.dr * k
+        layer_lv = b.logical(f"layer{k}", b.tube(rin, rin + spec.thickness, spec.layer_dz, 0.,
+                                                 2 * math.pi))
+        nk = spec.modules_in_layer(k)
+        rc = rin + 0.5 * spec.thickness
+        for j in range(nk):
+            module_lv = b.logical(f"module{k}_{j}", module_box)
+            for t in sensor_t:
+                placed.append(b.place_daughter(module_lv, sensor_lv, t))
+            phi = 360. * j / nk
+            a = math.radians(phi)
+            placed.append(b.place_daughter(layer_lv, module_lv,
+                                           b.transform(rc * math.cos(a), rc * math.sin(a), 0.,
+                                                       phi, 0., 0.)))
+        placed.append(b.place_daughter(world_lv, layer_lv, b.transform()))
+    b.set_world(world)
+    b.close()
+    return placed
+
+
+def isotropic_tracks(n: int, seed: int):
+    """n tracks from the origin with isotropic unit directions (normalised 3-D
+    Gaussians)."""
+    rng = np.random.default_rng(seed)
+    v = rng.normal(size=(3, n))
+    v /= np.linalg.norm(v, axis=0)
+    z = np.zeros(n)
+    return (z.copy(), z.copy(), z.copy()), (v[0].copy(), v[1].copy(), v[2].copy())
