@@ -39,6 +39,23 @@ def test_python_signatures_cover_header():
     assert not missing, f"no ctypes signature for {missing}"
 
 
+def declared_arity():
+    """Number of parameters of every vgb_* function declared in include/*.h."""
+    out = {}
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        src = re.sub(r"/\*.*?\*/", "", open(h).read(), flags=re.S)
+        for m in re.finditer(r"\b(vgb_\w+)\s*\(([^;{]*?)\)\s*;", src, flags=re.S):
+            args = m.group(2).strip()
+            out[m.group(1)] = 0 if args in ("", "void") else args.count(",") + 1
+    return out
+
+
+def test_python_signatures_match_header_arity():
+    bad = {n: (k, len(_lib.SIGNATURES[n][1])) for n, k in declared_arity().items()
+           if n in _lib.SIGNATURES and len(_lib.SIGNATURES[n][1]) != k}
+    assert not bad, f"argument counts (header, ctypes) differ: {bad}"
+
+
 def test_errors_are_statuses_not_aborts():
     L = vecgeom_b200.lib()
     assert L.vgb_geometry_create(None) == _lib.EINVAL
@@ -55,3 +72,43 @@ def test_errors_are_statuses_not_aborts():
     pts = vecgeom_b200.SOA3D(np.zeros(4), np.zeros(4), np.zeros(4))
     with pytest.raises(vecgeom_b200.VgbError, match="not closed"):
         pv.Inside(pts, np.zeros(4, np.int32))
+
+
+def test_cpp_facade_compiles_and_links(tmp_path):
+    """include/vecgeom_b200.hpp (the VPlacedVolume/SOA3D facade) compiles with the
+    reference's call shapes and links against libvgb.so."""
+    import subprocess
+    src = tmp_path / "facade.cpp"
+    src.write_text(r'''
+#include "vecgeom_b200.hpp"
+#include <cstdio>
+using namespace vecgeom_b200;
+int main(int argc, char **) {
+  static_assert(sizeof(SOA3D<double>) == 48, "SOA3D member layout");
+  if (argc > 5) {  // never taken: the calls only have to compile and link
+    Geometry g;
+    VPlacedVolume pv = g.Place(g.LogicalVolume("b", g.UnplacedBox(1, 2, 3)), g.Transformation3D());
+    double x[1] = {0}, out[1];
+    SOA3D<double> p(x, x, x, 1);
+    bool c[1];
+    int in[1], ids[1];
+    pv.Contains(p, c);
+    pv.Inside(p, in);
+    pv.DistanceToIn(p, p, x, out);
+    pv.DistanceToInMinimize(p, p, 3, out, ids);
+    pv.DistanceToOut(p, p, x, out);
+    pv.DistanceToOut(p, p, x, out, ids);
+    pv.SafetyToIn(p, out);
+    pv.SafetyToInMinimize(p, out);
+    pv.SafetyToOut(p, out);
+    pv.SafetyToOutMinimize(p, out);
+  }
+  std::puts("ok");
+  return 0;
+}
+''')
+    exe = tmp_path / "facade"
+    lib = os.path.join(ROOT, "vecgeom_b200", "lib")
+    subprocess.run(["g++", "-std=c++17", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"),
+                    str(src), "-o", str(exe), "-L", lib, "-lvgb", f"-Wl,-rpath,{lib}",
+                    "-Wl,--unresolved-symbols=ignore-in-shared-libs"], check=True)

@@ -90,7 +90,7 @@ SIGNATURES = {
     "vgb_navpool_upload": (ctypes.c_int, [_vp, _vp, _i64, _vp]),
     "vgb_navpool_download": (ctypes.c_int, [_vp, _vp, _i64, _vp]),
     "vgb_nav_locate": (ctypes.c_int, [_vp, _i64, _vp, _vp, _vp, _vp, _vp]),
-    "vgb_nav_find_next_boundary_and_step": (ctypes.c_int, [_vp, _i64] + [_vp] * 13),
+    "vgb_nav_find_next_boundary_and_step": (ctypes.c_int, [_vp, _i64] + [_vp] * 12),
     "vgb_nav_trace": (ctypes.c_int, [_vp, _i64] + [_vp] * 6 + [_dbl, _i32] + [_vp] * 5),
     "vgb_nav_error_flags": (ctypes.c_int, [_vp, ctypes.POINTER(_u32)]),
 }
