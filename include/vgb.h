@@ -213,6 +213,63 @@ vgb_status vgb_batch_fused(const vgb_geometry *g, int32_t placed, uint32_t ops, 
                            void *const *outs, uint32_t flags, int32_t precision, void *stream);
 
 /* ---------------------------------------------------------------------------
+ * Baskets: many placed volumes (of any shapes) and their point batches in one
+ * persistent launch.  The reference runs one SOA3D virtual call per volume and
+ * batch (volumes/PlacedVolume.h:145-250, the basket loops of
+ * SimpleNavigator.h:599-743); a plan packs all baskets into tiles of points that
+ * the CTAs of one launch take in turn, each tile belonging to one basket (one
+ * shape), so the shape dispatch is uniform per tile.
+ *
+ * The points of all baskets are concatenated: basket b owns [offset, offset +
+ * count) of x..dz, step_max and of every output array.  Each basket evaluates
+ * the ops of the plan's mask with vgb_batch_fused's semantics (outs[op]).
+ * ------------------------------------------------------------------------- */
+typedef struct {
+  int32_t placed; /* placed volume of this basket */
+  int32_t pad;
+  int64_t offset; /* first point of the basket in the concatenated arrays */
+  int64_t count;  /* number of points */
+} vgb_basket;
+
+typedef struct vgb_basket_plan vgb_basket_plan;
+
+/* Builds the tile table of nb baskets (host array) for the op mask `ops` (bits
+ * 1 << vgb_op over CONTAINS, INSIDE, DISTANCE_TO_IN, DISTANCE_TO_OUT,
+ * SAFETY_TO_IN, SAFETY_TO_OUT).  block = threads per CTA (128, 256 or 512) and
+ * tile = points per tile (a multiple of block); 0 picks the defaults (256,
+ * 1024) until vgb_basket_tune chooses. */
+vgb_status vgb_basket_plan_create(const vgb_geometry *g, const vgb_basket *baskets, int32_t nb,
+                                  uint32_t ops, int32_t block, int32_t tile,
+                                  vgb_basket_plan **plan);
+vgb_status vgb_basket_plan_destroy(vgb_basket_plan *plan);
+/* total points and tiles of the plan, and its current launch shape */
+vgb_status vgb_basket_plan_info(const vgb_basket_plan *plan, int64_t *points, int64_t *tiles,
+                                int32_t *block, int32_t *tile);
+
+/* One persistent launch over every basket of the plan (device pointers). */
+vgb_status vgb_basket_run(vgb_basket_plan *plan, const double *x, const double *y,
+                          const double *z, const double *dx, const double *dy, const double *dz,
+                          const double *step_max, void *const *outs, uint32_t flags,
+                          void *stream);
+
+/* Autotuner: times every (block, tile) candidate on these inputs (reps
+ * launches each, CUDA events on `stream`), keeps the fastest in the plan and
+ * returns it with its time per launch.  The outputs are overwritten. */
+vgb_status vgb_basket_tune(vgb_basket_plan *plan, const double *x, const double *y,
+                           const double *z, const double *dx, const double *dy, const double *dz,
+                           const double *step_max, void *const *outs, uint32_t flags, int32_t reps,
+                           void *stream, int32_t *best_block, int32_t *best_tile,
+                           float *best_ms);
+
+/* Captures vgb_basket_run with these pointers into a CUDA graph held by the
+ * plan; vgb_basket_graph_launch replays it on `stream`. */
+vgb_status vgb_basket_graph_capture(vgb_basket_plan *plan, const double *x, const double *y,
+                                    const double *z, const double *dx, const double *dy,
+                                    const double *dz, const double *step_max, void *const *outs,
+                                    uint32_t flags);
+vgb_status vgb_basket_graph_launch(vgb_basket_plan *plan, void *stream);
+
+/* ---------------------------------------------------------------------------
  * Navigation (navigation/SimpleNavigator.h, NavigationState.h, NavStatePool.h).
  *
  * A pool holds n NavigationStates in device memory in the reference's field

@@ -84,6 +84,15 @@ SIGNATURES = {
     "vgb_DistanceToOut": (ctypes.c_int, [_vp, _i32, _i64] + [_vp] * 9),
     "vgb_SafetyToIn": (ctypes.c_int, [_vp, _i32, _i64, _vp, _vp, _vp, _vp, _vp]),
     "vgb_SafetyToOut": (ctypes.c_int, [_vp, _i32, _i64, _vp, _vp, _vp, _vp, _vp]),
+    "vgb_basket_plan_create": (ctypes.c_int, [_vp, _vp, _i32, _u32, _i32, _i32,
+                                              ctypes.POINTER(_vp)]),
+    "vgb_basket_plan_destroy": (ctypes.c_int, [_vp]),
+    "vgb_basket_plan_info": (ctypes.c_int, [_vp, _pi64, _pi64, _pi32, _pi32]),
+    "vgb_basket_run": (ctypes.c_int, [_vp] + [_vp] * 8 + [_u32, _vp]),
+    "vgb_basket_tune": (ctypes.c_int, [_vp] + [_vp] * 8 + [_u32, _i32, _vp, _pi32, _pi32,
+                                                          ctypes.POINTER(ctypes.c_float)]),
+    "vgb_basket_graph_capture": (ctypes.c_int, [_vp] + [_vp] * 8 + [_u32]),
+    "vgb_basket_graph_launch": (ctypes.c_int, [_vp, _vp]),
     "vgb_navpool_create": (ctypes.c_int, [_vp, _i64, ctypes.POINTER(_vp)]),
     "vgb_navpool_destroy": (ctypes.c_int, [_vp]),
     "vgb_navpool_info": (ctypes.c_int, [_vp, ctypes.POINTER(_vp), _pi64, _pi64]),

@@ -1,0 +1,394 @@
+// baskets.cu -- many baskets (placed volume + its points) in one persistent launch,
+// the autotuner that picks its launch shape, and its CUDA-graph replay.
+//
+// A plan splits every basket into tiles of `tile` points; tile t belongs to the
+// basket found by a binary search over the per-basket tile prefix.  A CTA takes
+// tiles t = blockIdx.x, blockIdx.x + gridDim.x, ... (the grid is sized to the
+// resident CTAs of 148 SMs), stages the tile's shape record and transform in
+// shared memory (one broadcast read per tile instead of a parameter bank) and
+// runs the fused per-point ops of batch.cuh over the tile's points.  Each tile
+// holds one shape, so the shape switch is uniform across the CTA.
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "batch.cuh"
+#include "geometry.h"
+
+using namespace vgb;
+
+namespace vgb {
+namespace {
+
+struct BasketRec {
+  int32_t unplaced;
+  int32_t xform;
+  int64_t offset;
+  int64_t count;
+};
+
+struct BasketGeom {
+  const double *params;
+  const UnplacedRec *unplaced;
+  const DXform *xforms;
+};
+
+constexpr int kRecDoubles = 128;  // largest fixed shape record staged per tile (1 KB)
+
+template <class P> struct HasBase : std::false_type {};
+template <> struct HasBase<PolyconeP> : std::true_type {};
+template <> struct HasBase<PolyhedronP> : std::true_type {};
+template <> struct HasBase<BooleanP> : std::true_type {};
+
+template <class Ops, class P, int kBlock, uint32_t kOps>
+__device__ __forceinline__ void run_tile(const double *rec, const DXform *xg, int64_t first,
+                                         int64_t end, const FusedIO &io, double *srec,
+                                         DXform *sx) {
+  static_assert(sizeof(P) <= kRecDoubles * sizeof(double), "shape record too large to stage");
+  constexpr int nd = (int)((sizeof(P) + 7) / 8);
+  for (int k = threadIdx.x; k < nd; k += kBlock) srec[k] = rec[k];
+  if (threadIdx.x == 0) *sx = *xg;
+  __syncthreads();
+  P *sp = reinterpret_cast<P *>(srec);
+  if constexpr (HasBase<P>::value) {
+    if (threadIdx.x == 0) sp->base = rec;
+    __syncthreads();
+  }
+  const P &prm = *sp;
+  for (int64_t i = first + threadIdx.x; i < end; i += kBlock)
+    fused_point<Ops, P, kOps>(prm, *sx, io, i);
+  __syncthreads();  // the next tile overwrites the staged record
+}
+
+// Op sets with their own instantiation: DistanceToIn + SafetyToIn (the mixed
+// basket workload) and every fused op.
+constexpr uint32_t kOpsDtiSti = (1u << VGB_OP_DISTANCE_TO_IN) | (1u << VGB_OP_SAFETY_TO_IN);
+constexpr uint32_t kOpsAll = 0x3fu;
+
+template <int kBlock, uint32_t kOps>
+__global__ void __launch_bounds__(kBlock, 1)
+    k_baskets(const BasketGeom G, const BasketRec *__restrict__ baskets,
+              const int64_t *__restrict__ prefix, int32_t nb, int64_t ntiles, int32_t tile,
+              const FusedIO io) {
+  __shared__ __align__(16) double srec[kRecDoubles];
+  __shared__ DXform sx;
+  for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    int lo = 0, hi = nb;
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (prefix[mid] <= t) lo = mid; else hi = mid;
+    }
+    const BasketRec b = baskets[lo];
+    const int64_t first = b.offset + (t - prefix[lo]) * tile;
+    const int64_t last = b.offset + b.count;
+    const int64_t end = first + tile < last ? first + tile : last;
+    const UnplacedRec u = G.unplaced[b.unplaced];
+    const double *rec = G.params + u.param_off;
+    const DXform *xg = G.xforms + b.xform;
+    switch (u.type) {
+#define VGB_BASKET_CASE(T, OPS, P)                                                 \
+  case T:                                                                          \
+    run_tile<OPS<double>, P, kBlock, kOps>(rec, xg, first, end, io, srec, &sx);    \
+    break;
+      VGB_FOR_EACH_SHAPE(VGB_BASKET_CASE)
+#undef VGB_BASKET_CASE
+      default:
+        break;
+    }
+  }
+}
+
+template <uint32_t kOps> int occupancy_grid(int block) {
+  int dev = 0, sms = 148, per_sm = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaError_t e = cudaSuccess;
+  switch (block) {
+    case 128: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_baskets<128, kOps>, 128, 0); break;
+    case 256: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_baskets<256, kOps>, 256, 0); break;
+    default: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_baskets<512, kOps>, 512, 0); break;
+  }
+  if (e != cudaSuccess || per_sm < 1) {
+    cudaGetLastError();
+    per_sm = 1;
+  }
+  return sms * per_sm;
+}
+
+bool valid_shape(int block, int tile) {
+  return (block == 128 || block == 256 || block == 512) && tile >= block && tile % block == 0 &&
+         tile <= (1 << 16);
+}
+
+}  // namespace
+}  // namespace vgb
+
+struct vgb_basket_plan {
+  const vgb_geometry *g = nullptr;
+  int device = -1;
+  uint32_t ops = 0;
+  int32_t nb = 0;
+  int64_t points = 0;
+  std::vector<vgb::BasketRec> host;
+  vgb::BasketRec *d_baskets = nullptr;
+  int64_t *d_prefix = nullptr;  // nb + 1 tile prefix for the current tile size
+  int64_t ntiles = 0;
+  int32_t block = 256;
+  int32_t tile = 1024;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t graph_exec = nullptr;
+};
+
+namespace vgb {
+namespace {
+
+// Uploads the tile prefix for `tile` (stream-ordered; the host copy must live
+// until the copy ran, so it is synchronous).
+vgb_status set_tile(vgb_basket_plan *p, int32_t tile, cudaStream_t s) {
+  std::vector<int64_t> prefix(p->nb + 1, 0);
+  for (int b = 0; b < p->nb; ++b)
+    prefix[b + 1] = prefix[b] + (p->host[b].count + tile - 1) / tile;
+  cudaError_t e = cudaMemcpyAsync(p->d_prefix, prefix.data(), prefix.size() * sizeof(int64_t),
+                                  cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return cuda_error(e, "basket plan: tile prefix upload");
+  p->ntiles = prefix[p->nb];
+  p->tile = tile;
+  return VGB_OK;
+}
+
+FusedIO make_io(const vgb_basket_plan *p, const double *x, const double *y, const double *z,
+                const double *dx, const double *dy, const double *dz, const double *step,
+                void *const *outs, uint32_t flags) {
+  FusedIO io;
+  std::memset(&io, 0, sizeof(io));
+  io.x = x; io.y = y; io.z = z;
+  io.dx = dx; io.dy = dy; io.dz = dz;
+  io.step = step;
+  for (int k = 0; k < 6; ++k) io.out[k] = (p->ops >> k) & 1u ? outs[k] : nullptr;
+  io.n = p->points;
+  io.ops = p->ops;
+  io.flags = flags;
+  return io;
+}
+
+template <uint32_t kOps>
+void launch_k(const vgb_basket_plan *p, const FusedIO &io, cudaStream_t s) {
+  const BasketGeom G = {p->g->dev.params, p->g->dev.unplaced, p->g->dev.xforms};
+  const int64_t cap = occupancy_grid<kOps>(p->block);
+  const int grid = (int)std::min<int64_t>(p->ntiles, cap);
+  switch (p->block) {
+    case 128: k_baskets<128, kOps><<<grid, 128, 0, s>>>(G, p->d_baskets, p->d_prefix, p->nb, p->ntiles, p->tile, io); break;
+    case 256: k_baskets<256, kOps><<<grid, 256, 0, s>>>(G, p->d_baskets, p->d_prefix, p->nb, p->ntiles, p->tile, io); break;
+    default: k_baskets<512, kOps><<<grid, 512, 0, s>>>(G, p->d_baskets, p->d_prefix, p->nb, p->ntiles, p->tile, io); break;
+  }
+}
+
+vgb_status launch(const vgb_basket_plan *p, const FusedIO &io, cudaStream_t s) {
+  if (p->ntiles == 0) return VGB_OK;
+  if ((p->ops & ~kOpsDtiSti) == 0)
+    launch_k<kOpsDtiSti>(p, io, s);
+  else
+    launch_k<kOpsAll>(p, io, s);
+  count_launch();
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_error(e, "vgb_basket_run: kernel launch");
+  return VGB_OK;
+}
+
+vgb_status check_io(const vgb_basket_plan *p, const double *x, const double *y, const double *z,
+                    const double *dx, const double *dy, const double *dz, const double *step,
+                    void *const *outs, const char *fn) {
+  if (!p) return set_error(VGB_EINVAL, "%s: plan is NULL", fn);
+  if (!x || !y || !z) return set_error(VGB_EINVAL, "%s: points are NULL", fn);
+  const uint32_t dist = (1u << VGB_OP_DISTANCE_TO_IN) | (1u << VGB_OP_DISTANCE_TO_OUT);
+  if ((p->ops & dist) && (!dx || !dy || !dz || !step))
+    return set_error(VGB_EINVAL, "%s: distances need directions and step_max", fn);
+  if (!outs) return set_error(VGB_EINVAL, "%s: outs is NULL", fn);
+  for (int k = 0; k < 6; ++k)
+    if (((p->ops >> k) & 1u) && !outs[k])
+      return set_error(VGB_EINVAL, "%s: output of op %d is NULL", fn, k);
+  int dev = -1;
+  cudaGetDevice(&dev);
+  if (dev != p->device)
+    return set_error(VGB_EINVAL, "%s: current device %d is not the plan's device %d", fn, dev,
+                     p->device);
+  return VGB_OK;
+}
+
+}  // namespace
+}  // namespace vgb
+
+extern "C" {
+
+vgb_status vgb_basket_plan_create(const vgb_geometry *g, const vgb_basket *baskets, int32_t nb,
+                                  uint32_t ops, int32_t block, int32_t tile,
+                                  vgb_basket_plan **plan) {
+  if (!plan) return set_error(VGB_EINVAL, "vgb_basket_plan_create: plan is NULL");
+  *plan = nullptr;
+  if (!g || !g->closed) return set_error(VGB_EINVAL, "vgb_basket_plan_create: geometry not closed");
+  if (nb < 0 || (nb > 0 && !baskets))
+    return set_error(VGB_EINVAL, "vgb_basket_plan_create: bad basket array");
+  if (ops == 0 || (ops & ~0x3fu))
+    return set_error(VGB_EINVAL, "vgb_basket_plan_create: ops must be a mask over ops 0..5");
+  if (block == 0) block = 256;
+  if (tile == 0) tile = 1024;
+  if (!valid_shape(block, tile))
+    return set_error(VGB_EINVAL, "vgb_basket_plan_create: block %d / tile %d not supported", block,
+                     tile);
+  vgb_basket_plan *p = new vgb_basket_plan;
+  p->g = g;
+  p->device = g->device;
+  p->ops = ops;
+  p->nb = nb;
+  p->block = block;
+  p->host.resize(nb);
+  for (int b = 0; b < nb; ++b) {
+    const vgb_basket &k = baskets[b];
+    if (k.placed < 0 || k.placed >= (int32_t)g->placed.size() || k.offset < 0 || k.count < 0) {
+      delete p;
+      return set_error(VGB_EINVAL, "vgb_basket_plan_create: basket %d is invalid", b);
+    }
+    const PlacedRec &pr = g->placed[k.placed];
+    p->host[b] = BasketRec{pr.unplaced, pr.xform, k.offset, k.count};
+    p->points = std::max<int64_t>(p->points, k.offset + k.count);
+  }
+  cudaError_t e = cudaMalloc((void **)&p->d_baskets, std::max(1, nb) * sizeof(BasketRec));
+  if (e == cudaSuccess) e = cudaMalloc((void **)&p->d_prefix, (nb + 1) * sizeof(int64_t));
+  if (e == cudaSuccess && nb > 0)
+    e = cudaMemcpy(p->d_baskets, p->host.data(), nb * sizeof(BasketRec), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    vgb_basket_plan_destroy(p);
+    return cuda_error(e, "vgb_basket_plan_create");
+  }
+  vgb_status s = set_tile(p, tile, nullptr);
+  if (s != VGB_OK) {
+    vgb_basket_plan_destroy(p);
+    return s;
+  }
+  *plan = p;
+  return VGB_OK;
+}
+
+vgb_status vgb_basket_plan_destroy(vgb_basket_plan *p) {
+  if (!p) return VGB_OK;
+  if (p->graph_exec) cudaGraphExecDestroy(p->graph_exec);
+  if (p->graph) cudaGraphDestroy(p->graph);
+  cudaFree(p->d_baskets);
+  cudaFree(p->d_prefix);
+  delete p;
+  return VGB_OK;
+}
+
+vgb_status vgb_basket_plan_info(const vgb_basket_plan *p, int64_t *points, int64_t *tiles,
+                                int32_t *block, int32_t *tile) {
+  if (!p) return set_error(VGB_EINVAL, "vgb_basket_plan_info: plan is NULL");
+  if (points) *points = p->points;
+  if (tiles) *tiles = p->ntiles;
+  if (block) *block = p->block;
+  if (tile) *tile = p->tile;
+  return VGB_OK;
+}
+
+vgb_status vgb_basket_run(vgb_basket_plan *p, const double *x, const double *y, const double *z,
+                          const double *dx, const double *dy, const double *dz,
+                          const double *step_max, void *const *outs, uint32_t flags,
+                          void *stream) {
+  vgb_status s = check_io(p, x, y, z, dx, dy, dz, step_max, outs, "vgb_basket_run");
+  if (s != VGB_OK) return s;
+  return launch(p, make_io(p, x, y, z, dx, dy, dz, step_max, outs, flags), (cudaStream_t)stream);
+}
+
+vgb_status vgb_basket_tune(vgb_basket_plan *p, const double *x, const double *y, const double *z,
+                           const double *dx, const double *dy, const double *dz,
+                           const double *step_max, void *const *outs, uint32_t flags, int32_t reps,
+                           void *stream, int32_t *best_block, int32_t *best_tile,
+                           float *best_ms) {
+  vgb_status s = check_io(p, x, y, z, dx, dy, dz, step_max, outs, "vgb_basket_tune");
+  if (s != VGB_OK) return s;
+  if (reps < 1) reps = 1;
+  cudaStream_t st = (cudaStream_t)stream;
+  const FusedIO io = make_io(p, x, y, z, dx, dy, dz, step_max, outs, flags);
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  float best = -1.f;
+  int bb = p->block, bt = p->tile;
+  const int blocks[] = {128, 256, 512};
+  const int mults[] = {1, 2, 4, 8, 16};
+  for (int b : blocks) {
+    for (int m : mults) {
+      const int t = b * m;
+      if (!valid_shape(b, t)) continue;
+      p->block = b;
+      if ((s = set_tile(p, t, st)) != VGB_OK) break;
+      if ((s = launch(p, io, st)) != VGB_OK) break;  // warm-up
+      cudaEventRecord(e0, st);
+      for (int r = 0; r < reps && s == VGB_OK; ++r) s = launch(p, io, st);
+      cudaEventRecord(e1, st);
+      cudaError_t e = cudaEventSynchronize(e1);
+      if (e != cudaSuccess) {
+        s = cuda_error(e, "vgb_basket_tune");
+        break;
+      }
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      ms /= (float)reps;
+      if (best < 0.f || ms < best) {
+        best = ms;
+        bb = b;
+        bt = t;
+      }
+    }
+    if (s != VGB_OK) break;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (s != VGB_OK) return s;
+  p->block = bb;
+  if ((s = set_tile(p, bt, st)) != VGB_OK) return s;
+  if (best_block) *best_block = bb;
+  if (best_tile) *best_tile = bt;
+  if (best_ms) *best_ms = best;
+  return VGB_OK;
+}
+
+vgb_status vgb_basket_graph_capture(vgb_basket_plan *p, const double *x, const double *y,
+                                    const double *z, const double *dx, const double *dy,
+                                    const double *dz, const double *step_max, void *const *outs,
+                                    uint32_t flags) {
+  vgb_status s = check_io(p, x, y, z, dx, dy, dz, step_max, outs, "vgb_basket_graph_capture");
+  if (s != VGB_OK) return s;
+  if (p->graph_exec) cudaGraphExecDestroy(p->graph_exec);
+  if (p->graph) cudaGraphDestroy(p->graph);
+  p->graph_exec = nullptr;
+  p->graph = nullptr;
+  cudaStream_t cs;
+  cudaError_t e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
+  if (e != cudaSuccess) return cuda_error(e, "vgb_basket_graph_capture: stream");
+  e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    s = launch(p, make_io(p, x, y, z, dx, dy, dz, step_max, outs, flags), cs);
+    cudaError_t e2 = cudaStreamEndCapture(cs, &p->graph);
+    if (s == VGB_OK && e2 != cudaSuccess) s = cuda_error(e2, "vgb_basket_graph_capture: end");
+  } else {
+    s = cuda_error(e, "vgb_basket_graph_capture: begin");
+  }
+  if (s == VGB_OK) {
+    e = cudaGraphInstantiate(&p->graph_exec, p->graph, 0);
+    if (e != cudaSuccess) s = cuda_error(e, "vgb_basket_graph_capture: instantiate");
+  }
+  cudaStreamDestroy(cs);
+  return s;
+}
+
+vgb_status vgb_basket_graph_launch(vgb_basket_plan *p, void *stream) {
+  if (!p || !p->graph_exec)
+    return set_error(VGB_EINVAL, "vgb_basket_graph_launch: no graph captured");
+  cudaError_t e = cudaGraphLaunch(p->graph_exec, (cudaStream_t)stream);
+  if (e != cudaSuccess) return cuda_error(e, "vgb_basket_graph_launch");
+  count_launch();
+  return VGB_OK;
+}
+
+}  // extern "C"

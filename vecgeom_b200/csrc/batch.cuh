@@ -103,39 +103,45 @@ __global__ void __launch_bounds__(kBatchBlock) k_batch(const P prm, const DXform
 }
 
 // All requested ops for one point.  With VGB_FUSED_DTO_INSIDE_ONLY the
-// DistanceToOut result is computed only where Contains() holds.
+// DistanceToOut result is computed only where Contains() holds.  kOps bounds the
+// ops at compile time (callers that know their op set drop the other paths).
+template <class Ops, class P, uint32_t kOps = 0x3fu>
+__device__ __forceinline__ void fused_point(const P &prm, const DXform &X, const FusedIO &io,
+                                            int64_t i) {
+  using R = double;
+  const uint32_t ops = io.ops & kOps;
+  const bool need_dir = ops & ((1u << VGB_OP_DISTANCE_TO_IN) | (1u << VGB_OP_DISTANCE_TO_OUT));
+  const V3<R> m = {ldg(io.x + i), ldg(io.y + i), ldg(io.z + i)};
+  const V3<R> l = xf_point(X, m);
+  V3<R> d = {0, 0, 0};
+  if (need_dir) d = {ldg(io.dx + i), ldg(io.dy + i), ldg(io.dz + i)};
+  bool c = false;
+  if ((ops & (1u << VGB_OP_CONTAINS)) || (io.flags & VGB_FUSED_DTO_INSIDE_ONLY))
+    c = Ops::contains(prm, l);
+  if (ops & (1u << VGB_OP_CONTAINS)) static_cast<uint8_t *>(io.out[VGB_OP_CONTAINS])[i] = c;
+  if (ops & (1u << VGB_OP_INSIDE))
+    static_cast<int32_t *>(io.out[VGB_OP_INSIDE])[i] = Ops::inside(prm, l);
+  if (ops & (1u << VGB_OP_SAFETY_TO_IN))
+    static_cast<double *>(io.out[VGB_OP_SAFETY_TO_IN])[i] = Ops::safety_to_in(prm, l);
+  if (ops & (1u << VGB_OP_SAFETY_TO_OUT))
+    static_cast<double *>(io.out[VGB_OP_SAFETY_TO_OUT])[i] = Ops::safety_to_out(prm, m);
+  if (ops & (1u << VGB_OP_DISTANCE_TO_IN))
+    static_cast<double *>(io.out[VGB_OP_DISTANCE_TO_IN])[i] =
+        Ops::distance_to_in(prm, l, dti_dir<Ops>(X, d), ldg(io.step + i));
+  if (ops & (1u << VGB_OP_DISTANCE_TO_OUT)) {
+    R r = Lim<R>::inf();
+    if (!(io.flags & VGB_FUSED_DTO_INSIDE_ONLY) || c)
+      r = Ops::distance_to_out(prm, m, d, ldg(io.step + i));
+    static_cast<double *>(io.out[VGB_OP_DISTANCE_TO_OUT])[i] = r;
+  }
+}
+
 template <class Ops, class P>
 __global__ void __launch_bounds__(kBatchBlock) k_fused(const P prm, const DXform X,
                                                        const FusedIO io) {
-  using R = double;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  const uint32_t ops = io.ops;
-  const bool need_dir = ops & ((1u << VGB_OP_DISTANCE_TO_IN) | (1u << VGB_OP_DISTANCE_TO_OUT));
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < io.n; i += stride) {
-    const V3<R> m = {ldg(io.x + i), ldg(io.y + i), ldg(io.z + i)};
-    const V3<R> l = xf_point(X, m);
-    V3<R> d = {0, 0, 0};
-    if (need_dir) d = {ldg(io.dx + i), ldg(io.dy + i), ldg(io.dz + i)};
-    bool c = false;
-    if ((ops & (1u << VGB_OP_CONTAINS)) || (io.flags & VGB_FUSED_DTO_INSIDE_ONLY))
-      c = Ops::contains(prm, l);
-    if (ops & (1u << VGB_OP_CONTAINS)) static_cast<uint8_t *>(io.out[VGB_OP_CONTAINS])[i] = c;
-    if (ops & (1u << VGB_OP_INSIDE))
-      static_cast<int32_t *>(io.out[VGB_OP_INSIDE])[i] = Ops::inside(prm, l);
-    if (ops & (1u << VGB_OP_SAFETY_TO_IN))
-      static_cast<double *>(io.out[VGB_OP_SAFETY_TO_IN])[i] = Ops::safety_to_in(prm, l);
-    if (ops & (1u << VGB_OP_SAFETY_TO_OUT))
-      static_cast<double *>(io.out[VGB_OP_SAFETY_TO_OUT])[i] = Ops::safety_to_out(prm, m);
-    if (ops & (1u << VGB_OP_DISTANCE_TO_IN))
-      static_cast<double *>(io.out[VGB_OP_DISTANCE_TO_IN])[i] =
-          Ops::distance_to_in(prm, l, dti_dir<Ops>(X, d), ldg(io.step + i));
-    if (ops & (1u << VGB_OP_DISTANCE_TO_OUT)) {
-      R r = Lim<R>::inf();
-      if (!(io.flags & VGB_FUSED_DTO_INSIDE_ONLY) || c)
-        r = Ops::distance_to_out(prm, m, d, ldg(io.step + i));
-      static_cast<double *>(io.out[VGB_OP_DISTANCE_TO_OUT])[i] = r;
-    }
-  }
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < io.n; i += stride)
+    fused_point<Ops, P>(prm, X, io, i);
 }
 
 }  // namespace vgb

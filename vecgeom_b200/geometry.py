@@ -376,3 +376,74 @@ class SimpleNavigator:
         out = ctypes.c_uint32()
         check(self.geometry.L.vgb_nav_error_flags(self.geometry.handle, ctypes.byref(out)))
         return out.value
+
+
+# ---------------------------------------------------------------------------
+# baskets: many placed volumes in one persistent launch (vgb_basket_*)
+# ---------------------------------------------------------------------------
+class _Basket(ctypes.Structure):
+    _fields_ = [("placed", ctypes.c_int32), ("pad", ctypes.c_int32),
+                ("offset", ctypes.c_int64), ("count", ctypes.c_int64)]
+
+
+class BasketPlan:
+    """A plan over baskets (placed volume, offset, count) of concatenated SOA
+    arrays; ``ops`` is a mask of (1 << op) over the fused ops (Contains ...
+    SafetyToOut), ``outs`` maps op -> output array of all points."""
+
+    def __init__(self, geometry: "Geometry", baskets, ops: int, block: int = 0, tile: int = 0):
+        geometry._require_closed()
+        self.geometry = geometry
+        arr = (_Basket * max(1, len(baskets)))()
+        for k, (pv, off, cnt) in enumerate(baskets):
+            arr[k].placed = pv.id if hasattr(pv, "id") else int(pv)
+            arr[k].offset = int(off)
+            arr[k].count = int(cnt)
+        h = ctypes.c_void_p()
+        check(geometry.L.vgb_basket_plan_create(geometry.handle, arr, len(baskets), ops, block,
+                                                tile, ctypes.byref(h)))
+        self.handle = h
+        self.ops = ops
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h is not None:
+            self.geometry.L.vgb_basket_plan_destroy(h)
+            self.handle = None
+
+    def info(self) -> dict:
+        pts, tiles = ctypes.c_int64(), ctypes.c_int64()
+        block, tile = ctypes.c_int32(), ctypes.c_int32()
+        check(self.geometry.L.vgb_basket_plan_info(self.handle, ctypes.byref(pts),
+                                                   ctypes.byref(tiles), ctypes.byref(block),
+                                                   ctypes.byref(tile)))
+        return {"points": pts.value, "tiles": tiles.value, "block": block.value,
+                "tile": tile.value}
+
+    def _args(self, points: SOA3D, dirs, step, outs):
+        arr = (ctypes.c_void_p * 6)()
+        for op, a in outs.items():
+            arr[op] = _addr(a)
+        d = dirs
+        return (_addr(points.x), _addr(points.y), _addr(points.z),
+                _addr(d.x) if d else None, _addr(d.y) if d else None, _addr(d.z) if d else None,
+                _addr(step), arr)
+
+    def run(self, points: SOA3D, dirs, step, outs: dict, flags: int = 0, stream=None) -> None:
+        check(self.geometry.L.vgb_basket_run(self.handle, *self._args(points, dirs, step, outs),
+                                             flags, _stream(stream)))
+
+    def tune(self, points: SOA3D, dirs, step, outs: dict, flags: int = 0, reps: int = 3,
+             stream=None) -> tuple:
+        b, t, ms = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_float()
+        check(self.geometry.L.vgb_basket_tune(self.handle, *self._args(points, dirs, step, outs),
+                                              flags, reps, _stream(stream), ctypes.byref(b),
+                                              ctypes.byref(t), ctypes.byref(ms)))
+        return b.value, t.value, ms.value
+
+    def capture(self, points: SOA3D, dirs, step, outs: dict, flags: int = 0) -> None:
+        check(self.geometry.L.vgb_basket_graph_capture(
+            self.handle, *self._args(points, dirs, step, outs), flags))
+
+    def replay(self, stream=None) -> None:
+        check(self.geometry.L.vgb_basket_graph_launch(self.handle, _stream(stream)))

@@ -219,6 +219,9 @@ def boolsub_spec(box_half, tube_rmax, tube_dz, left_place=IDENTITY_PLACE,
 # ---------------------------------------------------------------------------
 
 def _rejection(spec: ShapeSpec, rng, n: int, want_inside: bool, scale: float):
+    if n <= 0:
+        e = np.zeros(0)
+        return e, e.copy(), e.copy()
     xs, ys, zs = [], [], []
     got = 0
     while got < n:
@@ -475,3 +478,110 @@ def isotropic_tracks(n: int, seed: int):
     v /= np.linalg.norm(v, axis=0)
     z = np.zeros(n)
     return (z.copy(), z.copy(), z.copy()), (v[0].copy(), v[1].copy(), v[2].copy())
+
+
+# ---------------------------------------------------------------------------
+# Mixed baskets: many jittered shape instances with their own point batches
+# ---------------------------------------------------------------------------
+BASKET_KINDS = ("box", "tube", "cone", "sphere", "torus", "polycone", "polyhedron", "boolsub")
+
+
+def basket_base_specs() -> dict:
+    """The eight benchmark shapes the baskets draw from (box, tube/cone/sphere,
+    torus/polycone/polyhedron/boolean subtraction)."""
+    return {"box": config1_box(), **config2_shapes(), **config3_shapes()}
+
+
+def jitter_spec(spec: ShapeSpec, rng) -> ShapeSpec:
+    """The shape with its lengths scaled by independent factors U(0.8, 1.2)
+    (angles and plane counts unchanged; radius ordering kept)."""
+    u = lambda: float(rng.uniform(0.8, 1.2))  # noqa: E731
+    p = spec.params
+    k = spec.kind
+    if k == "box":
+        return box_spec(p["dx"] * u(), p["dy"] * u(), p["dz"] * u())
+    if k == "tube":
+        return tube_spec(p["rmin"] * u(), p["rmax"] * u(), p["dz"] * u(), p["sphi"], p["dphi"])
+    if k == "cone":
+        return cone_spec(p["rmin1"] * u(), p["rmax1"] * u(), p["rmin2"] * u(), p["rmax2"] * u(),
+                         p["dz"] * u(), p["sphi"], p["dphi"])
+    if k == "sphere":
+        return sphere_spec(p["rmin"] * u(), p["rmax"] * u(), p["sphi"], p["dphi"], p["stheta"],
+                           p["dtheta"])
+    if k == "torus":
+        return torus_spec(p["rmin"] * u(), p["rmax"] * u(), p["rtor"] * u(), p["sphi"], p["dphi"])
+    if k == "polycone":
+        z = np.asarray(p["z"]) * u()
+        rmin = np.asarray(p["rmin"]) * u()
+        rmax = np.maximum(np.asarray(p["rmax"]) * u(), rmin + 1.)
+        return polycone_spec(p["sphi"], p["dphi"], z, rmin, rmax)
+    if k == "polyhedron":
+        z = np.asarray(p["z"]) * u()
+        return polyhedron_spec(p["phi_start_deg"], p["phi_delta_deg"], p["sides"], z,
+                               np.asarray(p["rmin"]) * u(), np.asarray(p["rmax"]) * u())
+    if k == "boolsub":
+        bx, by, bz = p["box_half"]
+        return boolsub_spec((bx * u(), by * u(), bz * u()), p["tube_rmax"] * u(),
+                            p["tube_dz"] * u())
+    raise ValueError(k)
+
+
+@dataclass
+class Basket:
+    spec: ShapeSpec
+    place: tuple          # (tx, ty, tz, phi, theta, psi), degrees
+    n: int
+    seed: int
+
+
+def config4_baskets(n_baskets: int = 4096, seed: int = SEED_BASE + 4, median: int = 1024,
+                    sigma: float = 1.0, lo: int = 16, hi: int = 65536) -> list:
+    """Baskets of the mixed workload: sizes clip(round(lognormal(ln median,
+    sigma)), lo, hi) (sigma is our choice; only the median is given), shape kind
+    uniform over the eight kinds, lengths jittered +-20%, Euler angles U(0, 360)
+    degrees, translation U(-100, 100) mm."""
+    rng = np.random.default_rng(seed)
+    base = basket_base_specs()
+    sizes = np.clip(np.round(rng.lognormal(math.log(median), sigma, n_baskets)), lo, hi)
+    kinds = rng.integers(0, len(BASKET_KINDS), n_baskets)
+    out = []
+    for b in range(n_baskets):
+        spec = jitter_spec(base[BASKET_KINDS[kinds[b]]], rng)
+        t = rng.uniform(-100., 100., 3)
+        a = rng.uniform(0., 360., 3)
+        out.append(Basket(spec, (float(t[0]), float(t[1]), float(t[2]), float(a[0]),
+                                 float(a[1]), float(a[2])), int(sizes[b]), seed + 17 * (b + 1)))
+    return out
+
+
+def basket_points(b: Basket):
+    """The basket's points (mixed in the shape's frame, then moved to the
+    mother frame of its placement), isotropic directions and step_max."""
+    wl = make_workload(b.spec, b.n, b.seed)
+    R = euler_rotation(*b.place[3:])
+    loc = np.stack([wl.x, wl.y, wl.z])
+    mst = R @ loc + np.asarray(b.place[:3])[:, None]
+    d = R @ np.stack([wl.dx, wl.dy, wl.dz])
+    return (mst[0], mst[1], mst[2]), (d[0], d[1], d[2]), wl.step
+
+
+def build_baskets(geom, baskets: list):
+    """Places every basket's shape instance in `geom` (one logical volume each)
+    and concatenates the baskets' points.  Returns (placed volumes, offsets,
+    (x, y, z), (dx, dy, dz), step_max)."""
+    placed, offsets = [], []
+    xs, ds, steps = [], [], []
+    off = 0
+    for k, b in enumerate(baskets):
+        lv = geom.LogicalVolume(f"basket{k}", build_unplaced(geom, b.spec))
+        placed.append(lv.Place(geom.Transformation3D(*b.place)))
+        p, d, s = basket_points(b)
+        xs.append(p)
+        ds.append(d)
+        steps.append(s)
+        offsets.append(off)
+        off += b.n
+    cat = lambda parts, j: np.ascontiguousarray(np.concatenate([q[j] for q in parts]))  # noqa: E731
+    pts = tuple(cat(xs, j) for j in range(3))
+    dirs = tuple(cat(ds, j) for j in range(3))
+    return placed, offsets, pts, dirs, np.ascontiguousarray(np.concatenate(steps))
