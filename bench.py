@@ -47,7 +47,9 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="vgb", choices=["vgb", "reference"])
-    ap.add_argument("--workload", default="shapes", choices=["shapes", "box"])
+    ap.add_argument("--workload", default="shapes", choices=["shapes", "box", "baskets", "nav"])
+    ap.add_argument("--baskets", type=int, default=4096, help="baskets of the basket workload")
+    ap.add_argument("--requests", type=int, default=300, help="requests of the nav workload")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32r"])
     ap.add_argument("--n", type=int, default=0, help="points per shape (0 = workload default)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -232,6 +234,208 @@ def run_reference_arm(args):
 
 
 # ---------------------------------------------------------------------------
+# mixed baskets: one persistent launch (CUDA graph) over many shape instances
+# ---------------------------------------------------------------------------
+
+def run_baskets(args):
+    """4096 baskets (lognormal sizes, median 1024, clipped 16..65536), one
+    jittered shape instance of the eight benchmark kinds each at a random
+    placement; DistanceToIn + SafetyToIn per point.  One step = one replay of
+    the captured persistent launch.  Inputs (~7 M points, ~400 MB) exceed L2."""
+    import torch
+    import vecgeom_b200 as V
+    from vecgeom_b200 import workloads as W
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    rank = int(os.environ.get("RANK", "0"))
+    bs = W.config4_baskets(args.baskets, seed=W.SEED_BASE + 4 + 1000 * rank)
+    g = V.Geometry()
+    placed, offsets, pts, dirs, step = W.build_baskets(g, bs)
+    g.CloseGeometry()
+    n = len(pts[0])
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()  # noqa: E731
+    P = V.SOA3D(*(dev(a) for a in pts))
+    D = V.SOA3D(*(dev(a) for a in dirs))
+    S = dev(step)
+    DTI, STI = 1 << 2, 1 << 4
+    outs = {2: torch.empty(n, dtype=torch.float64, device="cuda"),
+            4: torch.empty(n, dtype=torch.float64, device="cuda")}
+    plan = V.BasketPlan(g, [(pv, o, b.n) for pv, o, b in zip(placed, offsets, bs)], DTI | STI)
+    stream = torch.cuda.current_stream()
+    block, tile, tune_ms = plan.tune(P, D, S, outs, reps=3, stream=stream)
+    plan.capture(P, D, S, outs)
+    for _ in range(max(3, args.warmup)):
+        plan.replay(stream)
+    torch.cuda.synchronize()
+    V.lib().vgb_launch_count_reset()
+    clk = ClockSampler(torch.cuda.current_device())
+    clk.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        plan.replay(stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    launches = int(V.lib().vgb_launch_count())
+    ms = e0.elapsed_time(e1) / args.steps
+    value = 2 * n / (ms * 1e-3) / 1e6
+    # the same work as one fused call per basket (the unbatched form)
+    ref = {k: torch.empty_like(v) for k, v in outs.items()}
+
+    def unbatched():
+        for pv, off, b in zip(placed, offsets, bs):
+            if b.n:
+                sl = slice(off, off + b.n)
+                pv.fused(DTI | STI, V.SOA3D(P.x[sl], P.y[sl], P.z[sl]),
+                         {k: v[sl] for k, v in ref.items()},
+                         dirs=V.SOA3D(D.x[sl], D.y[sl], D.z[sl]), step_max=S[sl])
+    unbatched()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    unbatched()
+    torch.cuda.synchronize()
+    unb_ms = (time.perf_counter() - t0) * 1e3
+    same = all(bool(((outs[k] == ref[k]) | (outs[k].isnan() & ref[k].isnan())).all())
+               for k in outs)
+    # end to end: pinned host inputs in, results out, every step
+    hp = [torch.from_numpy(np.ascontiguousarray(a)).pin_memory() for a in (*pts, *dirs, step)]
+    ho = {k: torch.empty(n, dtype=torch.float64).pin_memory() for k in outs}
+    dv = [P.x, P.y, P.z, D.x, D.y, D.z, S]
+    for _ in range(2):
+        for a, b in zip(dv, hp):
+            a.copy_(b, non_blocking=True)
+        plan.replay(stream)
+        for k in outs:
+            ho[k].copy_(outs[k], non_blocking=True)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e2e_steps = max(1, min(args.steps, 5))
+    for _ in range(e2e_steps):
+        for a, b in zip(dv, hp):
+            a.copy_(b, non_blocking=True)
+        plan.replay(stream)
+        for k in outs:
+            ho[k].copy_(outs[k], non_blocking=True)
+    torch.cuda.synchronize()
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        pass
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    bpp = 24 + 24 + 8 + 8 + 8  # x,y,z + direction + step_max in, two doubles out
+    achieved = bpp * n / (ms * 1e-3) / 1e9
+    kinds = {k: sum(b.n for b in bs if b.spec.kind == k) for k in W.BASKET_KINDS}
+    line = {"metric": "Mpoints/s per shape op (fp64, mixed baskets in one persistent launch)",
+            "value": round(value, 2), "unit": "Mpoints/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": max(3, args.warmup), "ms_per_step": round(ms, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded)",
+            "config": {"workload": f"{len(bs)} baskets, lognormal sizes (median 1024, sigma 1, "
+                                   "clipped 16-65536), 8 shape kinds jittered +-20%, random "
+                                   "placements; DistanceToIn + SafetyToIn",
+                       "points": n, "points_per_kind": kinds,
+                       "l2": "inputs (~%d MB) exceed L2" % (bpp * n >> 20),
+                       "autotuned": {"block": block, "tile": tile, "ms": round(tune_ms, 4)}},
+            "unbatched": {"ms": round(unb_ms, 3), "mpoints_s": round(2 * n / unb_ms / 1e3, 2),
+                          "launches": sum(1 for b in bs if b.n),
+                          "results_identical": same},
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm,
+                         "unit": "GB/s", "frac": round(achieved / hbm, 4), "traffic": None,
+                         "kernel": "k_baskets", "bytes_per_point": bpp,
+                         "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"},
+            "e2e": {"value": round(2 * n / e2e_s / 1e6, 2), "unit": "Mpoints/s",
+                    "h2d_bytes_per_step": 56 * n, "d2h_bytes_per_step": 16 * n},
+            "gpu_launches": launches, "clocks": clocks}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# served navigation: continuous batching of Poisson-arriving track baskets
+# ---------------------------------------------------------------------------
+
+def run_nav(args):
+    """Layered detector (14,011 placed volumes).  Requests of 1-16384 tracks
+    (log-uniform sizes) from the origin, isotropic, arrive as a Poisson stream
+    at ~80% of the measured saturated throughput; each track steps (safety +
+    FindNextBoundaryAndStep) until it leaves the world or 64 steps."""
+    import torch
+    import vecgeom_b200 as V
+    from vecgeom_b200 import workloads as W
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    g = V.Geometry()
+    W.build_detector(W.VgbBuilder(g))
+    max_steps, spl = 64, 8
+    rng = np.random.default_rng(W.SEED_BASE + 5)
+    nreq = args.requests
+    sizes = np.clip(np.round(np.exp(rng.uniform(0., np.log(16384.), nreq))), 1, 16384).astype(int)
+    reqs = [W.isotropic_tracks(int(m), W.SEED_BASE + 500 + k) for k, m in enumerate(sizes)]
+    srv = V.NavServer(g, max_tracks=1 << 18, steps_per_launch=spl, max_steps=max_steps)
+
+    def drain(submit_times, arrivals=None):
+        """Runs until every request finished; submits request k when the wall
+        clock passes arrivals[k] (None: all at once).  Returns latencies and
+        total steps."""
+        t0 = time.perf_counter()
+        pending = list(range(nreq))
+        lat, steps, done_n = {}, 0, 0
+        rid_of = {}
+        while done_n < nreq:
+            now = time.perf_counter() - t0
+            while pending and (arrivals is None or arrivals[pending[0]] <= now):
+                k = pending.pop(0)
+                submit_times[k] = t0 + (arrivals[k] if arrivals is not None else now)
+                rid_of[srv.submit(*reqs[k])] = k
+            done, live, queued = srv.step()
+            tdone = time.perf_counter()
+            for rid in done:
+                k = rid_of.pop(rid)
+                r = srv.result(rid)
+                steps += int(r["nsteps"].sum())
+                lat[k] = tdone - submit_times[k]
+                done_n += 1
+            if not done and not live and not queued and pending and arrivals is not None:
+                time.sleep(max(0., min(0.002, arrivals[pending[0]] - now)))
+        return lat, steps, time.perf_counter() - t0
+
+    # saturated throughput (all requests queued at once) sets the arrival rate
+    sub = [0.] * nreq
+    drain(sub)  # warm-up
+    _, sat_steps, sat_s = drain(sub)
+    mean_steps = sat_steps / nreq
+    rate = 0.8 * (sat_steps / sat_s) / mean_steps      # requests per second
+    arrivals = np.cumsum(rng.exponential(1. / rate, nreq))
+    clk = ClockSampler(torch.cuda.current_device())
+    V.lib().vgb_launch_count_reset()
+    clk.start()
+    lat, steps, wall = drain(sub, arrivals)
+    clocks = clk.stop()
+    launches = int(V.lib().vgb_launch_count())
+    L = np.array([lat[k] for k in range(nreq)]) * 1e3
+    line = {"metric": "nav steps/s (fp64, served) with p50/p99 request latency",
+            "value": round(steps / wall, 1), "unit": "steps/s", "n_gpus": 1,
+            "steps": nreq, "warmup": 1, "ms_per_step": round(wall / nreq * 1e3, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded)",
+            "config": {"workload": "layered detector, 14011 placed volumes, 4 levels; "
+                                   f"{nreq} requests of 1-16384 tracks (log-uniform) from the "
+                                   "origin, Poisson arrivals at 80% of saturated throughput",
+                       "max_steps": max_steps, "steps_per_launch": spl,
+                       "slots": srv.max_tracks, "tracks": int(sizes.sum()),
+                       "saturated_steps_per_s": round(sat_steps / sat_s, 1),
+                       "arrival_rate_per_s": round(rate, 2)},
+            "latency_ms": {"p50": round(float(np.percentile(L, 50)), 3),
+                           "p99": round(float(np.percentile(L, 99)), 3),
+                           "max": round(float(L.max()), 3)},
+            "e2e": {"value": round(steps / wall, 1), "unit": "steps/s",
+                    "h2d_bytes_per_step": int(48 * sizes.sum() / nreq),
+                    "d2h_bytes_per_step": int(36 * sizes.sum() / nreq)},
+            "gpu_launches": launches, "clocks": clocks}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
 # the GPU arm
 # ---------------------------------------------------------------------------
 
@@ -239,6 +443,12 @@ def main():
     args = parse()
     if args.impl == "reference":
         run_reference_arm(args)
+        return
+    if args.workload == "baskets":
+        run_baskets(args)
+        return
+    if args.workload == "nav":
+        run_nav(args)
         return
     import torch
     import torch.distributed as dist

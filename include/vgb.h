@@ -333,6 +333,46 @@ vgb_status vgb_nav_trace(const vgb_geometry *g, int64_t n, const double *x, cons
 /* Navigation error flags (VGB_NAV_ERR_*) raised since the last call; clears them. */
 vgb_status vgb_nav_error_flags(const vgb_geometry *g, uint32_t *flags);
 
+/* ---------------------------------------------------------------------------
+ * Navigation server: continuous batching of track baskets (no counterpart in
+ * the reference, whose navigators step one caller-given basket at a time,
+ * navigation/SimpleNavigator.h:599-743).
+ *
+ * Requests (baskets of straight tracks, host arrays) are queued by
+ * vgb_server_submit.  Each vgb_server_step is one iteration: it admits queued
+ * requests in arrival order while the device track slots (allocated once, at
+ * create, from free HBM) can hold them, advances every live track of every
+ * admitted request by up to steps_per_launch navigation steps in one launch,
+ * and retires the requests whose tracks all finished.  A track finishes when
+ * its state leaves the world or after max_steps steps.  Per track the server
+ * keeps what vgb_nav_trace would produce: the step count, the final point and
+ * a 64-bit FNV-1a hash of its sequence of (next placed id, step) records, so a
+ * request's results do not depend on what else was in flight.
+ * ------------------------------------------------------------------------- */
+typedef struct vgb_server vgb_server;
+
+/* max_tracks = 0 sizes the slots to a quarter of the free device memory
+ * (at most 2^22 tracks).  Fails with VGB_ENOMEM when the slots do not fit. */
+vgb_status vgb_server_create(const vgb_geometry *g, int64_t max_tracks, int32_t steps_per_launch,
+                             int32_t max_steps, double pstep, vgb_server **server);
+vgb_status vgb_server_destroy(vgb_server *server);
+/* slot capacity (tracks) and device bytes held */
+vgb_status vgb_server_info(const vgb_server *server, int64_t *max_tracks, int64_t *device_bytes);
+/* Queues a request of n tracks (host arrays, copied); VGB_ENOSPC if n exceeds
+ * the slot capacity.  Request ids increase from 0. */
+vgb_status vgb_server_submit(vgb_server *server, int64_t n, const double *x, const double *y,
+                             const double *z, const double *dx, const double *dy,
+                             const double *dz, int64_t *request_id);
+/* One iteration (admit, launch, retire); synchronous.  Writes up to
+ * max_completed finished request ids; *live = tracks still in flight,
+ * *queued = requests waiting for admission. */
+vgb_status vgb_server_step(vgb_server *server, int64_t *completed, int32_t max_completed,
+                           int32_t *ncompleted, int64_t *live, int64_t *queued);
+/* Results of a finished request (arrays of its n tracks; any may be NULL);
+ * the request is then forgotten. */
+vgb_status vgb_server_result(vgb_server *server, int64_t request_id, int32_t *nsteps, double *x,
+                             double *y, double *z, uint64_t *hash);
+
 #ifdef __cplusplus
 }
 #endif

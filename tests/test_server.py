@@ -1,0 +1,126 @@
+"""Navigation server (continuous batching) on the layered detector.
+
+Each request's per-track results (step count, final point, FNV-1a hash of its
+(next placed id, step) records) must equal what vgb_nav_trace produces for the
+same tracks, whether the request is served alone or while other requests of
+uneven sizes arrive and finish around it.
+"""
+import numpy as np
+import pytest
+
+from vecgeom_b200 import workloads as W
+
+MAX_STEPS = 48
+
+
+def fnv1a(data: bytes, h: int = 0xcbf29ce484222325) -> int:
+    for b in data:
+        h ^= b
+        h = (h * 0x100000001b3) & 0xffffffffffffffff
+    return h
+
+
+def fnv_hash(ids, steps):
+    """FNV-1a 64 over the little-endian bytes of (int32 id, float64 step) records."""
+    return fnv1a(b"".join(np.int32(i).tobytes() + np.float64(s).tobytes()
+                          for i, s in zip(ids, steps)))
+
+
+def test_fnv1a_known_answers():
+    # published FNV-1a 64 test vectors
+    assert fnv1a(b"") == 0xcbf29ce484222325
+    assert fnv1a(b"a") == 0xaf63dc4c8601ec8c
+    assert fnv1a(b"foobar") == 0x85944171f73967e8
+
+
+def requests(sizes, seed):
+    rng = np.random.default_rng(seed)
+    out = []
+    for k, n in enumerate(sizes):
+        if k % 2:
+            pts, dirs = W.isotropic_tracks(n, seed + k)
+        else:
+            _, dirs = W.isotropic_tracks(n, seed + k)
+            pts = (rng.uniform(-1000, 1000, n), rng.uniform(-1000, 1000, n),
+                   rng.uniform(-1200, 1200, n))
+        out.append((pts, dirs))
+    return out
+
+
+def trace_truth(g, pts, dirs):
+    from test_navigation import gpu_trace
+    ids, steps, _, nst = gpu_trace(g, pts, dirs, MAX_STEPS)
+    n = len(pts[0])
+    ids = ids.reshape(n, MAX_STEPS)
+    steps = steps.reshape(n, MAX_STEPS)
+    hashes = np.array([fnv_hash(ids[i, :nst[i]], steps[i, :nst[i]]) for i in range(n)],
+                      np.uint64)
+    fx = np.array(pts[0], np.float64).copy()
+    fy = np.array(pts[1], np.float64).copy()
+    fz = np.array(pts[2], np.float64).copy()
+    for i in range(n):
+        for k in range(nst[i]):
+            fx[i] = fx[i] + dirs[0][i] * steps[i, k]
+            fy[i] = fy[i] + dirs[1][i] * steps[i, k]
+            fz[i] = fz[i] + dirs[2][i] * steps[i, k]
+    return {"nsteps": nst, "hash": hashes, "x": fx, "y": fy, "z": fz}
+
+
+def serve(srv, reqs, arrivals):
+    """Submits request k once `arrivals[k]` iterations have run; returns results."""
+    order = list(range(len(reqs)))
+    pending = sorted(order, key=lambda k: arrivals[k])
+    it = 0
+    rid_of = {}
+    results = {}
+    while pending or len(results) < len(reqs):
+        while pending and arrivals[pending[0]] <= it:
+            k = pending.pop(0)
+            rid_of[srv.submit(*reqs[k])] = k
+        done, live, queued = srv.step()
+        for rid in done:
+            results[rid_of[rid]] = srv.result(rid)
+        it += 1
+        assert it < 10000
+    return results
+
+
+def assert_same(res, want, what):
+    for key in ("nsteps", "hash", "x", "y", "z"):
+        assert np.array_equal(res[key], want[key]), f"{what}: {key} differs"
+
+
+@pytest.mark.gpu
+def test_served_alone_and_in_the_mix_match_the_trace():
+    import vecgeom_b200 as V
+    g = V.Geometry()
+    W.build_detector(W.VgbBuilder(g))
+    sizes = [300, 17, 1000, 1, 513, 2048, 64, 777]
+    reqs = requests(sizes, W.SEED_BASE + 91)
+    truth = [trace_truth(g, *r) for r in reqs]
+    # small slot table so admission has to wait for retirements
+    srv = V.NavServer(g, max_tracks=2560, steps_per_launch=5, max_steps=MAX_STEPS)
+    mixed = serve(srv, reqs, arrivals=[0, 0, 1, 2, 2, 3, 7, 9])
+    for k in range(len(reqs)):
+        assert_same(mixed[k], truth[k], f"request {k} in the mix")
+    for k in (0, 5):
+        alone = serve(V.NavServer(g, max_tracks=4096, steps_per_launch=3, max_steps=MAX_STEPS),
+                      [reqs[k]], arrivals=[0])
+        assert_same(alone[0], truth[k], f"request {k} alone")
+
+
+@pytest.mark.gpu
+def test_server_capacity_and_errors():
+    import vecgeom_b200 as V
+    g = V.Geometry()
+    W.build_detector(W.VgbBuilder(g))
+    srv = V.NavServer(g, max_tracks=512, steps_per_launch=4, max_steps=MAX_STEPS)
+    assert srv.max_tracks == 512
+    pts, dirs = W.isotropic_tracks(600, 5)
+    with pytest.raises(V.VgbError):
+        srv.submit(pts, dirs)
+    rid = srv.submit(*W.isotropic_tracks(0, 5))
+    done, live, queued = srv.step()
+    assert rid in done or srv.result(rid)["nsteps"].size == 0
+    with pytest.raises(V.VgbError):
+        srv.result(12345)

@@ -93,6 +93,12 @@ SIGNATURES = {
                                                           ctypes.POINTER(ctypes.c_float)]),
     "vgb_basket_graph_capture": (ctypes.c_int, [_vp] + [_vp] * 8 + [_u32]),
     "vgb_basket_graph_launch": (ctypes.c_int, [_vp, _vp]),
+    "vgb_server_create": (ctypes.c_int, [_vp, _i64, _i32, _i32, _dbl, ctypes.POINTER(_vp)]),
+    "vgb_server_destroy": (ctypes.c_int, [_vp]),
+    "vgb_server_info": (ctypes.c_int, [_vp, _pi64, _pi64]),
+    "vgb_server_submit": (ctypes.c_int, [_vp, _i64] + [_vp] * 6 + [_pi64]),
+    "vgb_server_step": (ctypes.c_int, [_vp, _pi64, _i32, _pi32, _pi64, _pi64]),
+    "vgb_server_result": (ctypes.c_int, [_vp, _i64] + [_vp] * 5),
     "vgb_navpool_create": (ctypes.c_int, [_vp, _i64, ctypes.POINTER(_vp)]),
     "vgb_navpool_destroy": (ctypes.c_int, [_vp]),
     "vgb_navpool_info": (ctypes.c_int, [_vp, ctypes.POINTER(_vp), _pi64, _pi64]),

@@ -1,0 +1,455 @@
+// server.cu -- continuous batching of navigation requests (vgb_server_*).
+//
+// Device memory holds a fixed table of track slots, carved into chunks of
+// kChunk tracks.  A request owns whole chunks; the last one is padded with
+// finished tracks.  Every iteration:
+//   1. admit: queued requests, in arrival order, take free chunks; their points
+//      are copied into the slots and one launch locates them (LocatePoint from
+//      the world) and clears their counters;
+//   2. step: one launch over the chunks of all admitted requests advances every
+//      live track by up to steps_per_launch steps (one warp per track, the
+//      navigator of navigation.cuh) and counts the tracks still live per chunk;
+//   3. retire: a request whose chunks have no live track is finished; its
+//      results stay in the slots until vgb_server_result copies them out and
+//      frees the chunks.
+// Requests that arrive while others are in flight join at the next iteration,
+// so their steps share launches with the older requests' steps.
+#include <algorithm>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <vector>
+
+#include "navigation.cuh"
+
+using namespace vgb;
+
+namespace vgb {
+namespace {
+
+constexpr int kChunk = 256;
+constexpr int kSrvBlock = 128;
+constexpr int kSrvWarps = kSrvBlock / 32;
+constexpr uint64_t kFnvOffset = 0xcbf29ce484222325ull;
+constexpr uint64_t kFnvPrime = 0x100000001b3ull;
+
+struct Slots {
+  double *x, *y, *z, *dx, *dy, *dz;
+  unsigned char *states;
+  int64_t stride;
+  int32_t *nsteps;
+  uint64_t *hash;
+  uint8_t *done;
+};
+
+VGB_HD uint64_t fnv_bytes(uint64_t h, const void *p, int n) {
+  const unsigned char *b = static_cast<const unsigned char *>(p);
+  for (int i = 0; i < n; ++i) {
+    h ^= b[i];
+    h *= kFnvPrime;
+  }
+  return h;
+}
+
+// slot of the t-th track of the chunk list
+VGB_D int64_t slot_of(const int32_t *chunks, int64_t t) {
+  return (int64_t)chunks[t / kChunk] * kChunk + (t % kChunk);
+}
+
+template <uint32_t kMask>
+__global__ void __launch_bounds__(kSrvBlock)
+    k_srv_admit(const NavGeom G, const int32_t *chunks, int64_t ntracks, int64_t nvalid, Slots S,
+                uint32_t *flags) {
+  using Nav = Navigator<WarpLanes, kMask>;
+  const int64_t warps = (int64_t)gridDim.x * kSrvWarps;
+  for (int64_t t = (int64_t)blockIdx.x * kSrvWarps + threadIdx.x / 32; t < ntracks; t += warps) {
+    const int64_t s = slot_of(chunks, t);
+    NavPath p;
+    bool ok = true;
+    if (t < nvalid) {
+      ok = Nav::locate_from_world(G, p, V3<double>{S.x[s], S.y[s], S.z[s]});
+    } else {
+      p.level = 0;
+      p.boundary = false;
+    }
+    if (WarpLanes::lane() == 0) {
+      if (!ok) {
+        atomicOr(flags, (uint32_t)VGB_NAV_ERR_DEPTH);
+        p.level = 0;
+      }
+      nav_store(p, NavStateRef{S.states + s * S.stride}, G.max_depth);
+      S.nsteps[s] = 0;
+      S.hash[s] = kFnvOffset;
+      S.done[s] = (t < nvalid && p.level > 0) ? 0 : 1;
+    }
+  }
+}
+
+template <uint32_t kMask>
+__global__ void __launch_bounds__(kSrvBlock)
+    k_srv_step(const NavGeom G, const int32_t *chunks, int64_t ntracks, Slots S, double pstep,
+               int32_t max_steps, int32_t steps_per_launch, int32_t *live, uint32_t *flags) {
+  using Nav = Navigator<WarpLanes, kMask>;
+  const int64_t warps = (int64_t)gridDim.x * kSrvWarps;
+  const bool lane0 = WarpLanes::lane() == 0;
+  for (int64_t t = (int64_t)blockIdx.x * kSrvWarps + threadIdx.x / 32; t < ntracks; t += warps) {
+    const int64_t s = slot_of(chunks, t);
+    if (S.done[s]) continue;
+    NavPath cur, nxt;
+    nav_load(cur, NavStateRef{S.states + s * S.stride});
+    V3<double> p = {S.x[s], S.y[s], S.z[s]};
+    const V3<double> d = {S.dx[s], S.dy[s], S.dz[s]};
+    int32_t k = S.nsteps[s];
+    uint64_t h = S.hash[s];
+    bool ok = true;
+    for (int it = 0; it < steps_per_launch && cur.level > 0 && k < max_steps; ++it) {
+      const DXform m = nav_top_matrix(G, cur);
+      const V3<double> lp = xf_point(m, p);
+      const V3<double> ld = xf_dir(m, d);
+      double st = 0.;
+      ok = Nav::step(G, cur, nxt, lp, ld, pstep, st);
+      if (!ok) break;
+      const int32_t id = nxt.top();
+      h = fnv_bytes(h, &id, 4);
+      h = fnv_bytes(h, &st, 8);
+      p = {p.x + d.x * st, p.y + d.y * st, p.z + d.z * st};
+      cur = nxt;
+      ++k;
+    }
+    if (lane0) {
+      const bool fin = !ok || cur.level == 0 || k >= max_steps;
+      if (!ok) atomicOr(flags, (uint32_t)VGB_NAV_ERR_DEPTH);
+      nav_store(cur, NavStateRef{S.states + s * S.stride}, G.max_depth);
+      S.x[s] = p.x;
+      S.y[s] = p.y;
+      S.z[s] = p.z;
+      S.nsteps[s] = ok ? k : -1;
+      S.hash[s] = h;
+      S.done[s] = fin ? 1 : 0;
+      if (!fin) atomicAdd(live + t / kChunk, 1);
+    }
+  }
+}
+
+NavGeom server_geom(const vgb_geometry *g) {
+  NavGeom G;
+  G.params = g->dev.params;
+  G.unplaced = g->dev.unplaced;
+  G.placed = g->dev.placed;
+  G.xforms = g->dev.xforms;
+  G.raw = g->dev.raw;
+  G.logicals = g->dev.logicals;
+  G.daughters = g->dev.daughters;
+  G.world = g->world;
+  G.max_depth = g->max_depth;
+  return G;
+}
+
+int srv_grid(int64_t ntracks) {
+  const int64_t want = (ntracks + kSrvWarps - 1) / kSrvWarps;
+  const int64_t cap = 148 * 16;
+  return (int)std::max<int64_t>(1, std::min(want, cap));
+}
+
+struct Request {
+  int64_t id = -1;
+  int64_t n = 0;
+  std::vector<double> in;  // x, y, z, dx, dy, dz (6 n)
+  std::vector<int32_t> chunks;
+  bool finished = false;
+};
+
+}  // namespace
+}  // namespace vgb
+
+struct vgb_server {
+  const vgb_geometry *g = nullptr;
+  int device = -1;
+  int32_t steps_per_launch = 8;
+  int32_t max_steps = 1000;
+  double pstep = 1e30;
+  int64_t nchunks = 0;
+  int64_t bytes = 0;
+  vgb::Slots S{};
+  int32_t *d_chunks = nullptr;   // chunk list of the current launch
+  int32_t *d_live = nullptr;     // live tracks per listed chunk
+  cudaStream_t stream = nullptr;
+  std::vector<int32_t> free_chunks;
+  std::deque<vgb::Request *> queue;
+  std::vector<vgb::Request *> active;
+  std::map<int64_t, vgb::Request *> done;
+  int64_t next_id = 0;
+  bool all_shapes = false;
+};
+
+namespace vgb {
+namespace {
+
+template <class T> cudaError_t srv_alloc(vgb_server *s, T **p, size_t n) {
+  cudaError_t e = cudaMalloc((void **)p, std::max<size_t>(1, n) * sizeof(T));
+  if (e == cudaSuccess) s->bytes += (int64_t)(std::max<size_t>(1, n) * sizeof(T));
+  return e;
+}
+
+void srv_free(vgb_server *s) {
+  Slots &S = s->S;
+  void *ptrs[] = {S.x, S.y, S.z, S.dx, S.dy, S.dz, S.states, S.nsteps, S.hash, S.done,
+                  s->d_chunks, s->d_live};
+  for (void *p : ptrs) cudaFree(p);
+  if (s->stream) cudaStreamDestroy(s->stream);
+  for (Request *r : s->queue) delete r;
+  for (Request *r : s->active) delete r;
+  for (auto &kv : s->done) delete kv.second;
+}
+
+template <uint32_t kMask>
+void launch_admit(vgb_server *s, const int32_t *chunks, int64_t nt, int64_t nv) {
+  k_srv_admit<kMask><<<srv_grid(nt), kSrvBlock, 0, s->stream>>>(server_geom(s->g), chunks, nt, nv,
+                                                                  s->S, s->g->dev.nav_flags);
+}
+template <uint32_t kMask> void launch_step(vgb_server *s, int64_t nt) {
+  k_srv_step<kMask><<<srv_grid(nt), kSrvBlock, 0, s->stream>>>(
+      server_geom(s->g), s->d_chunks, nt, s->S, s->pstep, s->max_steps, s->steps_per_launch,
+      s->d_live, s->g->dev.nav_flags);
+}
+
+// Admits queued requests while free chunks last (arrival order: a request that
+// does not fit blocks the ones behind it).
+vgb_status admit(vgb_server *s) {
+  while (!s->queue.empty()) {
+    Request *r = s->queue.front();
+    const int64_t need = (r->n + kChunk - 1) / kChunk;
+    if (need > (int64_t)s->free_chunks.size()) break;
+    s->queue.pop_front();
+    r->chunks.assign(s->free_chunks.end() - need, s->free_chunks.end());
+    s->free_chunks.resize(s->free_chunks.size() - need);
+    std::sort(r->chunks.begin(), r->chunks.end());
+    // inputs: one copy per chunk and coordinate
+    double *dst[6] = {s->S.x, s->S.y, s->S.z, s->S.dx, s->S.dy, s->S.dz};
+    cudaError_t e = cudaSuccess;
+    for (int64_t c = 0; c < need && e == cudaSuccess; ++c) {
+      const int64_t first = c * kChunk, cnt = std::min<int64_t>(kChunk, r->n - first);
+      if (cnt <= 0) break;
+      for (int k = 0; k < 6 && e == cudaSuccess; ++k)
+        e = cudaMemcpyAsync(dst[k] + (int64_t)r->chunks[c] * kChunk, r->in.data() + k * r->n + first,
+                            cnt * sizeof(double), cudaMemcpyHostToDevice, s->stream);
+    }
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(s->d_chunks, r->chunks.data(), need * sizeof(int32_t),
+                          cudaMemcpyHostToDevice, s->stream);
+    if (e != cudaSuccess) return cuda_error(e, "vgb_server_step: admit copy");
+    if (s->all_shapes)
+      launch_admit<kNavMaskAll>(s, s->d_chunks, need * kChunk, r->n);
+    else
+      launch_admit<kNavMaskBoxTubeTrd>(s, s->d_chunks, need * kChunk, r->n);
+    count_launch();
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);  // r->in is read by the copies
+    if (e != cudaSuccess) return cuda_error(e, "vgb_server_step: admit");
+    std::vector<double>().swap(r->in);
+    s->active.push_back(r);
+  }
+  return VGB_OK;
+}
+
+}  // namespace
+}  // namespace vgb
+
+extern "C" {
+
+vgb_status vgb_server_create(const vgb_geometry *g, int64_t max_tracks, int32_t steps_per_launch,
+                             int32_t max_steps, double pstep, vgb_server **server) {
+  if (!server) return set_error(VGB_EINVAL, "vgb_server_create: server is NULL");
+  *server = nullptr;
+  if (!g || !g->closed || g->world < 0)
+    return set_error(VGB_EINVAL, "vgb_server_create: geometry not closed or without world");
+  if (g->max_depth > kNavMaxLevels)
+    return set_error(VGB_ENOTSUP, "vgb_server_create: geometry deeper than %d levels",
+                     kNavMaxLevels);
+  if (max_tracks < 0 || steps_per_launch < 1 || max_steps < 0)
+    return set_error(VGB_EINVAL, "vgb_server_create: bad capacity or step counts");
+  const int64_t stride = nav_state_stride(g->max_depth);
+  const int64_t per_track = 6 * 8 + stride + 4 + 8 + 1;
+  if (max_tracks == 0) {
+    size_t fr = 0, tot = 0;
+    cudaError_t e = cudaMemGetInfo(&fr, &tot);
+    if (e != cudaSuccess) return cuda_error(e, "vgb_server_create: cudaMemGetInfo");
+    max_tracks = std::min<int64_t>((int64_t)(fr / 4) / per_track, (int64_t)1 << 22);
+  }
+  const int64_t nchunks = (max_tracks + kChunk - 1) / kChunk;
+  const int64_t nslots = nchunks * kChunk;
+  size_t fr = 0, tot = 0;
+  cudaError_t e = cudaMemGetInfo(&fr, &tot);
+  if (e != cudaSuccess) return cuda_error(e, "vgb_server_create: cudaMemGetInfo");
+  if ((double)nslots * per_track > 0.9 * (double)fr)
+    return set_error(VGB_ENOMEM, "vgb_server_create: %lld track slots need %lld bytes, %zu free",
+                     (long long)nslots, (long long)(nslots * per_track), fr);
+  vgb_server *s = new vgb_server;
+  s->g = g;
+  s->device = g->device;
+  s->steps_per_launch = steps_per_launch;
+  s->max_steps = max_steps;
+  s->pstep = pstep;
+  s->nchunks = nchunks;
+  s->all_shapes = (g->type_mask & ~kNavMaskBoxTubeTrd) != 0;
+  Slots &S = s->S;
+  S.stride = stride;
+  e = cudaSuccess;
+  double **coords[] = {&S.x, &S.y, &S.z, &S.dx, &S.dy, &S.dz};
+  for (double **c : coords)
+    if (e == cudaSuccess) e = srv_alloc(s, c, nslots);
+  if (e == cudaSuccess) e = srv_alloc(s, &S.states, nslots * stride);
+  if (e == cudaSuccess) e = srv_alloc(s, &S.nsteps, nslots);
+  if (e == cudaSuccess) e = srv_alloc(s, &S.hash, nslots);
+  if (e == cudaSuccess) e = srv_alloc(s, &S.done, nslots);
+  if (e == cudaSuccess) e = srv_alloc(s, &s->d_chunks, nchunks);
+  if (e == cudaSuccess) e = srv_alloc(s, &s->d_live, nchunks);
+  if (e == cudaSuccess) e = cudaMemset(S.done, 1, nslots);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    srv_free(s);
+    delete s;
+    return cuda_error(e, "vgb_server_create");
+  }
+  s->free_chunks.resize(nchunks);
+  for (int64_t c = 0; c < nchunks; ++c) s->free_chunks[c] = (int32_t)(nchunks - 1 - c);
+  *server = s;
+  return VGB_OK;
+}
+
+vgb_status vgb_server_destroy(vgb_server *s) {
+  if (!s) return VGB_OK;
+  cudaStreamSynchronize(s->stream);
+  srv_free(s);
+  delete s;
+  return VGB_OK;
+}
+
+vgb_status vgb_server_info(const vgb_server *s, int64_t *max_tracks, int64_t *device_bytes) {
+  if (!s) return set_error(VGB_EINVAL, "vgb_server_info: server is NULL");
+  if (max_tracks) *max_tracks = s->nchunks * kChunk;
+  if (device_bytes) *device_bytes = s->bytes;
+  return VGB_OK;
+}
+
+vgb_status vgb_server_submit(vgb_server *s, int64_t n, const double *x, const double *y,
+                             const double *z, const double *dx, const double *dy,
+                             const double *dz, int64_t *request_id) {
+  if (!s) return set_error(VGB_EINVAL, "vgb_server_submit: server is NULL");
+  if (n < 0 || (n > 0 && (!x || !y || !z || !dx || !dy || !dz)))
+    return set_error(VGB_EINVAL, "vgb_server_submit: bad track arrays");
+  if ((n + kChunk - 1) / kChunk > s->nchunks)
+    return set_error(VGB_ENOSPC, "vgb_server_submit: %lld tracks exceed the %lld slots",
+                     (long long)n, (long long)(s->nchunks * kChunk));
+  Request *r = new Request;
+  r->id = s->next_id++;
+  r->n = n;
+  r->in.resize(6 * n);
+  const double *src[6] = {x, y, z, dx, dy, dz};
+  for (int k = 0; k < 6; ++k)
+    if (n) std::memcpy(r->in.data() + k * n, src[k], n * sizeof(double));
+  if (n == 0) {
+    r->finished = true;
+    s->done[r->id] = r;
+  } else {
+    s->queue.push_back(r);
+  }
+  if (request_id) *request_id = r->id;
+  return VGB_OK;
+}
+
+vgb_status vgb_server_step(vgb_server *s, int64_t *completed, int32_t max_completed,
+                           int32_t *ncompleted, int64_t *live, int64_t *queued) {
+  if (!s) return set_error(VGB_EINVAL, "vgb_server_step: server is NULL");
+  if (ncompleted) *ncompleted = 0;
+  int dev = -1;
+  cudaGetDevice(&dev);
+  if (dev != s->device)
+    return set_error(VGB_EINVAL, "vgb_server_step: current device is not the server's");
+  vgb_status st = admit(s);
+  if (st != VGB_OK) return st;
+  // chunk list of every admitted request
+  std::vector<int32_t> list;
+  std::vector<std::pair<size_t, size_t>> span(s->active.size());
+  for (size_t k = 0; k < s->active.size(); ++k) {
+    span[k].first = list.size();
+    list.insert(list.end(), s->active[k]->chunks.begin(), s->active[k]->chunks.end());
+    span[k].second = list.size();
+  }
+  std::vector<int32_t> live_h(list.size(), 0);
+  int64_t live_total = 0;
+  if (!list.empty()) {
+    cudaError_t e = cudaMemcpyAsync(s->d_chunks, list.data(), list.size() * sizeof(int32_t),
+                                    cudaMemcpyHostToDevice, s->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(s->d_live, 0, list.size() * sizeof(int32_t), s->stream);
+    if (e != cudaSuccess) return cuda_error(e, "vgb_server_step: chunk list");
+    const int64_t nt = (int64_t)list.size() * kChunk;
+    if (s->all_shapes)
+      launch_step<kNavMaskAll>(s, nt);
+    else
+      launch_step<kNavMaskBoxTubeTrd>(s, nt);
+    count_launch();
+    e = cudaGetLastError();
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(live_h.data(), s->d_live, list.size() * sizeof(int32_t),
+                          cudaMemcpyDeviceToHost, s->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    if (e != cudaSuccess) return cuda_error(e, "vgb_server_step: step");
+  }
+  // retire
+  std::vector<Request *> still;
+  int32_t nc = 0;
+  for (size_t k = 0; k < s->active.size(); ++k) {
+    int64_t l = 0;
+    for (size_t c = span[k].first; c < span[k].second; ++c) l += live_h[c];
+    live_total += l;
+    Request *r = s->active[k];
+    if (l == 0) {
+      r->finished = true;
+      s->done[r->id] = r;
+      if (completed && nc < max_completed) completed[nc] = r->id;
+      ++nc;
+    } else {
+      still.push_back(r);
+    }
+  }
+  s->active.swap(still);
+  if (ncompleted) *ncompleted = std::min(nc, max_completed);
+  if (live) *live = live_total;
+  if (queued) *queued = (int64_t)s->queue.size();
+  return VGB_OK;
+}
+
+vgb_status vgb_server_result(vgb_server *s, int64_t request_id, int32_t *nsteps, double *x,
+                             double *y, double *z, uint64_t *hash) {
+  if (!s) return set_error(VGB_EINVAL, "vgb_server_result: server is NULL");
+  auto it = s->done.find(request_id);
+  if (it == s->done.end())
+    return set_error(VGB_EINVAL, "vgb_server_result: request %lld is not finished",
+                     (long long)request_id);
+  Request *r = it->second;
+  cudaError_t e = cudaSuccess;
+  for (size_t c = 0; c < r->chunks.size() && e == cudaSuccess; ++c) {
+    const int64_t first = (int64_t)c * kChunk, cnt = std::min<int64_t>(kChunk, r->n - first);
+    if (cnt <= 0) break;
+    const int64_t src = (int64_t)r->chunks[c] * kChunk;
+    if (nsteps && e == cudaSuccess)
+      e = cudaMemcpyAsync(nsteps + first, s->S.nsteps + src, cnt * 4, cudaMemcpyDeviceToHost, s->stream);
+    if (x && e == cudaSuccess)
+      e = cudaMemcpyAsync(x + first, s->S.x + src, cnt * 8, cudaMemcpyDeviceToHost, s->stream);
+    if (y && e == cudaSuccess)
+      e = cudaMemcpyAsync(y + first, s->S.y + src, cnt * 8, cudaMemcpyDeviceToHost, s->stream);
+    if (z && e == cudaSuccess)
+      e = cudaMemcpyAsync(z + first, s->S.z + src, cnt * 8, cudaMemcpyDeviceToHost, s->stream);
+    if (hash && e == cudaSuccess)
+      e = cudaMemcpyAsync(hash + first, s->S.hash + src, cnt * 8, cudaMemcpyDeviceToHost, s->stream);
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+  if (e != cudaSuccess) return cuda_error(e, "vgb_server_result");
+  for (int32_t c : r->chunks) s->free_chunks.push_back(c);
+  s->done.erase(it);
+  delete r;
+  return VGB_OK;
+}
+
+}  // extern "C"

@@ -447,3 +447,57 @@ class BasketPlan:
 
     def replay(self, stream=None) -> None:
         check(self.geometry.L.vgb_basket_graph_launch(self.handle, _stream(stream)))
+
+
+# ---------------------------------------------------------------------------
+# navigation server: continuous batching of track baskets (vgb_server_*)
+# ---------------------------------------------------------------------------
+class NavServer:
+    """Requests of straight tracks (host arrays) served by continuous batching;
+    see vgb_server_* in include/vgb.h."""
+
+    def __init__(self, geometry: "Geometry", max_tracks: int = 0, steps_per_launch: int = 8,
+                 max_steps: int = 1000, pstep: float = 1e30):
+        geometry._require_closed()
+        self.geometry = geometry
+        h = ctypes.c_void_p()
+        check(geometry.L.vgb_server_create(geometry.handle, max_tracks, steps_per_launch,
+                                           max_steps, pstep, ctypes.byref(h)))
+        self.handle = h
+        mt, nb = ctypes.c_int64(), ctypes.c_int64()
+        check(geometry.L.vgb_server_info(h, ctypes.byref(mt), ctypes.byref(nb)))
+        self.max_tracks = mt.value
+        self.device_bytes = nb.value
+        self._sizes = {}
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h is not None:
+            self.geometry.L.vgb_server_destroy(h)
+            self.handle = None
+
+    def submit(self, points, dirs) -> int:
+        arrs = [np.ascontiguousarray(a, np.float64) for a in (*points, *dirs)]
+        rid = ctypes.c_int64()
+        check(self.geometry.L.vgb_server_submit(self.handle, len(arrs[0]),
+                                                *(a.ctypes.data for a in arrs), ctypes.byref(rid)))
+        self._sizes[rid.value] = len(arrs[0])
+        return rid.value
+
+    def step(self, max_completed: int = 4096):
+        """One iteration; returns (completed request ids, live tracks, queued requests)."""
+        out = (ctypes.c_int64 * max_completed)()
+        nc, live, queued = ctypes.c_int32(), ctypes.c_int64(), ctypes.c_int64()
+        check(self.geometry.L.vgb_server_step(self.handle, out, max_completed, ctypes.byref(nc),
+                                              ctypes.byref(live), ctypes.byref(queued)))
+        return [out[k] for k in range(nc.value)], live.value, queued.value
+
+    def result(self, rid: int) -> dict:
+        n = self._sizes.get(rid, 0)
+        res = {"nsteps": np.zeros(n, np.int32), "x": np.zeros(n), "y": np.zeros(n),
+               "z": np.zeros(n), "hash": np.zeros(n, np.uint64)}
+        check(self.geometry.L.vgb_server_result(self.handle, rid,
+                                                *(res[k].ctypes.data for k in
+                                                  ("nsteps", "x", "y", "z", "hash"))))
+        self._sizes.pop(rid, None)
+        return res
