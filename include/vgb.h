@@ -269,6 +269,30 @@ vgb_status vgb_basket_graph_capture(vgb_basket_plan *plan, const double *x, cons
                                     uint32_t flags);
 vgb_status vgb_basket_graph_launch(vgb_basket_plan *plan, void *stream);
 
+/* The basket launch of vgb_basket_run for callers that cannot allocate device
+ * memory: a framework that has handed the GPU's memory to its own pool at
+ * start-up, or an online event loop where a cudaMalloc could stall or fail in
+ * the middle of a run.  This entry point calls no cudaMalloc/cudaFree and no
+ * allocating routine, on the device or the host.  The basket tables live in a
+ * fixed array compiled into the library (one per GPU, about 450 KB, held until the
+ * process exits), so it takes at most VGB_NOALLOC_MAX_BASKETS baskets and
+ * returns VGB_ENOSPC beyond that.  It has no counterpart in the reference.
+ *
+ *  - baskets is a host array; it is read (copied to the device) before the call
+ *    returns.  Launch shape: 256 threads per CTA, 1024 points per tile.
+ *  - The first call on each device looks up the array's device address; make
+ *    that first call from a thread whose current device is the geometry's.
+ *  - Every call reuses the same array and leaves its tables in it; nothing in
+ *    it needs to start at zero, since each call writes every entry it reads.
+ *    Calls whose work overlaps on the GPU (two streams, or two threads) race
+ *    on the array: issue them on one stream, or wait for one before the next. */
+enum { VGB_NOALLOC_MAX_BASKETS = 8192 };
+vgb_status vgb_basket_run_noalloc(const vgb_geometry *g, const vgb_basket *baskets, int32_t nb,
+                                  uint32_t ops, const double *x, const double *y,
+                                  const double *z, const double *dx, const double *dy,
+                                  const double *dz, const double *step_max, void *const *outs,
+                                  uint32_t flags, void *stream);
+
 /* ---------------------------------------------------------------------------
  * Navigation (navigation/SimpleNavigator.h, NavigationState.h, NavStatePool.h).
  *

@@ -93,6 +93,7 @@ SIGNATURES = {
                                                           ctypes.POINTER(ctypes.c_float)]),
     "vgb_basket_graph_capture": (ctypes.c_int, [_vp] + [_vp] * 8 + [_u32]),
     "vgb_basket_graph_launch": (ctypes.c_int, [_vp, _vp]),
+    "vgb_basket_run_noalloc": (ctypes.c_int, [_vp, _vp, _i32, _u32] + [_vp] * 8 + [_u32, _vp]),
     "vgb_server_create": (ctypes.c_int, [_vp, _i64, _i32, _i32, _dbl, ctypes.POINTER(_vp)]),
     "vgb_server_destroy": (ctypes.c_int, [_vp]),
     "vgb_server_info": (ctypes.c_int, [_vp, _pi64, _pi64]),
@@ -111,6 +112,7 @@ SIGNATURES = {
 }
 
 NAV_ERR_DEPTH = 1
+NOALLOC_MAX_BASKETS = 8192
 
 
 def lib():

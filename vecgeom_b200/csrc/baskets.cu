@@ -10,6 +10,7 @@
 // holds one shape, so the shape switch is uniform across the CTA.
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "batch.cuh"
@@ -392,3 +393,159 @@ vgb_status vgb_basket_graph_launch(vgb_basket_plan *p, void *stream) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// vgb_basket_run_noalloc: the basket launch with its tables in a fixed array
+// compiled into the library, for callers that cannot allocate device memory.
+// ---------------------------------------------------------------------------
+namespace vgb {
+namespace {
+
+constexpr int32_t kNoallocMax = VGB_NOALLOC_MAX_BASKETS;
+constexpr int32_t kNoallocBlock = 256;
+constexpr int32_t kNoallocTile = 1024;
+// layout: the caller's vgb_basket records as copied, the resolved BasketRec
+// records, then the nb + 1 tile prefix
+constexpr size_t kNoallocRawOff = 0;
+constexpr size_t kNoallocRecOff = kNoallocRawOff + sizeof(vgb_basket) * kNoallocMax;
+constexpr size_t kNoallocPrefixOff = kNoallocRecOff + sizeof(BasketRec) * kNoallocMax;
+constexpr size_t kNoallocBytes = kNoallocPrefixOff + sizeof(int64_t) * (kNoallocMax + 1);
+static_assert(kNoallocRecOff % 16 == 0 && kNoallocPrefixOff % 16 == 0, "table alignment");
+
+// Every GPU that loads the library holds this array until the process exits.
+// In host code the name is only a stand-in: its device address comes from
+// cudaGetSymbolAddress, once per device.
+static __device__ __align__(256) unsigned char g_noalloc_tables[kNoallocBytes];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+void *g_noalloc_addr[kMaxDevices] = {};
+
+// Device address of the array on `dev` (the current device); looked up once.
+vgb_status noalloc_tables(int dev, unsigned char **p) {
+  if (dev < 0 || dev >= kMaxDevices)
+    return set_error(VGB_EINVAL, "vgb_basket_run_noalloc: device %d out of range", dev);
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_addr[dev]) {
+    void *ptr = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_tables);
+    if (e != cudaSuccess) return cuda_error(e, "vgb_basket_run_noalloc: cudaGetSymbolAddress");
+    g_noalloc_addr[dev] = ptr;
+  }
+  *p = static_cast<unsigned char *>(g_noalloc_addr[dev]);
+  return VGB_OK;
+}
+
+// Resolves the copied records into BasketRec and writes the tile prefix
+// (one CTA: every thread scans up to 8 consecutive baskets, then a block scan).
+__global__ void __launch_bounds__(1024)
+    k_noalloc_tables(const vgb_basket *raw, int32_t nb, const PlacedRec *placed, int32_t tile,
+                     BasketRec *rec, int64_t *prefix) {
+  __shared__ int64_t part[1024];
+  const int per = (nb + 1023) / 1024;
+  const int b0 = threadIdx.x * per;
+  int64_t sum = 0;
+  for (int k = 0; k < per; ++k) {
+    const int b = b0 + k;
+    if (b < nb) {
+      const vgb_basket r = raw[b];
+      const PlacedRec pr = placed[r.placed];
+      rec[b] = BasketRec{pr.unplaced, pr.xform, r.offset, r.count};
+      sum += (r.count + tile - 1) / tile;
+    }
+  }
+  part[threadIdx.x] = sum;
+  __syncthreads();
+  for (int o = 1; o < 1024; o <<= 1) {
+    const int64_t v = threadIdx.x >= (unsigned)o ? part[threadIdx.x - o] : 0;
+    __syncthreads();
+    part[threadIdx.x] += v;
+    __syncthreads();
+  }
+  int64_t run = threadIdx.x ? part[threadIdx.x - 1] : 0;
+  if (threadIdx.x == 0) prefix[0] = 0;
+  for (int k = 0; k < per; ++k) {
+    const int b = b0 + k;
+    if (b < nb) {
+      run += (raw[b].count + tile - 1) / tile;
+      prefix[b + 1] = run;
+    }
+  }
+}
+
+template <uint32_t kOps>
+void noalloc_launch(const vgb_geometry *g, const BasketRec *rec, const int64_t *prefix,
+                    int32_t nb, int64_t ntiles, const FusedIO &io, cudaStream_t s) {
+  const BasketGeom G = {g->dev.params, g->dev.unplaced, g->dev.xforms};
+  const int grid = (int)std::min<int64_t>(ntiles, occupancy_grid<kOps>(kNoallocBlock));
+  k_baskets<kNoallocBlock, kOps><<<grid, kNoallocBlock, 0, s>>>(G, rec, prefix, nb, ntiles,
+                                                                 kNoallocTile, io);
+}
+
+}  // namespace
+}  // namespace vgb
+
+extern "C" vgb_status vgb_basket_run_noalloc(const vgb_geometry *g, const vgb_basket *baskets,
+                                             int32_t nb, uint32_t ops, const double *x,
+                                             const double *y, const double *z, const double *dx,
+                                             const double *dy, const double *dz,
+                                             const double *step_max, void *const *outs,
+                                             uint32_t flags, void *stream) {
+  const char *fn = "vgb_basket_run_noalloc";
+  if (!g || !g->closed) return set_error(VGB_EINVAL, "%s: geometry not closed", fn);
+  if (nb < 0 || (nb > 0 && !baskets)) return set_error(VGB_EINVAL, "%s: bad basket array", fn);
+  if (nb > kNoallocMax)
+    return set_error(VGB_ENOSPC, "%s: %d baskets exceed the fixed table of %d", fn, nb,
+                     kNoallocMax);
+  if (ops == 0 || (ops & ~0x3fu))
+    return set_error(VGB_EINVAL, "%s: ops must be a mask over ops 0..5", fn);
+  if (!x || !y || !z || !outs) return set_error(VGB_EINVAL, "%s: points or outs are NULL", fn);
+  const uint32_t dist = (1u << VGB_OP_DISTANCE_TO_IN) | (1u << VGB_OP_DISTANCE_TO_OUT);
+  if ((ops & dist) && (!dx || !dy || !dz || !step_max))
+    return set_error(VGB_EINVAL, "%s: distances need directions and step_max", fn);
+  for (int k = 0; k < 6; ++k)
+    if (((ops >> k) & 1u) && !outs[k])
+      return set_error(VGB_EINVAL, "%s: output of op %d is NULL", fn, k);
+  int dev = -1;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_error(e, fn);
+  if (dev != g->device)
+    return set_error(VGB_EINVAL, "%s: current device %d is not the geometry's device %d", fn,
+                     dev, g->device);
+  int64_t ntiles = 0, npoints = 0;
+  for (int32_t b = 0; b < nb; ++b) {
+    const vgb_basket &k = baskets[b];
+    if (k.placed < 0 || k.placed >= (int32_t)g->placed.size() || k.offset < 0 || k.count < 0)
+      return set_error(VGB_EINVAL, "%s: basket %d is invalid", fn, b);
+    ntiles += (k.count + kNoallocTile - 1) / kNoallocTile;
+    npoints = std::max<int64_t>(npoints, k.offset + k.count);
+  }
+  if (ntiles == 0) return VGB_OK;
+  unsigned char *tables = nullptr;
+  vgb_status st = noalloc_tables(dev, &tables);
+  if (st != VGB_OK) return st;
+  cudaStream_t s = (cudaStream_t)stream;
+  vgb_basket *raw = reinterpret_cast<vgb_basket *>(tables + kNoallocRawOff);
+  BasketRec *rec = reinterpret_cast<BasketRec *>(tables + kNoallocRecOff);
+  int64_t *prefix = reinterpret_cast<int64_t *>(tables + kNoallocPrefixOff);
+  e = cudaMemcpyAsync(raw, baskets, sizeof(vgb_basket) * nb, cudaMemcpyHostToDevice, s);
+  if (e != cudaSuccess) return cuda_error(e, "vgb_basket_run_noalloc: basket copy");
+  k_noalloc_tables<<<1, 1024, 0, s>>>(raw, nb, g->dev.placed, kNoallocTile, rec, prefix);
+  FusedIO io;
+  std::memset(&io, 0, sizeof(io));
+  io.x = x; io.y = y; io.z = z;
+  io.dx = dx; io.dy = dy; io.dz = dz;
+  io.step = step_max;
+  for (int k = 0; k < 6; ++k) io.out[k] = ((ops >> k) & 1u) ? outs[k] : nullptr;
+  io.n = npoints;
+  io.ops = ops;
+  io.flags = flags;
+  if ((ops & ~kOpsDtiSti) == 0)
+    noalloc_launch<kOpsDtiSti>(g, rec, prefix, nb, ntiles, io, s);
+  else
+    noalloc_launch<kOpsAll>(g, rec, prefix, nb, ntiles, io, s);
+  count_launch(2);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_error(e, "vgb_basket_run_noalloc: kernel launch");
+  return VGB_OK;
+}
