@@ -95,6 +95,8 @@ vgb_status vgb_batch(const vgb_geometry *gc, int32_t placed, int32_t op, int64_t
   if (op < 0 || op >= VGB_OP_COUNT) return set_error(VGB_EINVAL, "vgb_batch: unknown op %d", op);
   if (precision != VGB_PREC_FP64 && precision != VGB_PREC_FP32_REFINE)
     return set_error(VGB_EINVAL, "vgb_batch: unknown precision %d", precision);
+  if (precision == VGB_PREC_FP32_REFINE)
+    return set_error(VGB_ENOTSUP, "vgb_batch: the FP32+refine form is not available");
   if (n < 0) return set_error(VGB_EINVAL, "vgb_batch: n < 0");
   if (n == 0) return VGB_OK;
   if (!x || !y || !z || !out) return set_error(VGB_EINVAL, "vgb_batch: NULL point or output");
@@ -184,6 +186,8 @@ vgb_status vgb_batch_fused(const vgb_geometry *gc, int32_t placed, uint32_t ops,
   if (ops & ~allowed) return set_error(VGB_EINVAL, "vgb_batch_fused: unsupported op mask 0x%x", ops);
   if (precision != VGB_PREC_FP64 && precision != VGB_PREC_FP32_REFINE)
     return set_error(VGB_EINVAL, "vgb_batch_fused: unknown precision %d", precision);
+  if (precision == VGB_PREC_FP32_REFINE)
+    return set_error(VGB_ENOTSUP, "vgb_batch_fused: the FP32+refine form is not available");
   if (n < 0) return set_error(VGB_EINVAL, "vgb_batch_fused: n < 0");
   if (n == 0 || ops == 0) return VGB_OK;
   if (!x || !y || !z || !outs) return set_error(VGB_EINVAL, "vgb_batch_fused: NULL argument");
