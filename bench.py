@@ -47,7 +47,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="vgb", choices=["vgb", "reference"])
-    ap.add_argument("--workload", default="shapes", choices=["shapes", "box", "baskets", "nav"])
+    ap.add_argument("--workload", default="shapes",
+                    choices=["shapes", "heavy", "box", "baskets", "nav"])
     ap.add_argument("--baskets", type=int, default=4096, help="baskets of the basket workload")
     ap.add_argument("--requests", type=int, default=300, help="requests of the nav workload")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32r"])
@@ -71,10 +72,17 @@ def workload_shapes(name: str):
     from vecgeom_b200 import workloads as W
     if name == "box":
         return {"box": W.config1_box()}, 1 << 20, "uniform"
+    if name == "heavy":
+        return W.config3_shapes(), 1 << 22, "mixed"
     return W.config2_shapes(), 1 << 22, "mixed"
 
 
 def workload_desc(name, n, precision):
+    if name == "heavy":
+        return {"workload": "torus/polycone/polyhedron/box-minus-tube, 2^22 mixed points each",
+                "shapes": ["torus(0,5,50)", "polycone(10 planes, phi 0-300deg)",
+                           "polyhedron(8 sides, 6 planes, 10/40)", "box(30,30,30)-tube(15,dz 40)"],
+                "points_per_shape": n, "ops": list(OPS), "precision": precision}
     if name == "box":
         return {"workload": "box (10,20,30) mm fp64, 2^20 uniform points in 1.5x box",
                 "points_per_shape": n, "ops": list(OPS), "precision": precision}

@@ -22,7 +22,7 @@ struct BatchIO {
   int32_t *aux;
   int64_t n;
   int32_t daughter;
-  int32_t pad;
+  int32_t stage;  // doubles of the shape record staged in shared memory (0: none)
 };
 
 // Fused: the outputs of every op of the mask, one read of the inputs.
@@ -37,6 +37,26 @@ struct FusedIO {
 };
 
 template <class T> VGB_D T ldg(const T *p) { return __ldg(p); }
+
+// Shapes whose tables hang off the record (polycone sections, polyhedron
+// segments and quadrilaterals) can run with the record and its tables staged in
+// shared memory: every thread of a block reads the same table entries, which a
+// shared-memory copy serves without the global-load latency.
+template <class P> struct Stageable : std::false_type {};
+template <> struct Stageable<PolyconeP> : std::true_type {};
+template <> struct Stageable<PolyhedronP> : std::true_type {};
+constexpr int kStageMaxDoubles = 6144;  // 48 KB of dynamic shared memory
+extern __shared__ double vgb_stage[];
+
+// Distance kernels carry the most live state; they are compiled for four
+// resident 256-thread blocks per SM (64 registers); the others keep the
+// compiler's own choice (0: no minimum).
+template <int OP> struct MinBlocks {
+  static constexpr int value =
+      (OP == VGB_OP_DISTANCE_TO_IN || OP == VGB_OP_DISTANCE_TO_OUT ||
+       OP == VGB_OP_DISTANCE_TO_IN_MINIMIZE || OP == VGB_OP_DISTANCE_TO_OUT_NODE ||
+       OP == VGB_OP_PLACED_DISTANCE_TO_OUT) ? 4 : 0;
+};
 
 template <class Ops, class P, int OP>
 __device__ __forceinline__ void batch_point(const P &prm, const DXform &X, const BatchIO &io,
@@ -95,11 +115,26 @@ __device__ __forceinline__ void batch_point(const P &prm, const DXform &X, const
 }
 
 template <class Ops, class P, int OP>
-__global__ void __launch_bounds__(kBatchBlock) k_batch(const P prm, const DXform X,
-                                                       const BatchIO io) {
+__device__ __forceinline__ void batch_loop(const P &prm, const DXform &X, const BatchIO &io) {
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < io.n; i += stride)
     batch_point<Ops, P, OP>(prm, X, io, i);
+}
+
+template <class Ops, class P, int OP>
+__global__ void __launch_bounds__(kBatchBlock, MinBlocks<OP>::value)
+    k_batch(const P prm, const DXform X, const BatchIO io) {
+  if constexpr (Stageable<P>::value) {
+    if (io.stage > 0) {
+      for (int k = threadIdx.x; k < io.stage; k += blockDim.x) vgb_stage[k] = prm.base[k];
+      __syncthreads();
+      P sp = prm;
+      sp.base = vgb_stage;
+      batch_loop<Ops, P, OP>(sp, X, io);
+      return;
+    }
+  }
+  batch_loop<Ops, P, OP>(prm, X, io);
 }
 
 // All requested ops for one point.  With VGB_FUSED_DTO_INSIDE_ONLY the

@@ -17,13 +17,15 @@ static int grid_for(int64_t n) {
 }
 
 template <class Ops, class P>
-static vgb_status launch_ops(const P &prm, const DXform &X, int op, const BatchIO &io,
-                             cudaStream_t s) {
+static vgb_status launch_ops(const P &prm, const DXform &X, int op, BatchIO io, cudaStream_t s,
+                             int32_t rec_len = 0) {
   const int grid = grid_for(io.n);
+  io.stage = (Stageable<P>::value && rec_len > 0 && rec_len <= kStageMaxDoubles) ? rec_len : 0;
+  const size_t smem = (size_t)io.stage * sizeof(double);
   switch (op) {
 #define VGB_OP_CASE(OPC)                                                      \
   case OPC:                                                                   \
-    k_batch<Ops, P, OPC><<<grid, kBatchBlock, 0, s>>>(prm, X, io);            \
+    k_batch<Ops, P, OPC><<<grid, kBatchBlock, smem, s>>>(prm, X, io);         \
     break;
     VGB_OP_CASE(VGB_OP_CONTAINS)
     VGB_OP_CASE(VGB_OP_INSIDE)
@@ -84,7 +86,8 @@ vgb_status launch_batch_f64(const vgb_geometry *g, int32_t placed, int op, const
 #define VGB_SHAPE_CASE(TYPE, OPS, P) \
   case TYPE:                         \
     return launch_ops<OPS<double>>(                                                     \
-        bind_params(*static_cast<const P *>(prm), shape_params_dev(g, pr.unplaced)), X, op, io, s);
+        bind_params(*static_cast<const P *>(prm), shape_params_dev(g, pr.unplaced)), X, op, io, s, \
+        g->unplaced[pr.unplaced].param_len);
     VGB_FOR_EACH_SHAPE(VGB_SHAPE_CASE)
 #undef VGB_SHAPE_CASE
   default:

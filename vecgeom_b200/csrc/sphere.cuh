@@ -104,7 +104,17 @@ template <class R> struct SphereOps {
 
     const R rho2 = p.x * p.x + p.y * p.y;
     const R rad2 = rho2 + p.z * p.z;
-    const R pTheta = atan2(sqrt(rho2), p.z);
+    // polar angle of the point, computed on first use (only the theta-cone
+    // branches read it; the value is the reference's atan2(sqrt(rho2), z))
+    R pThetaV = 0;
+    bool pThetaSet = false;
+    auto pTheta = [&]() {
+      if (!pThetaSet) {
+        pThetaV = atan2(sqrt(rho2), p.z);
+        pThetaSet = true;
+      }
+      return pThetaV;
+    };
     const R pDotV2d = p.x * v.x + p.y * v.y;
     const R pDotV3d = pDotV2d + p.z * v.z;
     if (!s.fullTheta) {
@@ -113,7 +123,7 @@ template <class R> struct SphereOps {
     }
     auto theta_in = [&](R th) { return (th >= tolSTheta) && (th <= tolETheta); };
     auto strictly_theta = [&]() {
-      return (pTheta >= tolSTheta + kAng) && (pTheta <= tolETheta - kAng);
+      return (pTheta() >= tolSTheta + kAng) && (pTheta() <= tolETheta - kAng);
     };
 
     // outer sphere (:667-760)
@@ -287,7 +297,7 @@ template <class R> struct SphereOps {
         }
       };
       const R tanS2 = (R)s.tanSTheta2, tanE2 = (R)s.tanETheta2;
-      if (pTheta < tolSTheta) {
+      if (pTheta() < tolSTheta) {
         t1 = (R)1 - v.z * v.z * ((R)1 + tanS2);
         t2 = pDotV2d - p.z * v.z * tanS2;
         if (t1 != 0) {
@@ -316,7 +326,7 @@ template <class R> struct SphereOps {
             }
           }
         }
-      } else if (pTheta > tolETheta) {
+      } else if (pTheta() > tolETheta) {
         t1 = (R)1 - v.z * v.z * ((R)1 + tanE2);
         t2 = pDotV2d - p.z * v.z * tanE2;
         if (t1 != 0) {
@@ -345,7 +355,7 @@ template <class R> struct SphereOps {
             }
           }
         }
-      } else if ((pTheta < tolSTheta + kAng) && (fSTheta > halfAngTol)) {
+      } else if ((pTheta() < tolSTheta + kAng) && (fSTheta > halfAngTol)) {
         t2 = pDotV2d - p.z * v.z * tanS2;
         if ((t2 >= 0 && tolIRMin2 < rad2 && rad2 < tolIRMax2 && s.stheta < kPi / 2) ||
             (t2 < 0 && tolIRMin2 < rad2 && rad2 < tolIRMax2 && s.stheta > kPi / 2) ||
@@ -367,7 +377,7 @@ template <class R> struct SphereOps {
             if ((sd >= halfCarTol) && (sd < snxt) && (s.stheta < kPi / 2)) accept(sd, fSTheta);
           }
         }
-      } else if ((pTheta > tolETheta - kAng) && (s.eTheta < kPi - kAngTolerance)) {
+      } else if ((pTheta() > tolETheta - kAng) && (s.eTheta < kPi - kAngTolerance)) {
         t2 = pDotV2d - p.z * v.z * tanE2;
         if (((t2 < 0) && (s.eTheta < kPi / 2) && (tolIRMin2 < rad2) && (rad2 < tolIRMax2)) ||
             ((t2 >= 0) && (s.eTheta > kPi / 2) && (tolIRMin2 < rad2) && (rad2 < tolIRMax2)) ||
