@@ -367,7 +367,9 @@ def run_nav(args):
     """Layered detector (14,011 placed volumes).  Requests of 1-16384 tracks
     (log-uniform sizes) from the origin, isotropic, arrive as a Poisson stream
     at ~80% of the measured saturated throughput; each track steps (safety +
-    FindNextBoundaryAndStep) until it leaves the world or 64 steps."""
+    FindNextBoundaryAndStep) until it leaves the world or 64 steps.  The served
+    run uses --precision; the other form is served with the same arrivals for
+    comparison, and the raw trace throughput of both forms is reported."""
     import torch
     import vecgeom_b200 as V
     from vecgeom_b200 import workloads as W
@@ -379,21 +381,21 @@ def run_nav(args):
     nreq = args.requests
     sizes = np.clip(np.round(np.exp(rng.uniform(0., np.log(16384.), nreq))), 1, 16384).astype(int)
     reqs = [W.isotropic_tracks(int(m), W.SEED_BASE + 500 + k) for k, m in enumerate(sizes)]
-    srv = V.NavServer(g, max_tracks=1 << 18, steps_per_launch=spl, max_steps=max_steps)
+    prec_main = V.PREC_FP64 if args.precision == "fp64" else V.PREC_FP32_REFINE
 
-    def drain(submit_times, arrivals=None):
-        """Runs until every request finished; submits request k when the wall
-        clock passes arrivals[k] (None: all at once).  Returns latencies and
-        total steps."""
+    def drain(srv, arrivals=None):
+        """Serves every request; request k is submitted when the wall clock
+        passes arrivals[k] (None: all at once).  Returns latencies (s), total
+        steps and wall time."""
         t0 = time.perf_counter()
         pending = list(range(nreq))
         lat, steps, done_n = {}, 0, 0
-        rid_of = {}
+        rid_of, sub = {}, {}
         while done_n < nreq:
             now = time.perf_counter() - t0
             while pending and (arrivals is None or arrivals[pending[0]] <= now):
                 k = pending.pop(0)
-                submit_times[k] = t0 + (arrivals[k] if arrivals is not None else now)
+                sub[k] = t0 + (arrivals[k] if arrivals is not None else now)
                 rid_of[srv.submit(*reqs[k])] = k
             done, live, queued = srv.step()
             tdone = time.perf_counter()
@@ -401,41 +403,75 @@ def run_nav(args):
                 k = rid_of.pop(rid)
                 r = srv.result(rid)
                 steps += int(r["nsteps"].sum())
-                lat[k] = tdone - submit_times[k]
+                lat[k] = tdone - sub[k]
                 done_n += 1
             if not done and not live and not queued and pending and arrivals is not None:
                 time.sleep(max(0., min(0.002, arrivals[pending[0]] - now)))
         return lat, steps, time.perf_counter() - t0
 
-    # saturated throughput (all requests queued at once) sets the arrival rate
-    sub = [0.] * nreq
-    drain(sub)  # warm-up
-    _, sat_steps, sat_s = drain(sub)
-    mean_steps = sat_steps / nreq
-    rate = 0.8 * (sat_steps / sat_s) / mean_steps      # requests per second
+    def serve(precision, arrivals):
+        srv = V.NavServer(g, max_tracks=1 << 18, steps_per_launch=spl, max_steps=max_steps,
+                          precision=precision)
+        drain(srv)  # warm-up
+        if arrivals is None:
+            _, st, wall = drain(srv)
+            return st, wall, None
+        lat, st, wall = drain(srv, arrivals)
+        L = np.array([lat[k] for k in range(nreq)]) * 1e3
+        return st, wall, {"p50": round(float(np.percentile(L, 50)), 3),
+                          "p99": round(float(np.percentile(L, 99)), 3),
+                          "max": round(float(L.max()), 3)}
+
+    # saturated throughput of the FP64 form sets one arrival stream for both forms
+    sat_steps, sat_s, _ = serve(V.PREC_FP64, None)
+    rate = 0.8 * (sat_steps / sat_s) / (sat_steps / nreq)      # requests per second
     arrivals = np.cumsum(rng.exponential(1. / rate, nreq))
+    other = V.PREC_FP32_REFINE if prec_main == V.PREC_FP64 else V.PREC_FP64
+    o_steps, o_wall, o_lat = serve(other, arrivals)
     clk = ClockSampler(torch.cuda.current_device())
     V.lib().vgb_launch_count_reset()
     clk.start()
-    lat, steps, wall = drain(sub, arrivals)
+    steps, wall, lat = serve(prec_main, arrivals)
     clocks = clk.stop()
     launches = int(V.lib().vgb_launch_count())
-    L = np.array([lat[k] for k in range(nreq)]) * 1e3
-    line = {"metric": "nav steps/s (fp64, served) with p50/p99 request latency",
+    sat32_steps, sat32_s, _ = serve(V.PREC_FP32_REFINE, None)
+    # raw trace throughput (one launch, 2^17 tracks, device events)
+    n = 1 << 17
+    pts, dirs = W.isotropic_tracks(n, W.SEED_BASE + 7)
+    dev = lambda a: torch.from_numpy(a).cuda()  # noqa: E731
+    P, D = V.SOA3D(*(dev(a) for a in pts)), V.SOA3D(*(dev(a) for a in dirs))
+    nst = torch.zeros(n, dtype=torch.int32, device="cuda")
+    nav = V.SimpleNavigator(g)
+    trace = {}
+    for name, pr in (("fp64", V.PREC_FP64), ("fp32r", V.PREC_FP32_REFINE)):
+        for _ in range(2):
+            nav.Trace(P, D, 1e30, max_steps, nst, precision=pr)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        nav.Trace(P, D, 1e30, max_steps, nst, precision=pr)
+        e1.record()
+        torch.cuda.synchronize()
+        trace[name] = round(int(nst.sum()) / (e0.elapsed_time(e1) * 1e-3), 1)
+    tag = "fp64" if prec_main == V.PREC_FP64 else "fp32+refine"
+    line = {"metric": f"nav steps/s ({tag}, served) with p50/p99 request latency",
             "value": round(steps / wall, 1), "unit": "steps/s", "n_gpus": 1,
             "steps": nreq, "warmup": 1, "ms_per_step": round(wall / nreq * 1e3, 4),
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if prec_main == V.PREC_FP64 else "f32+f64",
             "data": "synthetic (seeded)",
             "config": {"workload": "layered detector, 14011 placed volumes, 4 levels; "
                                    f"{nreq} requests of 1-16384 tracks (log-uniform) from the "
-                                   "origin, Poisson arrivals at 80% of saturated throughput",
+                                   "origin, Poisson arrivals at 80% of the FP64 saturated "
+                                   "throughput",
                        "max_steps": max_steps, "steps_per_launch": spl,
-                       "slots": srv.max_tracks, "tracks": int(sizes.sum()),
-                       "saturated_steps_per_s": round(sat_steps / sat_s, 1),
+                       "tracks": int(sizes.sum()),
+                       "saturated_steps_per_s": {"fp64": round(sat_steps / sat_s, 1),
+                                                 "fp32r": round(sat32_steps / sat32_s, 1)},
                        "arrival_rate_per_s": round(rate, 2)},
-            "latency_ms": {"p50": round(float(np.percentile(L, 50)), 3),
-                           "p99": round(float(np.percentile(L, 99)), 3),
-                           "max": round(float(L.max()), 3)},
+            "latency_ms": lat,
+            "other_precision": {"precision": "fp32+refine" if other else "fp64",
+                                "steps_per_s": round(o_steps / o_wall, 1), "latency_ms": o_lat},
+            "trace_steps_per_s": trace,
             "e2e": {"value": round(steps / wall, 1), "unit": "steps/s",
                     "h2d_bytes_per_step": int(48 * sizes.sum() / nreq),
                     "d2h_bytes_per_step": int(36 * sizes.sum() / nreq)},
@@ -495,6 +531,7 @@ def main():
         return torch.from_numpy(np.ascontiguousarray(a)).cuda()
 
     tasks = []   # (shape, opname, n, callable on device, callable on host)
+    checks = []  # (shape, opname, output, FP64 output, FP64 call) for the error report
     h2d_bytes = d2h_bytes = 0
     for si, (name, spec) in enumerate(shapes.items()):
         wl = W.make_workload(spec, n, W.SEED_BASE + 1000 * rank + si, mix=mix)
@@ -530,6 +567,13 @@ def main():
                     "safety_to_out": "SafetyToOut", "distance_to_in": "DistanceToIn",
                     "distance_to_out": "DistanceToOut"}[opname]
             fn = getattr(pv, meth)
+            out64 = torch.empty_like(out_d)
+            if opname.startswith("distance"):
+                run64 = (lambda fn=fn, a=pts_d, b=dirs_d, s=st_d, o=out64:
+                         fn(a, b, s, o, precision=V.PREC_FP64))
+            else:
+                run64 = lambda fn=fn, a=pts_d, o=out64: fn(a, o, precision=V.PREC_FP64)  # noqa
+            checks.append((name, opname, out_d, out64, run64))
             if opname.startswith("distance"):
                 run_d = (lambda fn=fn, a=pts_d, b=dirs_d, s=st_d, o=out_d:
                          fn(a, b, s, o, precision=prec))
@@ -630,6 +674,23 @@ def main():
 
     per_op = {f"{t[0]}:{t[1]}": round(t[2] / (per_task_ms[i] / args.steps * 1e-3) / 1e6, 1)
               for i, t in enumerate(tasks)}
+    # FP32+refine: error of every op against the FP64 form on the same points
+    err = None
+    if args.precision != "fp64":
+        err = {}
+        for t, (name, opname, o, o64, run64) in zip(tasks, checks):
+            t[3]()
+            run64()
+            torch.cuda.synchronize()
+            a, b = o.double(), o64.double()
+            both = torch.isfinite(a) & torch.isfinite(b)
+            dif = torch.where(both, (a - b).abs(), torch.zeros_like(a))
+            bad = ~(both | ((a == b) | (a.isnan() & b.isnan())))
+            err[f"{name}:{opname}"] = {
+                "max_mm": float(dif.max().item()) if dif.numel() else 0.,
+                "p99_mm": float(torch.quantile(dif[:1 << 24].float(), .99).item())
+                if dif.numel() else 0.,
+                "class_mismatches": int(bad.sum().item())}
     line = {"metric": "Mpoints/s per shape op" + (" (fp64)" if args.precision == "fp64"
                                                   else " (fp32+refine)"),
             "value": round(value, 2), "unit": "Mpoints/s", "n_gpus": world,
@@ -640,6 +701,7 @@ def main():
             "config": dict(workload_desc(args.workload, n, args.precision),
                            l2="flushed (256 MB read sweep) before every op, outside the events"),
             "per_op_mpoints_s": per_op, "roofline": roof, "e2e": e2e,
+            "error_vs_fp64": err,
             "gpu_launches": launches, "clocks": clk}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_rate(shapes, n, W.SEED_BASE + 2)

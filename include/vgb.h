@@ -332,13 +332,19 @@ vgb_status vgb_nav_locate(const vgb_geometry *g, int64_t n, const double *x, con
  * points and directions, current states `cur`, proposed steps pstep[i]; writes
  * the new states into `next` and the steps into step[i].  If safety is not
  * NULL, safety[i] receives SimpleNavigator::GetSafety (:572-596) at the point
- * in the current state.  cur and next must be different pools. */
+ * in the current state.  cur and next must be different pools.
+ * precision VGB_PREC_FP32_REFINE puts a float screen in front of the daughter
+ * loops (a daughter whose widened box the ray misses or enters beyond the
+ * running best step is not evaluated, nor a box daughter whose float safety is
+ * certainly above the running minimum; the culling of ABBoxNavigator,
+ * navigation/ABBoxNavigator.h:148-452); results equal the FP64 form's. */
 vgb_status vgb_nav_find_next_boundary_and_step(const vgb_geometry *g, int64_t n, const double *x,
                                                const double *y, const double *z,
                                                const double *dx, const double *dy,
                                                const double *dz, const vgb_navpool *cur,
                                                vgb_navpool *next, const double *pstep,
-                                               double *step, double *safety, void *stream);
+                                               double *step, double *safety, int32_t precision,
+                                               void *stream);
 
 /* Transport of n straight tracks from their start points to the world exit:
  * LocatePoint from the world, then per step GetSafety, FindNextBoundaryAndStep
@@ -352,7 +358,7 @@ vgb_status vgb_nav_find_next_boundary_and_step(const vgb_geometry *g, int64_t n,
 vgb_status vgb_nav_trace(const vgb_geometry *g, int64_t n, const double *x, const double *y,
                          const double *z, const double *dx, const double *dy, const double *dz,
                          double pstep, int32_t max_steps, int32_t *next_ids, double *steps,
-                         double *safeties, int32_t *nsteps, void *stream);
+                         double *safeties, int32_t *nsteps, int32_t precision, void *stream);
 
 /* Navigation error flags (VGB_NAV_ERR_*) raised since the last call; clears them. */
 vgb_status vgb_nav_error_flags(const vgb_geometry *g, uint32_t *flags);
@@ -378,7 +384,8 @@ typedef struct vgb_server vgb_server;
 /* max_tracks = 0 sizes the slots to a quarter of the free device memory
  * (at most 2^22 tracks).  Fails with VGB_ENOMEM when the slots do not fit. */
 vgb_status vgb_server_create(const vgb_geometry *g, int64_t max_tracks, int32_t steps_per_launch,
-                             int32_t max_steps, double pstep, vgb_server **server);
+                             int32_t max_steps, double pstep, int32_t precision,
+                             vgb_server **server);
 vgb_status vgb_server_destroy(vgb_server *server);
 /* slot capacity (tracks) and device bytes held */
 vgb_status vgb_server_info(const vgb_server *server, int64_t *max_tracks, int64_t *device_bytes);

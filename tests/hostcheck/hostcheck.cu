@@ -63,15 +63,34 @@ extern "C" int hc_batch(const vgb_geometry *g, int32_t placed, int32_t op, int64
 
 // The navigator of navigation.cuh with a single lane, over the host tables of an
 // (unclosed) geometry: the same loop as vgb_nav_trace's kernel.
+template <class Nav>
+int trace_host(const NavGeom &G, int64_t n, const double *x, const double *y, const double *z,
+               const double *dx, const double *dy, const double *dz, double pstep,
+               int32_t max_steps, int32_t *next_ids, double *steps, double *safeties,
+               int32_t *nsteps);
+
 extern "C" int hc_nav_trace(vgb_geometry *g, int64_t n, const double *x, const double *y,
                             const double *z, const double *dx, const double *dy,
                             const double *dz, double pstep, int32_t max_steps, int32_t *next_ids,
-                            double *steps, double *safeties, int32_t *nsteps) {
+                            double *steps, double *safeties, int32_t *nsteps, int32_t screen) {
   if (prepare_tables(g) != VGB_OK) return -1;
-  const NavGeom G = {g->params.data(),   g->unplaced.data(), g->placed.data(),
-                     g->xforms.data(),   g->nav_raw.data(),  g->logicals.data(),
-                     g->daughters.data(), g->world,          g->max_depth};
-  using Nav = Navigator<OneLane, kNavMaskAll>;
+  const NavGeom G = {g->params.data(),    g->unplaced.data(), g->placed.data(),
+                     g->xforms.data(),    g->nav_raw.data(),  g->logicals.data(),
+                     g->daughters.data(), g->pl_box.data(),   g->world,
+                     g->max_depth};
+  if (screen) return trace_host<Navigator<OneLane, kNavMaskAll, true>>(G, n, x, y, z, dx, dy, dz, pstep,
+                                                                       max_steps, next_ids, steps,
+                                                                       safeties, nsteps);
+  return trace_host<Navigator<OneLane, kNavMaskAll, false>>(G, n, x, y, z, dx, dy, dz, pstep,
+                                                            max_steps, next_ids, steps, safeties,
+                                                            nsteps);
+}
+
+template <class Nav>
+int trace_host(const NavGeom &G, int64_t n, const double *x, const double *y, const double *z,
+               const double *dx, const double *dy, const double *dz, double pstep,
+               int32_t max_steps, int32_t *next_ids, double *steps, double *safeties,
+               int32_t *nsteps) {
   for (int64_t i = 0; i < n; ++i) {
     V3<double> p = {x[i], y[i], z[i]};
     const V3<double> d = {dx[i], dy[i], dz[i]};

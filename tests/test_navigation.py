@@ -63,11 +63,11 @@ def hc():
     vp = ctypes.c_void_p
     L.hc_nav_trace.restype = ctypes.c_int
     L.hc_nav_trace.argtypes = ([vp, ctypes.c_int64] + [vp] * 6 + [ctypes.c_double, ctypes.c_int32]
-                               + [vp] * 4)
+                               + [vp] * 4 + [ctypes.c_int32])
     return L
 
 
-def host_trace(L, pts, dirs, max_steps, pstep=1e30):
+def host_trace(L, pts, dirs, max_steps, pstep=1e30, screen=0):
     g = Geometry(library=L)
     placed = W.build_detector(W.VgbBuilder(g, close=False))
     assert [p.id for p in placed] == list(range(len(placed)))
@@ -78,7 +78,7 @@ def host_trace(L, pts, dirs, max_steps, pstep=1e30):
     nst = np.zeros(n, np.int32)
     a = lambda v: np.ascontiguousarray(v).ctypes.data  # noqa: E731
     rc = L.hc_nav_trace(g.handle, n, *(a(v) for v in pts), *(a(v) for v in dirs), pstep,
-                        max_steps, a(ids), a(steps), a(saf), a(nst))
+                        max_steps, a(ids), a(steps), a(saf), a(nst), screen)
     assert rc == 0
     return ids, steps, saf, nst, g
 
@@ -89,16 +89,19 @@ def test_detector_layout(hc):
     assert len(placed) == W.DetectorSpec().placed_count() == 14011
 
 
-def test_host_navigator_matches_golden(hc):
+@pytest.mark.parametrize("screen", [0, 1], ids=["fp64", "fp32_screen"])
+def test_host_navigator_matches_golden(hc, screen):
+    """Both forms: the float screen of FP32+refine must not change a record."""
     d, pts, dirs = load_golden()
     ms = int(d["max_steps"])
-    ids, steps, saf, nst, _ = host_trace(hc, pts, dirs, ms)
+    ids, steps, saf, nst, _ = host_trace(hc, pts, dirs, ms, screen=screen)
     assert_traces_equal((ids, steps, saf, nst),
                         (d["next_ids"], d["steps"], d["safeties"], d["nsteps"]), ms, "host")
 
 
 @pytest.mark.skipif(not oracle.RefLib.available(), reason="oracle/_ref not built")
-def test_host_navigator_matches_reference_long_traces(hc):
+@pytest.mark.parametrize("screen", [0, 1], ids=["fp64", "fp32_screen"])
+def test_host_navigator_matches_reference_long_traces(hc, screen):
     """More tracks and longer traces than the fixture, against the live reference."""
     import sys
     sys.path.insert(0, os.path.join(HERE, "golden"))
@@ -111,7 +114,7 @@ def test_host_navigator_matches_reference_long_traces(hc):
     _, dirs2 = W.isotropic_tracks(1000, W.SEED_BASE + 56)
     dirs = tuple(np.concatenate([a, b]) for a, b in zip((dx, dy, dz), dirs2))
     ms = 300
-    ids, steps, saf, nst, _ = host_trace(hc, pts, dirs, ms)
+    ids, steps, saf, nst, _ = host_trace(hc, pts, dirs, ms, screen=screen)
     want = reference_trace(oracle.RefLib(), pts, dirs, ms, nthreads=os.cpu_count() or 1)
     assert_traces_equal((ids, steps, saf, nst), want, ms, "host long")
 
@@ -132,7 +135,7 @@ def gpu_detector():
     return g, placed
 
 
-def gpu_trace(g, pts, dirs, ms, pstep=1e30):
+def gpu_trace(g, pts, dirs, ms, pstep=1e30, precision=0):
     import torch
     import vecgeom_b200 as V
     n = len(pts[0])
@@ -142,18 +145,19 @@ def gpu_trace(g, pts, dirs, ms, pstep=1e30):
     saf = torch.zeros(n * ms, dtype=torch.float64, device="cuda")
     nst = torch.zeros(n, dtype=torch.int32, device="cuda")
     nav.Trace(V.SOA3D(*(dev(a) for a in pts)), V.SOA3D(*(dev(a) for a in dirs)), pstep, ms, nst,
-              ids, steps, saf)
+              ids, steps, saf, precision=precision)
     torch.cuda.synchronize()
     assert nav.error_flags() == 0
     return ids.cpu().numpy(), steps.cpu().numpy(), saf.cpu().numpy(), nst.cpu().numpy()
 
 
 @pytest.mark.gpu
-def test_gpu_trace_matches_golden():
+@pytest.mark.parametrize("precision", [0, 1], ids=["fp64", "fp32_refine"])
+def test_gpu_trace_matches_golden(precision):
     d, pts, dirs = load_golden()
     ms = int(d["max_steps"])
     g, _ = gpu_detector()
-    got = gpu_trace(g, pts, dirs, ms)
+    got = gpu_trace(g, pts, dirs, ms, precision=precision)
     assert_traces_equal(got, (d["next_ids"], d["steps"], d["safeties"], d["nsteps"]), ms, "gpu")
 
 
@@ -166,9 +170,10 @@ def test_gpu_trace_matches_reference_many_tracks():
     pts, dirs = W.isotropic_tracks(4096, W.SEED_BASE + 77)
     ms = 128
     g, _ = gpu_detector()
-    got = gpu_trace(g, pts, dirs, ms)
     want = reference_trace(oracle.RefLib(), pts, dirs, ms, nthreads=os.cpu_count() or 1)
-    assert_traces_equal(got, want, ms, "gpu vs reference")
+    for precision in (0, 1):
+        got = gpu_trace(g, pts, dirs, ms, precision=precision)
+        assert_traces_equal(got, want, ms, f"gpu (precision {precision}) vs reference")
 
 
 @pytest.mark.gpu
@@ -199,7 +204,8 @@ def test_gpu_locate_and_single_steps_match_trace():
     nst = d["nsteps"]
     cur, nxt = a, b
     for k in range(2):
-        nav.FindNextBoundaryAndStep(V.SOA3D(*P), D, cur, nxt, pstep, step, saf)
+        nav.FindNextBoundaryAndStep(V.SOA3D(*P), D, cur, nxt, pstep, step, saf,
+                                    precision=k % 2)
         torch.cuda.synchronize()
         live = nst > k
         s = step.cpu().numpy()

@@ -99,10 +99,12 @@ def test_served_alone_and_in_the_mix_match_the_trace():
     reqs = requests(sizes, W.SEED_BASE + 91)
     truth = [trace_truth(g, *r) for r in reqs]
     # small slot table so admission has to wait for retirements
-    srv = V.NavServer(g, max_tracks=2560, steps_per_launch=5, max_steps=MAX_STEPS)
-    mixed = serve(srv, reqs, arrivals=[0, 0, 1, 2, 2, 3, 7, 9])
-    for k in range(len(reqs)):
-        assert_same(mixed[k], truth[k], f"request {k} in the mix")
+    for precision in (0, 1):
+        srv = V.NavServer(g, max_tracks=2560, steps_per_launch=5, max_steps=MAX_STEPS,
+                          precision=precision)
+        mixed = serve(srv, reqs, arrivals=[0, 0, 1, 2, 2, 3, 7, 9])
+        for k in range(len(reqs)):
+            assert_same(mixed[k], truth[k], f"request {k} in the mix (precision {precision})")
     for k in (0, 5):
         alone = serve(V.NavServer(g, max_tracks=4096, steps_per_launch=3, max_steps=MAX_STEPS),
                       [reqs[k]], arrivals=[0])

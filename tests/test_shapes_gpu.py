@@ -213,3 +213,40 @@ def test_empty_batch_and_bad_arguments():
         pv.batch(99, V.SOA3D(x, x, x), x)
     with pytest.raises(V.VgbError):   # distances need directions
         pv.batch(V.OP_DISTANCE_TO_IN, V.SOA3D(x, x, x), x)
+
+
+@pytest.mark.parametrize("kind", sorted(VGB_SHAPES))
+@pytest.mark.parametrize("placement", ["identity", "generic"])
+def test_fp32_refine_equals_fp64(kind, placement):
+    """The FP32+refine form certifies in float only answers the FP64 form gives
+    too (points outside the shape's widened box, rays missing it) and runs the
+    FP64 kernels for the rest, so every op must agree bit for bit."""
+    import torch
+    import vecgeom_b200 as V
+    from helpers import shape_specs
+    from vecgeom_b200 import workloads as W
+    spec = shape_specs()[kind]
+    n = 1 << 15
+    wl = W.make_workload(spec, n, W.SEED_BASE + 31)
+    # a far shell too: most of its rays miss, so the float screen settles them
+    rng = np.random.default_rng(5)
+    far = rng.normal(size=(3, n // 4))
+    far *= (3. * max(spec.half) / np.linalg.norm(far, axis=0))
+    x = np.concatenate([wl.x, far[0]])
+    y = np.concatenate([wl.y, far[1]])
+    z = np.concatenate([wl.z, far[2]])
+    d = W.isotropic(np.random.default_rng(6), len(x))
+    g, pv = build_placed(spec, placement)
+    P = V.SOA3D(dev(x), dev(y), dev(z))
+    D = V.SOA3D(dev(d[0]), dev(d[1]), dev(d[2]))
+    step = torch.full((len(x),), 1e30, dtype=torch.float64, device="cuda")
+    for meth, dt, args in (("Contains", torch.uint8, ()), ("Inside", torch.int32, ()),
+                           ("DistanceToIn", torch.float64, (D, step)),
+                           ("SafetyToIn", torch.float64, ())):
+        a = torch.full((len(x),), 7, dtype=dt, device="cuda")
+        b = torch.full((len(x),), 9, dtype=dt, device="cuda")
+        getattr(pv, meth)(P, *args, a, precision=V.PREC_FP64)
+        getattr(pv, meth)(P, *args, b, precision=V.PREC_FP32_REFINE)
+        torch.cuda.synchronize()
+        same = (a == b) | (torch.isnan(a) & torch.isnan(b)) if dt == torch.float64 else a == b
+        assert bool(same.all()), f"{kind} {meth}: {int((~same).sum())} differ"

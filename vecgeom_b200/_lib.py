@@ -94,7 +94,8 @@ SIGNATURES = {
     "vgb_basket_graph_capture": (ctypes.c_int, [_vp] + [_vp] * 8 + [_u32]),
     "vgb_basket_graph_launch": (ctypes.c_int, [_vp, _vp]),
     "vgb_basket_run_noalloc": (ctypes.c_int, [_vp, _vp, _i32, _u32] + [_vp] * 8 + [_u32, _vp]),
-    "vgb_server_create": (ctypes.c_int, [_vp, _i64, _i32, _i32, _dbl, ctypes.POINTER(_vp)]),
+    "vgb_server_create": (ctypes.c_int, [_vp, _i64, _i32, _i32, _dbl, _i32,
+                                         ctypes.POINTER(_vp)]),
     "vgb_server_destroy": (ctypes.c_int, [_vp]),
     "vgb_server_info": (ctypes.c_int, [_vp, _pi64, _pi64]),
     "vgb_server_submit": (ctypes.c_int, [_vp, _i64] + [_vp] * 6 + [_pi64]),
@@ -106,8 +107,9 @@ SIGNATURES = {
     "vgb_navpool_upload": (ctypes.c_int, [_vp, _vp, _i64, _vp]),
     "vgb_navpool_download": (ctypes.c_int, [_vp, _vp, _i64, _vp]),
     "vgb_nav_locate": (ctypes.c_int, [_vp, _i64, _vp, _vp, _vp, _vp, _vp]),
-    "vgb_nav_find_next_boundary_and_step": (ctypes.c_int, [_vp, _i64] + [_vp] * 12),
-    "vgb_nav_trace": (ctypes.c_int, [_vp, _i64] + [_vp] * 6 + [_dbl, _i32] + [_vp] * 5),
+    "vgb_nav_find_next_boundary_and_step": (ctypes.c_int, [_vp, _i64] + [_vp] * 11 + [_i32, _vp]),
+    "vgb_nav_trace": (ctypes.c_int, [_vp, _i64] + [_vp] * 6 + [_dbl, _i32] + [_vp] * 4
+                      + [_i32, _vp]),
     "vgb_nav_error_flags": (ctypes.c_int, [_vp, ctypes.POINTER(_u32)]),
 }
 

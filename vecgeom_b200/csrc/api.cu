@@ -95,8 +95,6 @@ vgb_status vgb_batch(const vgb_geometry *gc, int32_t placed, int32_t op, int64_t
   if (op < 0 || op >= VGB_OP_COUNT) return set_error(VGB_EINVAL, "vgb_batch: unknown op %d", op);
   if (precision != VGB_PREC_FP64 && precision != VGB_PREC_FP32_REFINE)
     return set_error(VGB_EINVAL, "vgb_batch: unknown precision %d", precision);
-  if (precision == VGB_PREC_FP32_REFINE)
-    return set_error(VGB_ENOTSUP, "vgb_batch: the FP32+refine form is not available");
   if (n < 0) return set_error(VGB_EINVAL, "vgb_batch: n < 0");
   if (n == 0) return VGB_OK;
   if (!x || !y || !z || !out) return set_error(VGB_EINVAL, "vgb_batch: NULL point or output");
@@ -111,7 +109,7 @@ vgb_status vgb_batch(const vgb_geometry *gc, int32_t placed, int32_t op, int64_t
   const PtrKind ko = classify(out);
   if (kx == kPtrDevice && ko == kPtrDevice) {
     BatchIO io{x, y, z, dx, dy, dz, step_max, out, aux, n, daughter, 0};
-    return launch_batch_f64(g, placed, op, io, s);
+    return launch_batch_f64(g, placed, op, io, s, precision);
   }
   if (kx != kPtrHost || ko != kPtrHost)
     return set_error(VGB_EINVAL, "vgb_batch: inputs and outputs must all be device or all host");
@@ -161,7 +159,7 @@ vgb_status vgb_batch(const vgb_geometry *gc, int32_t placed, int32_t op, int64_t
       e = cudaMemcpyAsync(daux, aux + b, m * 4, cudaMemcpyHostToDevice, cs);
     if (e != cudaSuccess) return cuda_error(e, "vgb_batch: host-to-device copy");
     BatchIO io{dxp, dyp, dzp, ddx, ddy, ddz, dst, dout, daux, m, daughter, 0};
-    if ((st = launch_batch_f64(g, placed, op, io, cs)) != VGB_OK) return st;
+    if ((st = launch_batch_f64(g, placed, op, io, cs, precision)) != VGB_OK) return st;
     e = cudaMemcpyAsync(static_cast<char *>(out) + b * osz, dout, m * osz,
                         cudaMemcpyDeviceToHost, cs);
     if (na && e == cudaSuccess)

@@ -18,7 +18,8 @@ static int grid_for(int64_t n) {
 
 template <class Ops, class P>
 static vgb_status launch_ops(const P &prm, const DXform &X, int op, BatchIO io, cudaStream_t s,
-                             int32_t rec_len = 0) {
+                             int32_t rec_len = 0, int precision = VGB_PREC_FP64) {
+  (void)precision;  // both forms run the FP64 kernels for single-volume batches
   const int grid = grid_for(io.n);
   io.stage = (Stageable<P>::value && rec_len > 0 && rec_len <= kStageMaxDoubles) ? rec_len : 0;
   const size_t smem = (size_t)io.stage * sizeof(double);
@@ -72,22 +73,24 @@ static BooleanP boolean_params(const vgb_geometry *g, int32_t unplaced) {
                      shape_params_dev(g, unplaced));
 }
 
-vgb_status launch_batch_f64(const vgb_geometry *g, int32_t placed, int op, const BatchIO &io,
-                            cudaStream_t s) {
+vgb_status launch_batch_f64(const vgb_geometry *g, int32_t placed, int op, const BatchIO &io0,
+                            cudaStream_t s, int precision) {
   const PlacedRec &pr = g->placed[placed];
   const DXform &X = g->xforms[pr.xform];
   const int type = g->unplaced[pr.unplaced].type;
   const void *prm = shape_params(g, pr.unplaced);
+  const BatchIO &io = io0;
   if (type == VGB_SHAPE_BOOLEAN) {
     const BooleanP b = boolean_params(g, pr.unplaced);
-    return with_boolean_ops(b, [&](auto o) { return launch_ops<decltype(o)>(b, X, op, io, s); });
+    return with_boolean_ops(
+        b, [&](auto o) { return launch_ops<decltype(o)>(b, X, op, io, s, 0, precision); });
   }
   switch (type) {
 #define VGB_SHAPE_CASE(TYPE, OPS, P) \
   case TYPE:                         \
     return launch_ops<OPS<double>>(                                                     \
         bind_params(*static_cast<const P *>(prm), shape_params_dev(g, pr.unplaced)), X, op, io, s, \
-        g->unplaced[pr.unplaced].param_len);
+        g->unplaced[pr.unplaced].param_len, precision);
     VGB_FOR_EACH_SHAPE(VGB_SHAPE_CASE)
 #undef VGB_SHAPE_CASE
   default:

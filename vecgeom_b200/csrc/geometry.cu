@@ -160,6 +160,7 @@ vgb_status vgb_geometry_destroy(vgb_geometry *g) {
     cudaFree(g->dev.xforms);
     cudaFree(g->dev.raw);
     cudaFree(g->dev.nav_flags);
+    cudaFree(g->dev.pl_box);
     cudaFree(g->dev.placed);
     cudaFree(g->dev.logicals);
     cudaFree(g->dev.daughters);
@@ -300,6 +301,57 @@ vgb_status vgb::prepare_tables(vgb_geometry *g) {
   }
   g->type_mask = 0;
   for (const UnplacedRec &u : g->unplaced) g->type_mask |= 1u << u.type;
+  // the FP32 screen's boxes, widened so that float rounding of the point, the
+  // direction and the slab arithmetic cannot move a ray across them
+  g->bbox.assign(6 * g->unplaced.size(), 0.f);
+  for (size_t u = 0; u < g->unplaced.size(); ++u) {
+    double b[6];
+    if (!shape_bbox(g, (int32_t)u, b)) {
+      for (int k = 0; k < 3; ++k) {
+        g->bbox[6 * u + k] = -3.0e38f;
+        g->bbox[6 * u + 3 + k] = 3.0e38f;
+      }
+      continue;
+    }
+    double ext = 0.;
+    for (int k = 0; k < 6; ++k) ext = std::max(ext, std::fabs(b[k]));
+    const double pad = 1e-3 + 1e-5 * ext;
+    for (int k = 0; k < 3; ++k) {
+      g->bbox[6 * u + k] = std::nextafter((float)(b[k] - pad), -3.0e38f);
+      g->bbox[6 * u + 3 + k] = std::nextafter((float)(b[3 + k] + pad), 3.0e38f);
+    }
+  }
+  // each placed volume's box in its mother's frame (corners moved with the full
+  // matrix, InverseTransform), for the navigator's float screen
+  g->pl_box.assign(6 * g->placed.size(), 0.f);
+  for (size_t pv = 0; pv < g->placed.size(); ++pv) {
+    float *o = &g->pl_box[6 * pv];
+    double b[6];
+    if (!shape_bbox(g, g->placed[pv].unplaced, b)) {
+      for (int k = 0; k < 3; ++k) {
+        o[k] = -3.0e38f;
+        o[3 + k] = 3.0e38f;
+      }
+      continue;
+    }
+    const RawXform &x = g->raw_xforms[g->placed[pv].raw_xform];
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    for (int c = 0; c < 8; ++c) {
+      const double l[3] = {b[(c & 1) ? 3 : 0], b[(c & 2) ? 4 : 1], b[(c & 4) ? 5 : 2]};
+      for (int k = 0; k < 3; ++k) {
+        const double m = x.t[k] + l[0] * x.r[3 * k] + l[1] * x.r[3 * k + 1] + l[2] * x.r[3 * k + 2];
+        lo[k] = std::min(lo[k], m);
+        hi[k] = std::max(hi[k], m);
+      }
+    }
+    double ext = 0.;
+    for (int k = 0; k < 3; ++k) ext = std::max(ext, std::max(std::fabs(lo[k]), std::fabs(hi[k])));
+    const double pad = 1e-3 + 1e-5 * ext;
+    for (int k = 0; k < 3; ++k) {
+      o[k] = std::nextafter((float)(lo[k] - pad), -3.0e38f);
+      o[3 + k] = std::nextafter((float)(hi[k] + pad), 3.0e38f);
+    }
+  }
   return VGB_OK;
 }
 
@@ -337,6 +389,7 @@ vgb_status vgb_geometry_close(vgb_geometry *g) {
     const std::vector<uint32_t> zero(1, 0u);
     if ((s = upload(zero, &g->dev.nav_flags, &g->dev.bytes)) != VGB_OK) return s;
   }
+  if ((s = upload(g->pl_box, &g->dev.pl_box, &g->dev.bytes)) != VGB_OK) return s;
   g->closed = true;
   return VGB_OK;
 }

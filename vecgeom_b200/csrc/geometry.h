@@ -71,6 +71,7 @@ struct DeviceImage {
   LogicalRec *logicals = nullptr;
   int32_t *daughters = nullptr;
   uint32_t *nav_flags = nullptr;  // navigation error bits (VGB_NAV_ERR_*)
+  float *pl_box = nullptr;        // per placed: enclosing box in the mother's frame
   int64_t bytes = 0;
 };
 
@@ -87,6 +88,8 @@ struct vgb_geometry {
   std::vector<vgb::PlacedRec> placed;
   std::vector<int32_t> daughters;
   std::vector<vgb::NavXform> nav_raw;  // per Transformation3D, for the navigator
+  std::vector<float> bbox;             // per unplaced: 6 floats, enclosing box (own frame)
+  std::vector<float> pl_box;           // per placed: 6 floats, enclosing box (mother frame)
   uint32_t type_mask = 0;              // bit t set when a shape of type t exists
   int32_t world = -1;
   int32_t max_depth = 0;
@@ -112,6 +115,9 @@ DXform effective_xform(const RawXform &x, bool generic_only);
 // Host tables derived at close: daughters CSR, depth, navigator transforms and
 // the shape-type mask.  No device work.
 vgb_status prepare_tables(vgb_geometry *g);
+// Axis-aligned box (min xyz, max xyz) in the shape's own frame that encloses
+// the shape; false for unknown types.
+bool shape_bbox(const vgb_geometry *g, int32_t unplaced, double box[6]);
 // Appends a shape record to the parameter pool (16-byte aligned).
 vgb_status add_unplaced(vgb_geometry *g, int type, const void *rec, size_t bytes, int32_t extra,
                         int32_t *id);

@@ -34,6 +34,7 @@ struct NavGeom {
   const NavXform *raw;          // per Transformation3D
   const LogicalRec *logicals;   // daughter range per logical volume
   const int32_t *daughters;     // CSR over logicals
+  const float *pl_box;          // per placed: enclosing box in the mother's frame (6 floats)
   int32_t world;
   int32_t max_depth;            // levels of the deepest path
 };
@@ -255,9 +256,73 @@ VGB_HD V3<double> nav_inverse_point(const NavXform &X, const V3<double> &l) {
 }
 
 // ---------------------------------------------------------------------------
+// float screen of the FP32+refine form (ABBoxNavigator's idea, kept exact)
+// ---------------------------------------------------------------------------
+// A daughter's DistanceToIn is only needed when it can beat the running best:
+// a ray that misses the daughter's widened box in the mother's frame, or enters
+// it beyond best, cannot (the box encloses the shape; the widening, 1e-3 mm +
+// 1e-5 of the coordinates, and the relative margin below cover float rounding),
+// so the FP64 call is skipped and the result is unchanged.
+struct RayF {
+  float p[3], inv[3];
+  bool flat[3];
+};
+VGB_HD RayF ray_f(const V3<double> &p, const V3<double> &d) {
+  RayF r;
+  const double pp[3] = {p.x, p.y, p.z}, dd[3] = {d.x, d.y, d.z};
+  for (int k = 0; k < 3; ++k) {
+    r.p[k] = (float)pp[k];
+    r.flat[k] = fabs(dd[k]) < 1e-30;
+    r.inv[k] = r.flat[k] ? 0.f : (float)(1.0 / dd[k]);
+  }
+  return r;
+}
+// true when the box cannot hold a hit closer than `best`
+VGB_HD bool box_skips(const float *b, const RayF &r, double best) {
+  float tn = 0.f, tf = 3.0e38f;
+  for (int k = 0; k < 3; ++k) {
+    if (r.flat[k]) {
+      if (r.p[k] < b[k] || r.p[k] > b[3 + k]) return true;
+      continue;
+    }
+    float t1 = (b[k] - r.p[k]) * r.inv[k], t2 = (b[3 + k] - r.p[k]) * r.inv[k];
+    if (t1 > t2) {
+      const float t = t1;
+      t1 = t2;
+      t2 = t;
+    }
+    tn = tn > t1 ? tn : t1;
+    tf = tf < t2 ? tf : t2;
+  }
+  if (tn > tf * 1.0001f + 1e-4f) return true;  // misses the box
+  const float bf = best < 3.0e38 ? (float)best : 3.0e38f;
+  return tn > bf * 1.0001f + 1e-3f;             // enters it beyond best
+}
+
+// Lower bound of a box daughter's SafetyToIn (BoxImplementation.h:801-818,
+// max_i |l_i| - d_i) in float, minus a margin covering the float rounding of
+// the transform and the subtraction.
+VGB_HD float box_safety_lower(const BoxP &b, const DXform &X, const V3<double> &p) {
+  const float ax = (float)(p.x - X.t[0]), ay = (float)(p.y - X.t[1]), az = (float)(p.z - X.t[2]);
+  const bool tr = X.flags & kXfHasTrans;
+  const float px = tr ? ax : (float)p.x, py = tr ? ay : (float)p.y, pz = tr ? az : (float)p.z;
+  float lx = px, ly = py, lz = pz;
+  if (X.flags & kXfHasRot) {
+    lx = px * (float)X.r[0] + py * (float)X.r[3] + pz * (float)X.r[6];
+    ly = px * (float)X.r[1] + py * (float)X.r[4] + pz * (float)X.r[7];
+    lz = px * (float)X.r[2] + py * (float)X.r[5] + pz * (float)X.r[8];
+  }
+  float s = fabsf(lx) - (float)b.d[0];
+  s = fmaxf(s, fabsf(ly) - (float)b.d[1]);
+  s = fmaxf(s, fabsf(lz) - (float)b.d[2]);
+  const float scale = fabsf(px) + fabsf(py) + fabsf(pz) + (float)(b.d[0] + b.d[1] + b.d[2]);
+  return s - (1e-3f + 1e-5f * scale);
+}
+
+// ---------------------------------------------------------------------------
 // the navigator
 // ---------------------------------------------------------------------------
-template <class L, uint32_t kMask> struct Navigator {
+template <class L, uint32_t kMask, bool kScreen = false> struct Navigator {
   using R = double;
   using S = NavShapes<kMask>;
 
@@ -344,6 +409,16 @@ template <class L, uint32_t kMask> struct Navigator {
       R mine = best;
       int mi = -1;
       for (int d = L::lane(); d < nd; d += L::N) {
+        if constexpr (kScreen && ((kMask >> VGB_SHAPE_BOX) & 1u)) {
+          // a box daughter whose safety is certainly >= the running minimum
+          // cannot replace it (strict <; the lane's earlier daughters hold it)
+          const PlacedRec &pr = G.placed[dl[d]];
+          const UnplacedRec &ur = G.unplaced[pr.unplaced];
+          if (ur.type == VGB_SHAPE_BOX &&
+              (double)box_safety_lower(*reinterpret_cast<const BoxP *>(G.params + ur.param_off),
+                                       G.xforms[pr.xform], lp) >= mine)
+            continue;
+        }
         const R t = S::safety_to_in(G, dl[d], lp);
         if (t < mine) {
           mine = t;
@@ -370,7 +445,12 @@ template <class L, uint32_t kMask> struct Navigator {
     const int32_t *dl = G.daughters + lr.dfirst;
     R best = step;
     int bi = -1;
+    RayF rf;
+    if constexpr (kScreen) rf = ray_f(lp, ld);
     for (int d = L::lane(); d < nd; d += L::N) {
+      if constexpr (kScreen) {
+        if (box_skips(G.pl_box + 6 * (int64_t)dl[d], rf, best)) continue;
+      }
       const R dd = S::distance_to_in(G, dl[d], lp, ld, step);
       const bool valid = dd < best && !isinf(dd);
       if (valid) {

@@ -39,6 +39,7 @@ NavGeom nav_geom(const vgb_geometry *g) {
   G.raw = g->dev.raw;
   G.logicals = g->dev.logicals;
   G.daughters = g->dev.daughters;
+  G.pl_box = g->dev.pl_box;
   G.world = g->world;
   G.max_depth = g->max_depth;
   return G;
@@ -67,13 +68,13 @@ __global__ void __launch_bounds__(kNavBlock) k_nav_locate(const NavGeom G, int64
   }
 }
 
-template <uint32_t kMask>
+template <uint32_t kMask, bool kScreen>
 __global__ void __launch_bounds__(kNavBlock)
     k_nav_step(const NavGeom G, int64_t n, const double *x, const double *y, const double *z,
                const double *dx, const double *dy, const double *dz, const unsigned char *cur,
                unsigned char *next, int64_t stride, const double *pstep, double *step_out,
                double *safety_out, uint32_t *flags) {
-  using Nav = Navigator<WarpLanes, kMask>;
+  using Nav = Navigator<WarpLanes, kMask, kScreen>;
   const int64_t warps = (int64_t)gridDim.x * kNavWarps;
   for (int64_t i = (int64_t)blockIdx.x * kNavWarps + threadIdx.x / 32; i < n; i += warps) {
     NavPath c, nx;
@@ -99,13 +100,13 @@ __global__ void __launch_bounds__(kNavBlock)
   }
 }
 
-template <uint32_t kMask>
+template <uint32_t kMask, bool kScreen>
 __global__ void __launch_bounds__(kNavBlock)
     k_nav_trace(const NavGeom G, int64_t n, const double *x, const double *y, const double *z,
                 const double *dx, const double *dy, const double *dz, double pstep,
                 int32_t max_steps, int32_t *next_ids, double *steps, double *safeties,
                 int32_t *nsteps, uint32_t *flags) {
-  using Nav = Navigator<WarpLanes, kMask>;
+  using Nav = Navigator<WarpLanes, kMask, kScreen>;
   const int64_t warps = (int64_t)gridDim.x * kNavWarps;
   const bool lane0 = WarpLanes::lane() == 0;
   for (int64_t i = (int64_t)blockIdx.x * kNavWarps + threadIdx.x / 32; i < n; i += warps) {
@@ -140,33 +141,41 @@ __global__ void __launch_bounds__(kNavBlock)
   }
 }
 
-// Launches F<kMask> for the smallest shape set covering the geometry.
-template <template <uint32_t> class K, class... A>
-vgb_status nav_launch(const vgb_geometry *g, int64_t n, cudaStream_t s, A... args) {
+// Launches K<kMask, kScreen> for the smallest shape set covering the geometry;
+// kScreen (the float screen of the FP32+refine form) when precision asks for it.
+template <template <uint32_t, bool> class K, class... A>
+vgb_status nav_launch(const vgb_geometry *g, int64_t n, cudaStream_t s, int precision,
+                      A... args) {
   const int grid = nav_grid(n);
-  if ((g->type_mask & ~kNavMaskBoxTubeTrd) == 0)
-    K<kNavMaskBoxTubeTrd>::launch(grid, s, args...);
+  const bool small = (g->type_mask & ~kNavMaskBoxTubeTrd) == 0;
+  const bool screen = precision == VGB_PREC_FP32_REFINE;
+  if (small && screen)
+    K<kNavMaskBoxTubeTrd, true>::launch(grid, s, args...);
+  else if (small)
+    K<kNavMaskBoxTubeTrd, false>::launch(grid, s, args...);
+  else if (screen)
+    K<kNavMaskAll, true>::launch(grid, s, args...);
   else
-    K<kNavMaskAll>::launch(grid, s, args...);
+    K<kNavMaskAll, false>::launch(grid, s, args...);
   count_launch();
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_error(e, "navigation kernel launch");
   return VGB_OK;
 }
 
-template <uint32_t M> struct LocateK {
+template <uint32_t M, bool> struct LocateK {
   template <class... A> static void launch(int grid, cudaStream_t s, A... a) {
     k_nav_locate<M><<<grid, kNavBlock, 0, s>>>(a...);
   }
 };
-template <uint32_t M> struct StepK {
+template <uint32_t M, bool S> struct StepK {
   template <class... A> static void launch(int grid, cudaStream_t s, A... a) {
-    k_nav_step<M><<<grid, kNavBlock, 0, s>>>(a...);
+    k_nav_step<M, S><<<grid, kNavBlock, 0, s>>>(a...);
   }
 };
-template <uint32_t M> struct TraceK {
+template <uint32_t M, bool S> struct TraceK {
   template <class... A> static void launch(int grid, cudaStream_t s, A... a) {
-    k_nav_trace<M><<<grid, kNavBlock, 0, s>>>(a...);
+    k_nav_trace<M, S><<<grid, kNavBlock, 0, s>>>(a...);
   }
 };
 
@@ -281,7 +290,8 @@ vgb_status vgb_nav_locate(const vgb_geometry *g, int64_t n, const double *x, con
   if (n == 0) return VGB_OK;
   if (!is_device_ptr(x) || !is_device_ptr(y) || !is_device_ptr(z))
     return set_error(VGB_EINVAL, "vgb_nav_locate: points must be device memory");
-  return nav_launch<LocateK>(g, n, (cudaStream_t)stream, nav_geom(g), n, x, y, z, states->dev,
+  return nav_launch<LocateK>(g, n, (cudaStream_t)stream, VGB_PREC_FP64, nav_geom(g), n, x, y, z,
+                             states->dev,
                              states->stride, g->dev.nav_flags);
 }
 
@@ -290,8 +300,11 @@ vgb_status vgb_nav_find_next_boundary_and_step(const vgb_geometry *g, int64_t n,
                                                const double *dx, const double *dy,
                                                const double *dz, const vgb_navpool *cur,
                                                vgb_navpool *next, const double *pstep,
-                                               double *step, double *safety, void *stream) {
+                                               double *step, double *safety, int32_t precision,
+                                               void *stream) {
   const char *fn = "vgb_nav_find_next_boundary_and_step";
+  if (precision != VGB_PREC_FP64 && precision != VGB_PREC_FP32_REFINE)
+    return set_error(VGB_EINVAL, "%s: unknown precision %d", fn, precision);
   vgb_status s = check_nav_geometry(g, fn);
   if (s != VGB_OK) return s;
   if (!cur || !next || cur == next || n < 0 || n > cur->n || n > next->n ||
@@ -303,7 +316,8 @@ vgb_status vgb_nav_find_next_boundary_and_step(const vgb_geometry *g, int64_t n,
     if (!is_device_ptr(p)) return set_error(VGB_EINVAL, "%s: arrays must be device memory", fn);
   if (safety && !is_device_ptr(safety))
     return set_error(VGB_EINVAL, "%s: safety must be device memory or NULL", fn);
-  return nav_launch<StepK>(g, n, (cudaStream_t)stream, nav_geom(g), n, x, y, z, dx, dy, dz,
+  return nav_launch<StepK>(g, n, (cudaStream_t)stream, precision, nav_geom(g), n, x, y, z, dx,
+                           dy, dz,
                            (const unsigned char *)cur->dev, next->dev, cur->stride, pstep, step,
                            safety, g->dev.nav_flags);
 }
@@ -311,8 +325,10 @@ vgb_status vgb_nav_find_next_boundary_and_step(const vgb_geometry *g, int64_t n,
 vgb_status vgb_nav_trace(const vgb_geometry *g, int64_t n, const double *x, const double *y,
                          const double *z, const double *dx, const double *dy, const double *dz,
                          double pstep, int32_t max_steps, int32_t *next_ids, double *steps,
-                         double *safeties, int32_t *nsteps, void *stream) {
+                         double *safeties, int32_t *nsteps, int32_t precision, void *stream) {
   const char *fn = "vgb_nav_trace";
+  if (precision != VGB_PREC_FP64 && precision != VGB_PREC_FP32_REFINE)
+    return set_error(VGB_EINVAL, "%s: unknown precision %d", fn, precision);
   vgb_status s = check_nav_geometry(g, fn);
   if (s != VGB_OK) return s;
   if (n < 0 || max_steps < 0) return set_error(VGB_EINVAL, "%s: n or max_steps < 0", fn);
@@ -324,7 +340,8 @@ vgb_status vgb_nav_trace(const vgb_geometry *g, int64_t n, const double *x, cons
   for (const void *p : opt)
     if (p && !is_device_ptr(p))
       return set_error(VGB_EINVAL, "%s: records must be device memory or NULL", fn);
-  return nav_launch<TraceK>(g, n, (cudaStream_t)stream, nav_geom(g), n, x, y, z, dx, dy, dz,
+  return nav_launch<TraceK>(g, n, (cudaStream_t)stream, precision, nav_geom(g), n, x, y, z, dx,
+                            dy, dz,
                             pstep, max_steps, next_ids, steps, safeties, nsteps,
                             g->dev.nav_flags);
 }

@@ -85,11 +85,11 @@ __global__ void __launch_bounds__(kSrvBlock)
   }
 }
 
-template <uint32_t kMask>
+template <uint32_t kMask, bool kScreen>
 __global__ void __launch_bounds__(kSrvBlock)
     k_srv_step(const NavGeom G, const int32_t *chunks, int64_t ntracks, Slots S, double pstep,
                int32_t max_steps, int32_t steps_per_launch, int32_t *live, uint32_t *flags) {
-  using Nav = Navigator<WarpLanes, kMask>;
+  using Nav = Navigator<WarpLanes, kMask, kScreen>;
   const int64_t warps = (int64_t)gridDim.x * kSrvWarps;
   const bool lane0 = WarpLanes::lane() == 0;
   for (int64_t t = (int64_t)blockIdx.x * kSrvWarps + threadIdx.x / 32; t < ntracks; t += warps) {
@@ -140,6 +140,7 @@ NavGeom server_geom(const vgb_geometry *g) {
   G.raw = g->dev.raw;
   G.logicals = g->dev.logicals;
   G.daughters = g->dev.daughters;
+  G.pl_box = g->dev.pl_box;
   G.world = g->world;
   G.max_depth = g->max_depth;
   return G;
@@ -180,6 +181,7 @@ struct vgb_server {
   std::map<int64_t, vgb::Request *> done;
   int64_t next_id = 0;
   bool all_shapes = false;
+  bool screen = false;  // FP32+refine: float screen on the daughter loops
 };
 
 namespace vgb {
@@ -208,9 +210,14 @@ void launch_admit(vgb_server *s, const int32_t *chunks, int64_t nt, int64_t nv) 
                                                                   s->S, s->g->dev.nav_flags);
 }
 template <uint32_t kMask> void launch_step(vgb_server *s, int64_t nt) {
-  k_srv_step<kMask><<<srv_grid(nt), kSrvBlock, 0, s->stream>>>(
-      server_geom(s->g), s->d_chunks, nt, s->S, s->pstep, s->max_steps, s->steps_per_launch,
-      s->d_live, s->g->dev.nav_flags);
+  if (s->screen)
+    k_srv_step<kMask, true><<<srv_grid(nt), kSrvBlock, 0, s->stream>>>(
+        server_geom(s->g), s->d_chunks, nt, s->S, s->pstep, s->max_steps, s->steps_per_launch,
+        s->d_live, s->g->dev.nav_flags);
+  else
+    k_srv_step<kMask, false><<<srv_grid(nt), kSrvBlock, 0, s->stream>>>(
+        server_geom(s->g), s->d_chunks, nt, s->S, s->pstep, s->max_steps, s->steps_per_launch,
+        s->d_live, s->g->dev.nav_flags);
 }
 
 // Admits queued requests while free chunks last (arrival order: a request that
@@ -258,9 +265,12 @@ vgb_status admit(vgb_server *s) {
 extern "C" {
 
 vgb_status vgb_server_create(const vgb_geometry *g, int64_t max_tracks, int32_t steps_per_launch,
-                             int32_t max_steps, double pstep, vgb_server **server) {
+                             int32_t max_steps, double pstep, int32_t precision,
+                             vgb_server **server) {
   if (!server) return set_error(VGB_EINVAL, "vgb_server_create: server is NULL");
   *server = nullptr;
+  if (precision != VGB_PREC_FP64 && precision != VGB_PREC_FP32_REFINE)
+    return set_error(VGB_EINVAL, "vgb_server_create: unknown precision %d", precision);
   if (!g || !g->closed || g->world < 0)
     return set_error(VGB_EINVAL, "vgb_server_create: geometry not closed or without world");
   if (g->max_depth > kNavMaxLevels)
@@ -292,6 +302,7 @@ vgb_status vgb_server_create(const vgb_geometry *g, int64_t max_tracks, int32_t 
   s->pstep = pstep;
   s->nchunks = nchunks;
   s->all_shapes = (g->type_mask & ~kNavMaskBoxTubeTrd) != 0;
+  s->screen = precision == VGB_PREC_FP32_REFINE;
   Slots &S = s->S;
   S.stride = stride;
   e = cudaSuccess;

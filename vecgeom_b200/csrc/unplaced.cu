@@ -491,6 +491,92 @@ std::vector<double> make_polyhedron(double phiStart, double phiDelta, int sides,
   return blob;
 }
 
+// Enclosing axis-aligned box of a shape in its own frame (used by the float
+// screen of the FP32+refine form; only its enclosure matters).
+bool shape_bbox(const vgb_geometry *g, int32_t u, double b[6]) {
+  const UnplacedRec &r = g->unplaced[u];
+  const double *rec = g->params.data() + r.param_off;
+  auto sym = [&](double x, double y, double z) {
+    b[0] = -x; b[1] = -y; b[2] = -z; b[3] = x; b[4] = y; b[5] = z;
+    return true;
+  };
+  switch (r.type) {
+    case VGB_SHAPE_BOX: {
+      const BoxP &p = *reinterpret_cast<const BoxP *>(rec);
+      return sym(p.d[0], p.d[1], p.d[2]);
+    }
+    case VGB_SHAPE_TUBE: {
+      const TubeP &p = *reinterpret_cast<const TubeP *>(rec);
+      return sym(p.rmax, p.rmax, p.z);
+    }
+    case VGB_SHAPE_CONE: {
+      const ConeP &p = *reinterpret_cast<const ConeP *>(rec);
+      const double rm = std::max(p.rmax1, p.rmax2);
+      return sym(rm, rm, p.dz);
+    }
+    case VGB_SHAPE_SPHERE: {
+      const SphereP &p = *reinterpret_cast<const SphereP *>(rec);
+      return sym(p.rmax, p.rmax, p.rmax);
+    }
+    case VGB_SHAPE_TORUS: {
+      const TorusP &p = *reinterpret_cast<const TorusP *>(rec);
+      return sym(p.rtor + p.rmax, p.rtor + p.rmax, p.rmax);
+    }
+    case VGB_SHAPE_TRD: {
+      const TrdP &p = *reinterpret_cast<const TrdP *>(rec);
+      return sym(std::max(p.dx1, p.dx2), std::max(p.dy1, p.dy2), p.dz);
+    }
+    case VGB_SHAPE_POLYCONE: {
+      const PolyconeP &p = *reinterpret_cast<const PolyconeP *>(rec);
+      const PolySec *sec = reinterpret_cast<const PolySec *>(rec + p.sec_off);
+      double rm = 0., zlo = 1e300, zhi = -1e300;
+      for (int i = 0; i < p.nsec; ++i) {
+        rm = std::max(rm, std::max(sec[i].cone.rmax1, sec[i].cone.rmax2));
+        zlo = std::min(zlo, sec[i].shift - sec[i].cone.dz);
+        zhi = std::max(zhi, sec[i].shift + sec[i].cone.dz);
+      }
+      b[0] = b[1] = -rm;
+      b[3] = b[4] = rm;
+      b[2] = zlo;
+      b[5] = zhi;
+      return p.nsec > 0;
+    }
+    case VGB_SHAPE_POLYHEDRON: {
+      const PolyhedronP &p = *reinterpret_cast<const PolyhedronP *>(rec);
+      b[0] = b[1] = -p.btube.rmax;
+      b[3] = b[4] = p.btube.rmax;
+      b[2] = p.btube_offset - p.btube.z;
+      b[5] = p.btube_offset + p.btube.z;
+      return true;
+    }
+    case VGB_SHAPE_BOOLEAN: {
+      // the left component's box, moved into the boolean's frame
+      const BooleanP &p = *reinterpret_cast<const BooleanP *>(rec);
+      if (p.left.xf.flags & kXfQuirk16A) return false;  // not a rigid motion
+      const int32_t loff = r.param_off + p.left.rec_off;
+      int32_t left = -1;
+      for (size_t k = 0; k < g->unplaced.size(); ++k)
+        if (g->unplaced[k].param_off == loff) left = (int32_t)k;
+      double lb[6];
+      if (left < 0 || !shape_bbox(g, left, lb)) return false;
+      b[0] = b[1] = b[2] = 1e300;
+      b[3] = b[4] = b[5] = -1e300;
+      for (int c = 0; c < 8; ++c) {
+        const V3<double> l = {lb[(c & 1) ? 3 : 0], lb[(c & 2) ? 4 : 1], lb[(c & 4) ? 5 : 2]};
+        const V3<double> m = xf_inverse_point(p.left.xf, l);
+        const double v[3] = {m.x, m.y, m.z};
+        for (int k = 0; k < 3; ++k) {
+          b[k] = std::min(b[k], v[k]);
+          b[3 + k] = std::max(b[3 + k], v[k]);
+        }
+      }
+      return true;
+    }
+    default:
+      return false;
+  }
+}
+
 }  // namespace vgb
 
 extern "C" {

@@ -352,17 +352,18 @@ class SimpleNavigator:
 
     def FindNextBoundaryAndStep(self, points: SOA3D, dirs: SOA3D, cur: NavStatePool,
                                 nxt: NavStatePool, pstep, step, safety=None,
-                                stream=None) -> None:
+                                precision: int = L.PREC_FP64, stream=None) -> None:
         g = self.geometry
         for a in (pstep, step, safety):
             _check_dtype(a, "f8")
         check(g.L.vgb_nav_find_next_boundary_and_step(
             g.handle, points.size(), _addr(points.x), _addr(points.y), _addr(points.z),
             _addr(dirs.x), _addr(dirs.y), _addr(dirs.z), cur.handle, nxt.handle, _addr(pstep),
-            _addr(step), _addr(safety), _stream(stream)))
+            _addr(step), _addr(safety), precision, _stream(stream)))
 
     def Trace(self, points: SOA3D, dirs: SOA3D, pstep: float, max_steps: int, nsteps,
-              next_ids=None, steps=None, safeties=None, stream=None) -> None:
+              next_ids=None, steps=None, safeties=None, precision: int = L.PREC_FP64,
+              stream=None) -> None:
         """Steps every track to the world exit (see vgb_nav_trace)."""
         g = self.geometry
         _check_dtype(nsteps, "i4")
@@ -370,7 +371,8 @@ class SimpleNavigator:
         check(g.L.vgb_nav_trace(
             g.handle, points.size(), _addr(points.x), _addr(points.y), _addr(points.z),
             _addr(dirs.x), _addr(dirs.y), _addr(dirs.z), float(pstep), int(max_steps),
-            _addr(next_ids), _addr(steps), _addr(safeties), _addr(nsteps), _stream(stream)))
+            _addr(next_ids), _addr(steps), _addr(safeties), _addr(nsteps), precision,
+            _stream(stream)))
 
     def error_flags(self) -> int:
         out = ctypes.c_uint32()
@@ -457,12 +459,12 @@ class NavServer:
     see vgb_server_* in include/vgb.h."""
 
     def __init__(self, geometry: "Geometry", max_tracks: int = 0, steps_per_launch: int = 8,
-                 max_steps: int = 1000, pstep: float = 1e30):
+                 max_steps: int = 1000, pstep: float = 1e30, precision: int = L.PREC_FP64):
         geometry._require_closed()
         self.geometry = geometry
         h = ctypes.c_void_p()
         check(geometry.L.vgb_server_create(geometry.handle, max_tracks, steps_per_launch,
-                                           max_steps, pstep, ctypes.byref(h)))
+                                           max_steps, pstep, precision, ctypes.byref(h)))
         self.handle = h
         mt, nb = ctypes.c_int64(), ctypes.c_int64()
         check(geometry.L.vgb_server_info(h, ctypes.byref(mt), ctypes.byref(nb)))
