@@ -373,11 +373,12 @@ vgb_status vgb_nav_error_flags(const vgb_geometry *g, uint32_t *flags);
  * requests in arrival order while the device track slots (allocated once, at
  * create, from free HBM) can hold them, advances every live track of every
  * admitted request by up to steps_per_launch navigation steps in one launch,
- * and retires the requests whose tracks all finished.  A track finishes when
- * its state leaves the world or after max_steps steps.  Per track the server
- * keeps what vgb_nav_trace would produce: the step count, the final point and
- * a 64-bit FNV-1a hash of its sequence of (next placed id, step) records, so a
- * request's results do not depend on what else was in flight.
+ * and retires the requests whose tracks all finished: their results move to
+ * host memory and their slots are free for the next admission.  A track
+ * finishes when its state leaves the world or after max_steps steps.  Per track
+ * the server keeps what vgb_nav_trace would produce: the step count, the final
+ * point and a 64-bit FNV-1a hash of its sequence of (next placed id, step)
+ * records, so a request's results do not depend on what else was in flight.
  * ------------------------------------------------------------------------- */
 typedef struct vgb_server vgb_server;
 

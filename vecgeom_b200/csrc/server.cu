@@ -2,16 +2,17 @@
 //
 // Device memory holds a fixed table of track slots, carved into chunks of
 // kChunk tracks.  A request owns whole chunks; the last one is padded with
-// finished tracks.  Every iteration:
-//   1. admit: queued requests, in arrival order, take free chunks; their points
-//      are copied into the slots and one launch locates them (LocatePoint from
-//      the world) and clears their counters;
+// finished tracks.  Every iteration (vgb_server_step):
+//   1. admit: queued requests, in arrival order, take free chunks; the points
+//      of all of them go to the device in one copy from a pinned staging
+//      buffer, and one launch scatters them into their slots, locates them
+//      (LocatePoint from the world) and clears their counters;
 //   2. step: one launch over the chunks of all admitted requests advances every
 //      live track by up to steps_per_launch steps (one warp per track, the
 //      navigator of navigation.cuh) and counts the tracks still live per chunk;
-//   3. retire: a request whose chunks have no live track is finished; its
-//      results stay in the slots until vgb_server_result copies them out and
-//      frees the chunks.
+//   3. retire: the requests whose chunks have no live track are finished; one
+//      launch gathers their results into a staging buffer, one copy brings them
+//      to pinned host memory, and their chunks are free for the next admission.
 // Requests that arrive while others are in flight join at the next iteration,
 // so their steps share launches with the older requests' steps.
 #include <algorithm>
@@ -42,6 +43,14 @@ struct Slots {
   uint8_t *done;
 };
 
+// Per-track record of a finished request, as staged for the copy to the host.
+struct TrackResult {
+  double x, y, z;
+  uint64_t hash;
+  int32_t nsteps;
+  int32_t pad;
+};
+
 VGB_HD uint64_t fnv_bytes(uint64_t h, const void *p, int n) {
   const unsigned char *b = static_cast<const unsigned char *>(p);
   for (int i = 0; i < n; ++i) {
@@ -56,18 +65,23 @@ VGB_D int64_t slot_of(const int32_t *chunks, int64_t t) {
   return (int64_t)chunks[t / kChunk] * kChunk + (t % kChunk);
 }
 
+// in: 6 arrays of ntracks (x, y, z, dx, dy, dz) in chunk-list order; valid[t]
+// marks the request's tracks (the rest pad the last chunk of each request)
 template <uint32_t kMask>
 __global__ void __launch_bounds__(kSrvBlock)
-    k_srv_admit(const NavGeom G, const int32_t *chunks, int64_t ntracks, int64_t nvalid, Slots S,
-                uint32_t *flags) {
+    k_srv_admit(const NavGeom G, const int32_t *chunks, int64_t ntracks, const double *in,
+                const uint8_t *valid, Slots S, uint32_t *flags) {
   using Nav = Navigator<WarpLanes, kMask>;
   const int64_t warps = (int64_t)gridDim.x * kSrvWarps;
   for (int64_t t = (int64_t)blockIdx.x * kSrvWarps + threadIdx.x / 32; t < ntracks; t += warps) {
     const int64_t s = slot_of(chunks, t);
+    const bool v = valid[t] != 0;
     NavPath p;
     bool ok = true;
-    if (t < nvalid) {
-      ok = Nav::locate_from_world(G, p, V3<double>{S.x[s], S.y[s], S.z[s]});
+    V3<double> x = {0., 0., 0.};
+    if (v) {
+      x = {in[t], in[ntracks + t], in[2 * ntracks + t]};
+      ok = Nav::locate_from_world(G, p, x);
     } else {
       p.level = 0;
       p.boundary = false;
@@ -78,9 +92,15 @@ __global__ void __launch_bounds__(kSrvBlock)
         p.level = 0;
       }
       nav_store(p, NavStateRef{S.states + s * S.stride}, G.max_depth);
+      S.x[s] = x.x;
+      S.y[s] = x.y;
+      S.z[s] = x.z;
+      S.dx[s] = v ? in[3 * ntracks + t] : 0.;
+      S.dy[s] = v ? in[4 * ntracks + t] : 0.;
+      S.dz[s] = v ? in[5 * ntracks + t] : 0.;
       S.nsteps[s] = 0;
       S.hash[s] = kFnvOffset;
-      S.done[s] = (t < nvalid && p.level > 0) ? 0 : 1;
+      S.done[s] = (v && p.level > 0) ? 0 : 1;
     }
   }
 }
@@ -131,6 +151,15 @@ __global__ void __launch_bounds__(kSrvBlock)
   }
 }
 
+// results of the listed chunks' slots, in chunk-list order
+__global__ void k_srv_gather(const int32_t *chunks, int64_t ntracks, Slots S, TrackResult *out) {
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < ntracks;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t s = slot_of(chunks, t);
+    out[t] = TrackResult{S.x[s], S.y[s], S.z[s], S.hash[s], S.nsteps[s], 0};
+  }
+}
+
 NavGeom server_geom(const vgb_geometry *g) {
   NavGeom G;
   G.params = g->dev.params;
@@ -157,7 +186,7 @@ struct Request {
   int64_t n = 0;
   std::vector<double> in;  // x, y, z, dx, dy, dz (6 n)
   std::vector<int32_t> chunks;
-  bool finished = false;
+  std::vector<TrackResult> out;
 };
 
 }  // namespace
@@ -174,6 +203,15 @@ struct vgb_server {
   vgb::Slots S{};
   int32_t *d_chunks = nullptr;   // chunk list of the current launch
   int32_t *d_live = nullptr;     // live tracks per listed chunk
+  double *d_in = nullptr;        // staged inputs of an admission (6 * slots)
+  uint8_t *d_valid = nullptr;    // request track or padding, per staged track
+  vgb::TrackResult *d_out = nullptr;  // gathered results of a retirement
+  double *h_in = nullptr;        // pinned host mirrors of the three buffers
+  uint8_t *h_valid = nullptr;
+  vgb::TrackResult *h_out = nullptr;
+  int32_t *h_chunks = nullptr;   // chunk lists of the step and retire launches
+  int32_t *h_achunks = nullptr;  // chunk list of the admit launch (copied asynchronously)
+  int32_t *h_live = nullptr;
   cudaStream_t stream = nullptr;
   std::vector<int32_t> free_chunks;
   std::deque<vgb::Request *> queue;
@@ -192,22 +230,27 @@ template <class T> cudaError_t srv_alloc(vgb_server *s, T **p, size_t n) {
   if (e == cudaSuccess) s->bytes += (int64_t)(std::max<size_t>(1, n) * sizeof(T));
   return e;
 }
+template <class T> cudaError_t srv_pin(T **p, size_t n) {
+  return cudaHostAlloc((void **)p, std::max<size_t>(1, n) * sizeof(T), cudaHostAllocDefault);
+}
 
 void srv_free(vgb_server *s) {
   Slots &S = s->S;
-  void *ptrs[] = {S.x, S.y, S.z, S.dx, S.dy, S.dz, S.states, S.nsteps, S.hash, S.done,
-                  s->d_chunks, s->d_live};
+  void *ptrs[] = {S.x,         S.y,         S.z,      S.dx,       S.dy,    S.dz,
+                  S.states,    S.nsteps,    S.hash,   S.done,     s->d_chunks,
+                  s->d_live,   s->d_in,     s->d_valid, s->d_out};
   for (void *p : ptrs) cudaFree(p);
+  void *pins[] = {s->h_in, s->h_valid, s->h_out, s->h_chunks, s->h_achunks, s->h_live};
+  for (void *p : pins) cudaFreeHost(p);
   if (s->stream) cudaStreamDestroy(s->stream);
   for (Request *r : s->queue) delete r;
   for (Request *r : s->active) delete r;
   for (auto &kv : s->done) delete kv.second;
 }
 
-template <uint32_t kMask>
-void launch_admit(vgb_server *s, const int32_t *chunks, int64_t nt, int64_t nv) {
-  k_srv_admit<kMask><<<srv_grid(nt), kSrvBlock, 0, s->stream>>>(server_geom(s->g), chunks, nt, nv,
-                                                                  s->S, s->g->dev.nav_flags);
+template <uint32_t kMask> void launch_admit(vgb_server *s, int64_t nt) {
+  k_srv_admit<kMask><<<srv_grid(nt), kSrvBlock, 0, s->stream>>>(
+      server_geom(s->g), s->d_chunks, nt, s->d_in, s->d_valid, s->S, s->g->dev.nav_flags);
 }
 template <uint32_t kMask> void launch_step(vgb_server *s, int64_t nt) {
   if (s->screen)
@@ -221,8 +264,10 @@ template <uint32_t kMask> void launch_step(vgb_server *s, int64_t nt) {
 }
 
 // Admits queued requests while free chunks last (arrival order: a request that
-// does not fit blocks the ones behind it).
+// does not fit blocks the ones behind it), all in one copy and one launch.
 vgb_status admit(vgb_server *s) {
+  std::vector<Request *> batch;
+  int64_t nc = 0;
   while (!s->queue.empty()) {
     Request *r = s->queue.front();
     const int64_t need = (r->n + kChunk - 1) / kChunk;
@@ -230,32 +275,40 @@ vgb_status admit(vgb_server *s) {
     s->queue.pop_front();
     r->chunks.assign(s->free_chunks.end() - need, s->free_chunks.end());
     s->free_chunks.resize(s->free_chunks.size() - need);
-    std::sort(r->chunks.begin(), r->chunks.end());
-    // inputs: one copy per chunk and coordinate
-    double *dst[6] = {s->S.x, s->S.y, s->S.z, s->S.dx, s->S.dy, s->S.dz};
-    cudaError_t e = cudaSuccess;
-    for (int64_t c = 0; c < need && e == cudaSuccess; ++c) {
-      const int64_t first = c * kChunk, cnt = std::min<int64_t>(kChunk, r->n - first);
-      if (cnt <= 0) break;
-      for (int k = 0; k < 6 && e == cudaSuccess; ++k)
-        e = cudaMemcpyAsync(dst[k] + (int64_t)r->chunks[c] * kChunk, r->in.data() + k * r->n + first,
-                            cnt * sizeof(double), cudaMemcpyHostToDevice, s->stream);
+    batch.push_back(r);
+    nc += need;
+  }
+  if (batch.empty()) return VGB_OK;
+  const int64_t nt = nc * kChunk;
+  int64_t c = 0;
+  for (Request *r : batch) {
+    for (size_t k = 0; k < r->chunks.size(); ++k, ++c) {
+      s->h_achunks[c] = r->chunks[k];
+      for (int j = 0; j < kChunk; ++j) {
+        const int64_t src = (int64_t)k * kChunk + j, dst = c * kChunk + j;
+        const bool v = src < r->n;
+        s->h_valid[dst] = v ? 1 : 0;
+        for (int a = 0; a < 6; ++a) s->h_in[a * nt + dst] = v ? r->in[a * r->n + src] : 0.;
+      }
     }
-    if (e == cudaSuccess)
-      e = cudaMemcpyAsync(s->d_chunks, r->chunks.data(), need * sizeof(int32_t),
-                          cudaMemcpyHostToDevice, s->stream);
-    if (e != cudaSuccess) return cuda_error(e, "vgb_server_step: admit copy");
-    if (s->all_shapes)
-      launch_admit<kNavMaskAll>(s, s->d_chunks, need * kChunk, r->n);
-    else
-      launch_admit<kNavMaskBoxTubeTrd>(s, s->d_chunks, need * kChunk, r->n);
-    count_launch();
-    e = cudaGetLastError();
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);  // r->in is read by the copies
-    if (e != cudaSuccess) return cuda_error(e, "vgb_server_step: admit");
     std::vector<double>().swap(r->in);
     s->active.push_back(r);
   }
+  cudaError_t e = cudaMemcpyAsync(s->d_in, s->h_in, 6 * nt * sizeof(double),
+                                  cudaMemcpyHostToDevice, s->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(s->d_valid, s->h_valid, nt, cudaMemcpyHostToDevice, s->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(s->d_chunks, s->h_achunks, nc * sizeof(int32_t), cudaMemcpyHostToDevice,
+                        s->stream);
+  if (e != cudaSuccess) return cuda_error(e, "vgb_server_step: admit copy");
+  if (s->all_shapes)
+    launch_admit<kNavMaskAll>(s, nt);
+  else
+    launch_admit<kNavMaskBoxTubeTrd>(s, nt);
+  count_launch();
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_error(e, "vgb_server_step: admit");
   return VGB_OK;
 }
 
@@ -279,18 +332,14 @@ vgb_status vgb_server_create(const vgb_geometry *g, int64_t max_tracks, int32_t 
   if (max_tracks < 0 || steps_per_launch < 1 || max_steps < 0)
     return set_error(VGB_EINVAL, "vgb_server_create: bad capacity or step counts");
   const int64_t stride = nav_state_stride(g->max_depth);
-  const int64_t per_track = 6 * 8 + stride + 4 + 8 + 1;
-  if (max_tracks == 0) {
-    size_t fr = 0, tot = 0;
-    cudaError_t e = cudaMemGetInfo(&fr, &tot);
-    if (e != cudaSuccess) return cuda_error(e, "vgb_server_create: cudaMemGetInfo");
-    max_tracks = std::min<int64_t>((int64_t)(fr / 4) / per_track, (int64_t)1 << 22);
-  }
-  const int64_t nchunks = (max_tracks + kChunk - 1) / kChunk;
-  const int64_t nslots = nchunks * kChunk;
+  // slots (points, state, counters) + staged inputs + gathered results
+  const int64_t per_track = 6 * 8 + stride + 4 + 8 + 1 + 6 * 8 + 1 + (int64_t)sizeof(TrackResult);
   size_t fr = 0, tot = 0;
   cudaError_t e = cudaMemGetInfo(&fr, &tot);
   if (e != cudaSuccess) return cuda_error(e, "vgb_server_create: cudaMemGetInfo");
+  if (max_tracks == 0) max_tracks = std::min<int64_t>((int64_t)(fr / 4) / per_track, (int64_t)1 << 22);
+  const int64_t nchunks = (max_tracks + kChunk - 1) / kChunk;
+  const int64_t nslots = nchunks * kChunk;
   if ((double)nslots * per_track > 0.9 * (double)fr)
     return set_error(VGB_ENOMEM, "vgb_server_create: %lld track slots need %lld bytes, %zu free",
                      (long long)nslots, (long long)(nslots * per_track), fr);
@@ -315,6 +364,15 @@ vgb_status vgb_server_create(const vgb_geometry *g, int64_t max_tracks, int32_t 
   if (e == cudaSuccess) e = srv_alloc(s, &S.done, nslots);
   if (e == cudaSuccess) e = srv_alloc(s, &s->d_chunks, nchunks);
   if (e == cudaSuccess) e = srv_alloc(s, &s->d_live, nchunks);
+  if (e == cudaSuccess) e = srv_alloc(s, &s->d_in, 6 * nslots);
+  if (e == cudaSuccess) e = srv_alloc(s, &s->d_valid, nslots);
+  if (e == cudaSuccess) e = srv_alloc(s, &s->d_out, nslots);
+  if (e == cudaSuccess) e = srv_pin(&s->h_in, 6 * nslots);
+  if (e == cudaSuccess) e = srv_pin(&s->h_valid, nslots);
+  if (e == cudaSuccess) e = srv_pin(&s->h_out, nslots);
+  if (e == cudaSuccess) e = srv_pin(&s->h_chunks, nchunks);
+  if (e == cudaSuccess) e = srv_pin(&s->h_achunks, nchunks);
+  if (e == cudaSuccess) e = srv_pin(&s->h_live, nchunks);
   if (e == cudaSuccess) e = cudaMemset(S.done, 1, nslots);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) {
@@ -359,12 +417,10 @@ vgb_status vgb_server_submit(vgb_server *s, int64_t n, const double *x, const do
   const double *src[6] = {x, y, z, dx, dy, dz};
   for (int k = 0; k < 6; ++k)
     if (n) std::memcpy(r->in.data() + k * n, src[k], n * sizeof(double));
-  if (n == 0) {
-    r->finished = true;
+  if (n == 0)
     s->done[r->id] = r;
-  } else {
+  else
     s->queue.push_back(r);
-  }
   if (request_id) *request_id = r->id;
   return VGB_OK;
 }
@@ -380,21 +436,20 @@ vgb_status vgb_server_step(vgb_server *s, int64_t *completed, int32_t max_comple
   vgb_status st = admit(s);
   if (st != VGB_OK) return st;
   // chunk list of every admitted request
-  std::vector<int32_t> list;
-  std::vector<std::pair<size_t, size_t>> span(s->active.size());
+  int64_t nc = 0;
+  std::vector<std::pair<int64_t, int64_t>> span(s->active.size());
   for (size_t k = 0; k < s->active.size(); ++k) {
-    span[k].first = list.size();
-    list.insert(list.end(), s->active[k]->chunks.begin(), s->active[k]->chunks.end());
-    span[k].second = list.size();
+    span[k].first = nc;
+    for (int32_t c : s->active[k]->chunks) s->h_chunks[nc++] = c;
+    span[k].second = nc;
   }
-  std::vector<int32_t> live_h(list.size(), 0);
   int64_t live_total = 0;
-  if (!list.empty()) {
-    cudaError_t e = cudaMemcpyAsync(s->d_chunks, list.data(), list.size() * sizeof(int32_t),
+  if (nc > 0) {
+    cudaError_t e = cudaMemcpyAsync(s->d_chunks, s->h_chunks, nc * sizeof(int32_t),
                                     cudaMemcpyHostToDevice, s->stream);
-    if (e == cudaSuccess) e = cudaMemsetAsync(s->d_live, 0, list.size() * sizeof(int32_t), s->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(s->d_live, 0, nc * sizeof(int32_t), s->stream);
     if (e != cudaSuccess) return cuda_error(e, "vgb_server_step: chunk list");
-    const int64_t nt = (int64_t)list.size() * kChunk;
+    const int64_t nt = nc * kChunk;
     if (s->all_shapes)
       launch_step<kNavMaskAll>(s, nt);
     else
@@ -402,30 +457,58 @@ vgb_status vgb_server_step(vgb_server *s, int64_t *completed, int32_t max_comple
     count_launch();
     e = cudaGetLastError();
     if (e == cudaSuccess)
-      e = cudaMemcpyAsync(live_h.data(), s->d_live, list.size() * sizeof(int32_t),
-                          cudaMemcpyDeviceToHost, s->stream);
+      e = cudaMemcpyAsync(s->h_live, s->d_live, nc * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                          s->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
     if (e != cudaSuccess) return cuda_error(e, "vgb_server_step: step");
   }
-  // retire
-  std::vector<Request *> still;
-  int32_t nc = 0;
+  // retire: gather the finished requests' results in one launch and one copy
+  std::vector<Request *> still, fin;
+  int64_t nf = 0;
   for (size_t k = 0; k < s->active.size(); ++k) {
     int64_t l = 0;
-    for (size_t c = span[k].first; c < span[k].second; ++c) l += live_h[c];
+    for (int64_t c = span[k].first; c < span[k].second; ++c) l += s->h_live[c];
     live_total += l;
     Request *r = s->active[k];
     if (l == 0) {
-      r->finished = true;
-      s->done[r->id] = r;
-      if (completed && nc < max_completed) completed[nc] = r->id;
-      ++nc;
+      fin.push_back(r);
+      nf += (int64_t)r->chunks.size();
     } else {
       still.push_back(r);
     }
   }
+  if (!fin.empty()) {
+    int64_t c = 0;
+    for (Request *r : fin)
+      for (int32_t ch : r->chunks) s->h_chunks[c++] = ch;
+    const int64_t nt = nf * kChunk;
+    cudaError_t e = cudaMemcpyAsync(s->d_chunks, s->h_chunks, nf * sizeof(int32_t),
+                                    cudaMemcpyHostToDevice, s->stream);
+    if (e == cudaSuccess) {
+      const int grid = (int)std::min<int64_t>((nt + 255) / 256, 148 * 8);
+      k_srv_gather<<<grid, 256, 0, s->stream>>>(s->d_chunks, nt, s->S, s->d_out);
+      count_launch();
+      e = cudaGetLastError();
+    }
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(s->h_out, s->d_out, nt * sizeof(TrackResult), cudaMemcpyDeviceToHost,
+                          s->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    if (e != cudaSuccess) return cuda_error(e, "vgb_server_step: retire");
+    int64_t base = 0;
+    for (Request *r : fin) {
+      r->out.assign(s->h_out + base, s->h_out + base + r->n);
+      base += (int64_t)r->chunks.size() * kChunk;
+      for (int32_t ch : r->chunks) s->free_chunks.push_back(ch);
+      r->chunks.clear();
+      s->done[r->id] = r;
+    }
+  }
+  int32_t nout = 0;
+  for (Request *r : fin)
+    if (completed && nout < max_completed) completed[nout++] = r->id;
   s->active.swap(still);
-  if (ncompleted) *ncompleted = std::min(nc, max_completed);
+  if (ncompleted) *ncompleted = nout;
   if (live) *live = live_total;
   if (queued) *queued = (int64_t)s->queue.size();
   return VGB_OK;
@@ -439,25 +522,14 @@ vgb_status vgb_server_result(vgb_server *s, int64_t request_id, int32_t *nsteps,
     return set_error(VGB_EINVAL, "vgb_server_result: request %lld is not finished",
                      (long long)request_id);
   Request *r = it->second;
-  cudaError_t e = cudaSuccess;
-  for (size_t c = 0; c < r->chunks.size() && e == cudaSuccess; ++c) {
-    const int64_t first = (int64_t)c * kChunk, cnt = std::min<int64_t>(kChunk, r->n - first);
-    if (cnt <= 0) break;
-    const int64_t src = (int64_t)r->chunks[c] * kChunk;
-    if (nsteps && e == cudaSuccess)
-      e = cudaMemcpyAsync(nsteps + first, s->S.nsteps + src, cnt * 4, cudaMemcpyDeviceToHost, s->stream);
-    if (x && e == cudaSuccess)
-      e = cudaMemcpyAsync(x + first, s->S.x + src, cnt * 8, cudaMemcpyDeviceToHost, s->stream);
-    if (y && e == cudaSuccess)
-      e = cudaMemcpyAsync(y + first, s->S.y + src, cnt * 8, cudaMemcpyDeviceToHost, s->stream);
-    if (z && e == cudaSuccess)
-      e = cudaMemcpyAsync(z + first, s->S.z + src, cnt * 8, cudaMemcpyDeviceToHost, s->stream);
-    if (hash && e == cudaSuccess)
-      e = cudaMemcpyAsync(hash + first, s->S.hash + src, cnt * 8, cudaMemcpyDeviceToHost, s->stream);
+  for (int64_t t = 0; t < r->n; ++t) {
+    const TrackResult &o = r->out[t];
+    if (nsteps) nsteps[t] = o.nsteps;
+    if (x) x[t] = o.x;
+    if (y) y[t] = o.y;
+    if (z) z[t] = o.z;
+    if (hash) hash[t] = o.hash;
   }
-  if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
-  if (e != cudaSuccess) return cuda_error(e, "vgb_server_result");
-  for (int32_t c : r->chunks) s->free_chunks.push_back(c);
   s->done.erase(it);
   delete r;
   return VGB_OK;
