@@ -377,8 +377,9 @@ vgb_status vgb_nav_error_flags(const vgb_geometry *g, uint32_t *flags);
  * host memory and their slots are free for the next admission.  A track
  * finishes when its state leaves the world or after max_steps steps.  Per track
  * the server keeps what vgb_nav_trace would produce: the step count, the final
- * point and a 64-bit FNV-1a hash of its sequence of (next placed id, step)
- * records, so a request's results do not depend on what else was in flight.
+ * point and a 64-bit FNV-1a hash of its sequence of (next placed id, step,
+ * safety) records (int32, double, double, little-endian), so a request's
+ * results do not depend on what else was in flight.
  * ------------------------------------------------------------------------- */
 typedef struct vgb_server vgb_server;
 

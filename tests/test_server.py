@@ -1,7 +1,7 @@
 """Navigation server (continuous batching) on the layered detector.
 
 Each request's per-track results (step count, final point, FNV-1a hash of its
-(next placed id, step) records) must equal what vgb_nav_trace produces for the
+(next placed id, step, safety) records) must equal what vgb_nav_trace produces for the
 same tracks, whether the request is served alone or while other requests of
 uneven sizes arrive and finish around it.
 """
@@ -20,10 +20,11 @@ def fnv1a(data: bytes, h: int = 0xcbf29ce484222325) -> int:
     return h
 
 
-def fnv_hash(ids, steps):
-    """FNV-1a 64 over the little-endian bytes of (int32 id, float64 step) records."""
-    return fnv1a(b"".join(np.int32(i).tobytes() + np.float64(s).tobytes()
-                          for i, s in zip(ids, steps)))
+def fnv_hash(ids, steps, safeties):
+    """FNV-1a 64 over the little-endian bytes of (int32 id, float64 step,
+    float64 safety) records."""
+    return fnv1a(b"".join(np.int32(i).tobytes() + np.float64(s).tobytes() +
+                          np.float64(f).tobytes() for i, s, f in zip(ids, steps, safeties)))
 
 
 def test_fnv1a_known_answers():
@@ -49,12 +50,13 @@ def requests(sizes, seed):
 
 def trace_truth(g, pts, dirs):
     from test_navigation import gpu_trace
-    ids, steps, _, nst = gpu_trace(g, pts, dirs, MAX_STEPS)
+    ids, steps, saf, nst = gpu_trace(g, pts, dirs, MAX_STEPS)
     n = len(pts[0])
     ids = ids.reshape(n, MAX_STEPS)
     steps = steps.reshape(n, MAX_STEPS)
-    hashes = np.array([fnv_hash(ids[i, :nst[i]], steps[i, :nst[i]]) for i in range(n)],
-                      np.uint64)
+    saf = saf.reshape(n, MAX_STEPS)
+    hashes = np.array([fnv_hash(ids[i, :nst[i]], steps[i, :nst[i]], saf[i, :nst[i]])
+                       for i in range(n)], np.uint64)
     fx = np.array(pts[0], np.float64).copy()
     fy = np.array(pts[1], np.float64).copy()
     fz = np.array(pts[2], np.float64).copy()

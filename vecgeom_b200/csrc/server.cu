@@ -8,8 +8,9 @@
 //      buffer, and one launch scatters them into their slots, locates them
 //      (LocatePoint from the world) and clears their counters;
 //   2. step: one launch over the chunks of all admitted requests advances every
-//      live track by up to steps_per_launch steps (one warp per track, the
-//      navigator of navigation.cuh) and counts the tracks still live per chunk;
+//      live track by up to steps_per_launch steps, each GetSafety and
+//      FindNextBoundaryAndStep (one warp per track, the navigator of
+//      navigation.cuh), and counts the tracks still live per chunk;
 //   3. retire: the requests whose chunks have no live track are finished; one
 //      launch gathers their results into a staging buffer, one copy brings them
 //      to pinned host memory, and their chunks are free for the next admission.
@@ -126,12 +127,14 @@ __global__ void __launch_bounds__(kSrvBlock)
       const DXform m = nav_top_matrix(G, cur);
       const V3<double> lp = xf_point(m, p);
       const V3<double> ld = xf_dir(m, d);
+      const double sf = Nav::safety(G, cur, lp);
       double st = 0.;
       ok = Nav::step(G, cur, nxt, lp, ld, pstep, st);
       if (!ok) break;
       const int32_t id = nxt.top();
       h = fnv_bytes(h, &id, 4);
       h = fnv_bytes(h, &st, 8);
+      h = fnv_bytes(h, &sf, 8);
       p = {p.x + d.x * st, p.y + d.y * st, p.z + d.z * st};
       cur = nxt;
       ++k;
