@@ -117,10 +117,13 @@ vgb_status vgb_batch(const vgb_geometry *gc, int32_t placed, int32_t op, int64_t
   // host buffers: stage chunk by chunk
   const bool nd = op_needs_dir(op), ns = op_needs_step(op), na = op_needs_aux(op);
   const size_t osz = out_size(op);
-  const size_t per_pt = 24 + (nd ? 24 : 0) + (ns ? 8 : 0) + osz + (na ? 4 : 0) + 16;
   const int64_t chunk = n < (1 << 20) ? n : (1 << 20);
+  // every staged array starts on a 256-byte boundary; one half per stream
+  auto span = [&](size_t elem) { return ((chunk * elem + 255) / 256) * 256; };
+  const size_t half = 3 * span(8) + (nd ? 3 * span(8) : 0) + (ns ? span(8) : 0) + span(osz) +
+                      (na ? span(4) : 0);
   std::lock_guard<std::mutex> lock(g->staging_mu);
-  if ((st = ensure_staging(g, 2 * chunk * per_pt + 1024)) != VGB_OK) return st;
+  if ((st = ensure_staging(g, 2 * half)) != VGB_OK) return st;
   cudaStream_t *sts = g->staging_streams;
   cudaError_t e = cudaEventRecord(g->staging_start, s);
   if (e == cudaSuccess) e = cudaStreamWaitEvent(sts[0], g->staging_start, 0);
@@ -130,7 +133,7 @@ vgb_status vgb_batch(const vgb_geometry *gc, int32_t placed, int32_t op, int64_t
   for (int64_t b = 0, k = 0; b < n; b += chunk, ++k) {
     const int64_t m = (n - b < chunk) ? (n - b) : chunk;
     cudaStream_t cs = sts[k & 1];
-    char *p = base + (k & 1) * chunk * per_pt;
+    char *p = base + (k & 1) * half;
     auto carve = [&](size_t elem) {
       char *r = p;
       p += ((chunk * elem + 255) / 256) * 256;
