@@ -360,6 +360,36 @@ vgb_status vgb_nav_trace(const vgb_geometry *g, int64_t n, const double *x, cons
                          double pstep, int32_t max_steps, int32_t *next_ids, double *steps,
                          double *safeties, int32_t *nsteps, int32_t precision, void *stream);
 
+/* ABBoxNavigator::FindNextBoundaryAndStep (navigation/ABBoxNavigator.h:200-420)
+ * for n tracks; arguments and results as vgb_nav_find_next_boundary_and_step.
+ * The daughters are culled by ABBoxManager's aligned boxes (float ray-box
+ * test, source/ABBoxManager.cpp:88-126) and visited in the order of their box
+ * distance, and the new state follows ABBoxNavigator's own decisions (an
+ * infinite step beyond pstep returns pstep; leaving pops while the relocated
+ * path ends in the volume left).  safety[i] receives ABBoxNavigator::GetSafety
+ * (:424-452).  Equal box distances are visited in daughter order (libstdc++'s
+ * std::sort keeps that order for up to 16 hits). */
+vgb_status vgb_abbox_nav_find_next_boundary_and_step(const vgb_geometry *g, int64_t n,
+                                                     const double *x, const double *y,
+                                                     const double *z, const double *dx,
+                                                     const double *dy, const double *dz,
+                                                     const vgb_navpool *cur, vgb_navpool *next,
+                                                     const double *pstep, double *step,
+                                                     double *safety, void *stream);
+
+/* vgb_nav_trace with ABBoxNavigator's step (and its GetSafety). */
+vgb_status vgb_abbox_nav_trace(const vgb_geometry *g, int64_t n, const double *x, const double *y,
+                               const double *z, const double *dx, const double *dy,
+                               const double *dz, double pstep, int32_t max_steps,
+                               int32_t *next_ids, double *steps, double *safeties,
+                               int32_t *nsteps, void *stream);
+
+/* ABBoxManager::ComputeABBox (source/ABBoxManager.cpp:128-161) of a placed
+ * volume: lower xyz, upper xyz of its aligned box in the mother's frame, as
+ * doubles (the navigator uses them rounded to float).  Works on an open
+ * geometry too (host tables only). */
+vgb_status vgb_abbox_compute(const vgb_geometry *g, int32_t placed, double *lower_upper);
+
 /* Navigation error flags (VGB_NAV_ERR_*) raised since the last call; clears them. */
 vgb_status vgb_nav_error_flags(const vgb_geometry *g, uint32_t *flags);
 

@@ -135,6 +135,10 @@ class RefLib:
         L.vgref_placed_id.argtypes = [_vp]
         L.vgref_nav_trace.restype = _i
         L.vgref_nav_trace.argtypes = [_i64] + [_vp] * 6 + [_d, _i] + [_vp] * 4 + [_i]
+        L.vgref_abbox_compute.restype = None
+        L.vgref_abbox_compute.argtypes = [_vp, _vp]
+        L.vgref_abbox_nav_trace.restype = _i
+        L.vgref_abbox_nav_trace.argtypes = [_i64] + [_vp] * 6 + [_d, _i] + [_vp] * 4
         L.vgref_locate.restype = _i
         L.vgref_locate.argtypes = [_d, _d, _d, _vp]
         L.vgref_usphere_distance_to_in.restype = _i
@@ -207,6 +211,9 @@ class RefBuilder:
     def trd(self, dx1, dx2, dy1, dy2, dz):
         return self.L.vgref_trd(dx1, dx2, dy1, dy2, dz)
 
+    def shape(self, spec):
+        return ref_unplaced(self.ref, spec)
+
     def transform(self, tx=0., ty=0., tz=0., phi=0., theta=0., psi=0.):
         return self.L.vgref_transform_euler(tx, ty, tz, phi, theta, psi)
 
@@ -243,6 +250,28 @@ def ref_nav_trace(ref: RefLib, pts, dirs, pstep: float, max_steps: int, nthreads
     ref.L.vgref_nav_trace(n, _p(x), _p(y), _p(z), _p(dx), _p(dy), _p(dz), pstep, max_steps,
                           _p(ids), _p(steps), _p(saf), _p(nst), nthreads)
     return ids, steps, saf, nst
+
+
+def ref_abbox_nav_trace(ref: RefLib, pts, dirs, pstep: float, max_steps: int):
+    """ABBoxNavigator trace of the current reference world (single-threaded,
+    see ref_driver.cpp vgref_abbox_nav_trace); same records as ref_nav_trace."""
+    x, y, z = (np.ascontiguousarray(a, np.float64) for a in pts)
+    dx, dy, dz = (np.ascontiguousarray(a, np.float64) for a in dirs)
+    n = len(x)
+    ids = np.full(n * max_steps, -7, np.int32)
+    steps = np.zeros(n * max_steps)
+    saf = np.zeros(n * max_steps)
+    nst = np.zeros(n, np.int32)
+    ref.L.vgref_abbox_nav_trace(n, _p(x), _p(y), _p(z), _p(dx), _p(dy), _p(dz), pstep, max_steps,
+                                _p(ids), _p(steps), _p(saf), _p(nst))
+    return ids, steps, saf, nst
+
+
+def ref_abbox(ref: RefLib, placed) -> np.ndarray:
+    """ABBoxManager::ComputeABBox of a reference placed volume (lower, upper)."""
+    out = np.zeros(6)
+    ref.L.vgref_abbox_compute(placed, _p(out))
+    return out
 
 
 def ref_unplaced(ref: RefLib, spec):

@@ -285,6 +285,57 @@ int vgref_nav_trace(int64_t ntracks, const double *x, const double *y, const dou
   return 0;
 }
 
+// ---- ABBoxNavigator (navigation/ABBoxNavigator.h, source/ABBoxManager.cpp) ----
+// ABBoxManager::ComputeABBox of one placed volume: lower xyz, upper xyz.
+void vgref_abbox_compute(void *placed, double *out6) {
+  ABBoxManager::ABBox_t lo, hi;
+  ABBoxManager::ComputeABBox(static_cast<VPlacedVolume const *>(placed), &lo, &hi);
+  for (int k = 0; k < 3; ++k) {
+    out6[k] = lo[k];
+    out6[3 + k] = hi[k];
+  }
+}
+
+// ABBoxManager::InitABBoxesForCompleteGeometry, then the trace of
+// vgref_nav_trace with ABBoxNavigator::FindNextBoundaryAndStep / GetSafety.
+// Single-threaded: the reference's ABBoxManager shares one hit list
+// (navigation/ABBoxNavigator.h:79, :128-130).
+int vgref_abbox_nav_trace(int64_t ntracks, const double *x, const double *y, const double *z,
+                          const double *dx, const double *dy, const double *dz, double pstep,
+                          int max_steps, int *next_ids, double *steps, double *safeties,
+                          int *nsteps) {
+  ABBoxManager::Instance().InitABBoxesForCompleteGeometry();
+  const int depth = GeoManager::Instance().getMaxDepth();
+  VPlacedVolume const *world = GeoManager::Instance().GetWorld();
+  ABBoxNavigator nav;
+  SimpleNavigator locator;
+  NavigationState *cur = NavigationState::MakeInstance(depth);
+  NavigationState *nxt = NavigationState::MakeInstance(depth);
+  for (int64_t i = 0; i < ntracks; ++i) {
+    Vector3D<Precision> p(x[i], y[i], z[i]);
+    Vector3D<Precision> d(dx[i], dy[i], dz[i]);
+    cur->Clear();
+    locator.LocatePoint(world, p, *cur, true);
+    int k = 0;
+    while (!cur->IsOutside() && k < max_steps) {
+      double safety = nav.GetSafety(p, *cur);
+      double step = 0;
+      nxt->Clear();
+      nav.FindNextBoundaryAndStep(p, d, *cur, *nxt, pstep, step);
+      next_ids[i * max_steps + k] = nxt->IsOutside() ? -1 : nxt->Top()->id();
+      steps[i * max_steps + k] = step;
+      safeties[i * max_steps + k] = safety;
+      p = p + d * step;
+      std::swap(cur, nxt);
+      ++k;
+    }
+    nsteps[i] = k;
+  }
+  NavigationState::ReleaseInstance(cur);
+  NavigationState::ReleaseInstance(nxt);
+  return 0;
+}
+
 // Single calls for known-answer checks: LocatePoint from the world, returning
 // the id of Top() (-1 when outside) and the level.
 int vgref_locate(double x, double y, double z, int *level) {

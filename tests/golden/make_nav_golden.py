@@ -1,11 +1,34 @@
-"""Write tests/golden/nav/detector.npz from the reference itself.
+"""Write the navigation fixtures of tests/golden/nav/ from the reference itself.
 
-Builds the layered detector (vecgeom_b200.workloads.build_detector) in the
-reference (oracle/_ref/libvgref.so, built from the reference sources by
-``make -C oracle ref``) and traces tracks with its SimpleNavigator
-(LocatePoint, then GetSafety + FindNextBoundaryAndStep per step; see
-oracle/ref_driver.cpp vgref_nav_trace).  Next-volume ids are stored in this
-library's numbering (creation order of the placed volumes).
+Builds a geometry in the reference (oracle/_ref/libvgref.so, built from the
+reference sources by ``make -C oracle ref``) with the same builder code this
+library's tests use (vecgeom_b200.workloads) and traces tracks with the
+reference's navigators: LocatePoint, then GetSafety + FindNextBoundaryAndStep
+per step (oracle/ref_driver.cpp vgref_nav_trace / vgref_abbox_nav_trace).
+
+    detector.npz        layered detector, SimpleNavigator
+    detector_abbox.npz  layered detector, ABBoxNavigator
+    zoo.npz             mixed-shape geometry without the sphere and the torus,
+                        SimpleNavigator
+    zoo_abbox.npz       the same without the polyhedron too, ABBoxNavigator
+    row_abbox.npz       300 boxes on a line, ABBoxNavigator (hit lists longer
+                        than the GPU kernel's shared list)
+    zoo_boxes.npz       ABBoxManager::ComputeABBox of every placed volume of the
+                        mixed-shape geometry with all nine shapes
+
+Next-volume ids are positions in the list the geometry builder returns
+(for the detector that is also this library's placed-volume id).
+
+Why shapes are left out: the reference's SphereImplementation::DistanceToIn is
+a stub that returns kInfinity (volumes/kernel/SphereImplementation.h:84-93), so
+its navigators never enter a sphere, while this library runs USolids'
+USphere::DistanceToIn there; and the reference's polyhedron Contains reads past
+its z-segment array for points within kTolerance above the last z-plane
+(volumes/kernel/PolyhedronImplementation.h:745-780, FindZSegment returns the
+segment count), which ABBoxNavigator's Contains check of a box the point is in
+reaches when a track leaves a polyhedron through that plane.
+
+Every geometry is built in a fresh process: the reference keeps one world.
 
     python tests/golden/make_nav_golden.py
 """
@@ -25,9 +48,17 @@ from vecgeom_b200 import workloads as W  # noqa: E402
 
 N_ORIGIN = 256
 N_RANDOM = 256
+N_ZOO = 384
 MAX_STEPS = 64
 PSTEP = 1e30
 SEED = W.SEED_BASE + 5
+
+# the fixtures leave the torus out too: its GPU distances can differ from the
+# reference in the last bits (CUDA's and glibc's transcendentals), which a
+# trace would carry on; the CPU tests cover it against the live reference
+ZOO_EXCLUDE = {"zoo": ("sphere", "torus"), "zoo_abbox": ("sphere", "torus", "polyhedron"),
+               "zoo_torus": ("sphere",), "zoo_abbox_torus": ("sphere", "polyhedron"),
+               "zoo_all": ()}
 
 
 def nav_inputs():
@@ -42,25 +73,118 @@ def nav_inputs():
     return (cat(x0, x1), cat(y0, y1), cat(z0, z1)), (cat(dx0, dx1), cat(dy0, dy1), cat(dz0, dz1))
 
 
-def reference_trace(ref, pts, dirs, max_steps=MAX_STEPS, nthreads=1):
-    """Builds the detector in the reference and traces; ids mapped to ours."""
+def zoo_inputs():
+    return W.zoo_tracks(N_ZOO, SEED + 3)
+
+
+def build_row(b, n: int = 300, pitch: float = 8.) -> list:
+    """A world box (half 2000 mm, or more for long rows) with n small boxes
+    (half 2 mm) on the x axis, `pitch` mm apart from x = -1200 mm: a ray along
+    x has every one of them in its hit list."""
+    last = -1200. + pitch * (n - 1) + 2.
+    half = 2000. if last < 1900. else last + 100.
+    world_lv = b.logical("world", b.box(half, 2000., 2000.))
+    world = b.place(world_lv, b.transform())
+    placed = [world]
+    cell = b.logical("cell", b.box(2., 2., 2.))
+    for i in range(n):
+        placed.append(b.place_daughter(world_lv, cell, b.transform(-1200. + pitch * i, 0., 0.)))
+    b.set_world(world)
+    b.close()
+    return placed
+
+
+def row_inputs(n: int = 128):
+    """Tracks from x = -1900 mm towards +x, within 1 mm of the axis and 1e-3 rad."""
+    rng = np.random.default_rng(SEED + 4)
+    x = np.full(n, -1900.)
+    y, z = rng.uniform(-1., 1., n), rng.uniform(-1., 1., n)
+    d = np.stack([np.ones(n), rng.uniform(-1e-3, 1e-3, n), rng.uniform(-1e-3, 1e-3, n)])
+    d /= np.sqrt((d * d).sum(axis=0))
+    return (x, y, z), (d[0].copy(), d[1].copy(), d[2].copy())
+
+
+def build_geometry(b, geometry: str) -> list:
+    """The named geometry through a builder adapter; the placed volumes in
+    creation order."""
+    if geometry == "detector":
+        return W.build_detector(b)
+    if geometry == "row":
+        return build_row(b)
+    if geometry == "row_long":
+        return build_row(b, 6500, 5.)
+    return W.build_zoo(b, W.zoo_specs(exclude=ZOO_EXCLUDE[geometry]))
+
+
+def reference_trace(ref, pts, dirs, max_steps=MAX_STEPS, nthreads=1, geometry="detector",
+                    navigator="simple"):
+    """Builds the geometry in the reference and traces; ids mapped to list
+    positions.  ABBoxNavigator traces run on one thread (the reference's
+    ABBoxManager shares one hit list)."""
     rb = oracle.RefBuilder(ref)
-    placed = W.build_detector(rb)
+    placed = build_geometry(rb, geometry)
     to_ours = {int(r): k for k, r in enumerate(rb.ids(placed))}
-    ids, steps, saf, nst = oracle.ref_nav_trace(ref, pts, dirs, PSTEP, max_steps, nthreads)
+    if navigator == "simple":
+        ids, steps, saf, nst = oracle.ref_nav_trace(ref, pts, dirs, PSTEP, max_steps, nthreads)
+    else:
+        ids, steps, saf, nst = oracle.ref_abbox_nav_trace(ref, pts, dirs, PSTEP, max_steps)
     mapped = np.array([to_ours[int(i)] if i >= 0 else int(i) for i in ids], np.int32)
     return mapped, steps, saf, nst
 
 
+def reference_boxes(ref, geometry: str) -> np.ndarray:
+    """ABBoxManager::ComputeABBox of every placed volume, in list order."""
+    rb = oracle.RefBuilder(ref)
+    placed = build_geometry(rb, geometry)
+    return np.array([oracle.ref_abbox(ref, p) for p in placed])
+
+
+def _traced(pts, dirs, max_steps, nthreads, geometry, navigator):
+    return reference_trace(oracle.RefLib(), pts, dirs, max_steps, nthreads, geometry, navigator)
+
+
+def _boxes(geometry):
+    return reference_boxes(oracle.RefLib(), geometry)
+
+
+def isolated(fn, *args):
+    """fn(*args) in a fresh spawned process (a new reference world)."""
+    import multiprocessing as mp
+    from concurrent.futures import ProcessPoolExecutor
+    with ProcessPoolExecutor(max_workers=1, mp_context=mp.get_context("spawn")) as ex:
+        return ex.submit(fn, *args).result()
+
+
+def reference_trace_isolated(pts, dirs, max_steps=MAX_STEPS, nthreads=1, geometry="detector",
+                             navigator="simple"):
+    return isolated(_traced, pts, dirs, max_steps, nthreads, geometry, navigator)
+
+
+def reference_boxes_isolated(geometry: str) -> np.ndarray:
+    return isolated(_boxes, geometry)
+
+
 def main() -> None:
-    ref = oracle.RefLib()
-    pts, dirs = nav_inputs()
-    ids, steps, saf, nst = reference_trace(ref, pts, dirs)
-    path = os.path.join(HERE, "nav", "detector.npz")
-    np.savez_compressed(path, x=pts[0], y=pts[1], z=pts[2], dx=dirs[0], dy=dirs[1], dz=dirs[2],
-                        max_steps=MAX_STEPS, pstep=PSTEP, next_ids=ids, steps=steps,
-                        safeties=saf, nsteps=nst)
-    print("wrote", os.path.relpath(path, ROOT), "mean steps", float(nst.mean()))
+    out = os.path.join(HERE, "nav")
+    for name, geometry, navigator, inputs in (
+            ("detector", "detector", "simple", nav_inputs),
+            ("detector_abbox", "detector", "abbox", nav_inputs),
+            ("zoo", "zoo", "simple", zoo_inputs),
+            ("zoo_abbox", "zoo_abbox", "abbox", zoo_inputs),
+            ("row_abbox", "row", "abbox", row_inputs)):
+        pts, dirs = inputs()
+        ids, steps, saf, nst = reference_trace_isolated(pts, dirs, MAX_STEPS, 1, geometry,
+                                                        navigator)
+        path = os.path.join(out, name + ".npz")
+        np.savez_compressed(path, x=pts[0], y=pts[1], z=pts[2], dx=dirs[0], dy=dirs[1],
+                            dz=dirs[2], max_steps=MAX_STEPS, pstep=PSTEP, next_ids=ids,
+                            steps=steps, safeties=saf, nsteps=nst, geometry=geometry,
+                            navigator=navigator)
+        print("wrote", os.path.relpath(path, ROOT), "mean steps", float(nst.mean()))
+    boxes = reference_boxes_isolated("zoo_all")
+    path = os.path.join(out, "zoo_boxes.npz")
+    np.savez_compressed(path, boxes=boxes)
+    print("wrote", os.path.relpath(path, ROOT), boxes.shape)
 
 
 if __name__ == "__main__":

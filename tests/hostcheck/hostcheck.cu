@@ -6,9 +6,13 @@
 //
 // Built with -ffp-contract=off, like the FP64 kernels (-fmad=false), so the
 // host results round like the device results (transcendentals aside).
+#include <algorithm>
+#include <utility>
+#include <vector>
+
 #include "../../vecgeom_b200/csrc/batch.cuh"
 #include "../../vecgeom_b200/csrc/geometry.h"
-#include "../../vecgeom_b200/csrc/navigation.cuh"
+#include "../../vecgeom_b200/csrc/abbox.cuh"
 
 using namespace vgb;
 
@@ -76,7 +80,7 @@ extern "C" int hc_nav_trace(vgb_geometry *g, int64_t n, const double *x, const d
   if (prepare_tables(g) != VGB_OK) return -1;
   const NavGeom G = {g->params.data(),    g->unplaced.data(), g->placed.data(),
                      g->xforms.data(),    g->nav_raw.data(),  g->logicals.data(),
-                     g->daughters.data(), g->pl_box.data(),   g->world,
+                     g->daughters.data(), g->pl_box.data(),   g->ab_box.data(), g->world,
                      g->max_depth};
   if (screen) return trace_host<Navigator<OneLane, kNavMaskAll, true>>(G, n, x, y, z, dx, dy, dz, pstep,
                                                                        max_steps, next_ids, steps,
@@ -114,6 +118,68 @@ int trace_host(const NavGeom &G, int64_t n, const double *x, const double *y, co
       ++k;
     }
     nsteps[i] = ok ? k : -1;
+  }
+  return 0;
+}
+
+// ABBoxNavigator (abbox.cuh) with a single lane and a hit list of `cap`
+// entries (a small cap exercises the one-by-one walk of long lists).
+extern "C" int hc_abbox_trace(vgb_geometry *g, int64_t n, const double *x, const double *y,
+                              const double *z, const double *dx, const double *dy,
+                              const double *dz, double pstep, int32_t max_steps,
+                              int32_t *next_ids, double *steps, double *safeties, int32_t *nsteps,
+                              int32_t cap) {
+  if (prepare_tables(g) != VGB_OK || cap < 1) return -1;
+  const NavGeom G = {g->params.data(),    g->unplaced.data(), g->placed.data(),
+                     g->xforms.data(),    g->nav_raw.data(),  g->logicals.data(),
+                     g->daughters.data(), g->pl_box.data(),   g->ab_box.data(), g->world,
+                     g->max_depth};
+  using Nav = ABBoxNavigator<OneLane, kNavMaskAll>;
+  std::vector<AbCand> buf((size_t)cap + kAbSortThreshold);
+  for (int64_t i = 0; i < n; ++i) {
+    V3<double> p = {x[i], y[i], z[i]};
+    const V3<double> d = {dx[i], dy[i], dz[i]};
+    NavPath cur, nxt;
+    bool ok = Navigator<OneLane, kNavMaskAll>::locate_from_world(G, cur, p);
+    int32_t k = 0;
+    while (ok && cur.level > 0 && k < max_steps) {
+      const DXform m = nav_top_matrix(G, cur);
+      const V3<double> lp = xf_point(m, p);
+      const V3<double> ld = xf_dir(m, d);
+      const double sf = Nav::safety(G, cur, lp);
+      double st = 0.;
+      ok = Nav::step(G, cur, nxt, lp, ld, pstep, st, buf.data(), cap);
+      if (!ok) break;
+      const int64_t r = i * (int64_t)max_steps + k;
+      next_ids[r] = nxt.top();
+      steps[r] = st;
+      safeties[r] = sf;
+      p = {p.x + d.x * st, p.y + d.y * st, p.z + d.z * st};
+      cur = nxt;
+      ++k;
+    }
+    nsteps[i] = ok ? k : -1;
+  }
+  return 0;
+}
+
+// The introsort restatement of abbox.cuh next to the standard library's
+// std::sort (of this build, libstdc++) on the same (distance, index) pairs with
+// HitBoxComparatorFunctor's comparison; writes both orders of indices.
+extern "C" int hc_abbox_sort_check(const float *b, int32_t n, int32_t *ours, int32_t *std_order) {
+  std::vector<AbCand> a((size_t)n);
+  std::vector<std::pair<int, double>> h((size_t)n);
+  for (int i = 0; i < n; ++i) {
+    a[i] = AbCand{b[i], i};
+    h[i] = std::pair<int, double>(i, (double)b[i]);
+  }
+  ab_sort_like_libstdcxx(a.data(), n);
+  std::sort(h.begin(), h.end(), [](const std::pair<int, double> &l, const std::pair<int, double> &r) {
+    return l.second < r.second;
+  });
+  for (int i = 0; i < n; ++i) {
+    ours[i] = a[i].d;
+    std_order[i] = h[i].first;
   }
   return 0;
 }

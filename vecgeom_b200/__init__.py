@@ -9,8 +9,8 @@ from ._lib import (VgbError, lib, LIB_PATH, PREC_FP64, PREC_FP32_REFINE,  # noqa
                    OP_SAFETY_TO_IN_MINIMIZE, OP_SAFETY_TO_OUT_MINIMIZE,
                    OP_DISTANCE_TO_OUT_NODE, OP_PLACED_DISTANCE_TO_OUT)
 from .geometry import (Geometry, LogicalVolume, PlacedVolume, SOA3D,  # noqa: F401
-                       NavStatePool, SimpleNavigator, BasketPlan, NavServer,
-                       kInside, kSurface, kOutside, kTolerance, kInfinity)
+                       NavStatePool, SimpleNavigator, ABBoxNavigator, ComputeABBox,
+                       BasketPlan, NavServer, kInside, kSurface, kOutside, kTolerance, kInfinity)
 
 __all__ = ["Geometry", "LogicalVolume", "PlacedVolume", "SOA3D", "NavStatePool",
-           "SimpleNavigator", "BasketPlan", "NavServer", "VgbError", "lib"]
+           "SimpleNavigator", "ABBoxNavigator", "ComputeABBox", "BasketPlan", "NavServer", "VgbError", "lib"]

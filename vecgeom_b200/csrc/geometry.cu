@@ -7,6 +7,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <limits>
 #include <new>
 
 #include "geometry.h"
@@ -161,6 +162,7 @@ vgb_status vgb_geometry_destroy(vgb_geometry *g) {
     cudaFree(g->dev.raw);
     cudaFree(g->dev.nav_flags);
     cudaFree(g->dev.pl_box);
+    cudaFree(g->dev.ab_box);
     cudaFree(g->dev.placed);
     cudaFree(g->dev.logicals);
     cudaFree(g->dev.daughters);
@@ -283,6 +285,9 @@ vgb_status vgb::prepare_tables(vgb_geometry *g) {
     g->logicals[l].dcount = (int32_t)g->logical_daughters[l].size();
     for (int32_t d : g->logical_daughters[l]) g->daughters.push_back(d);
   }
+  g->max_daughters = 0;
+  for (const LogicalRec &l : g->logicals)
+    if (l.dcount > g->max_daughters) g->max_daughters = l.dcount;
   if (g->world >= 0) {
     g->max_depth = depth_of(g, g->placed[g->world].logical, 0);
     if (g->max_depth < 0)
@@ -352,6 +357,44 @@ vgb_status vgb::prepare_tables(vgb_geometry *g) {
       o[3 + k] = std::nextafter((float)(hi[k] + pad), 3.0e38f);
     }
   }
+  // ABBoxManager::ComputeABBox (source/ABBoxManager.cpp:128-161): the 8 corners
+  // of the shape's Extent, moved to the mother's frame with InverseTransform
+  // (base/Transformation3D.h:598-632), their min / max (std::min, std::max, in
+  // the reference's corner order) widened by 1e-3; InitABBoxes
+  // (:185-262) keeps a float copy for the navigator's hit test
+  g->ab_box_d.assign(6 * g->placed.size(), 0.);
+  g->ab_box.assign(6 * g->placed.size(), 0.f);
+  for (size_t pv = 0; pv < g->placed.size(); ++pv) {
+    const UnplacedRec &u = g->unplaced[g->placed[pv].unplaced];
+    double lo[3], hi[3];
+    if (!reference_extent(u.type, g->params.data() + u.param_off, lo, hi))
+      return set_error(VGB_EINVAL, "vgb_geometry_close: no extent for shape type %d", u.type);
+    const RawXform &x = g->raw_xforms[g->placed[pv].raw_xform];
+    const double delta[3] = {hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2]};
+    double mn[3], mx[3];
+    for (int k = 0; k < 3; ++k) {
+      mn[k] = std::numeric_limits<double>::infinity();
+      mx[k] = -std::numeric_limits<double>::infinity();
+    }
+    for (int cx = 0; cx <= 1; ++cx)
+      for (int cy = 0; cy <= 1; ++cy)
+        for (int cz = 0; cz <= 1; ++cz) {
+          const double c[3] = {lo[0] + cx * delta[0], lo[1] + cy * delta[1], lo[2] + cz * delta[2]};
+          for (int k = 0; k < 3; ++k) {
+            double m = x.t[k];
+            m = m + c[0] * x.r[3 * k];
+            m = m + c[1] * x.r[3 * k + 1];
+            m = m + c[2] * x.r[3 * k + 2];
+            mn[k] = vmin(mn[k], m);
+            mx[k] = vmax(mx[k], m);
+          }
+        }
+    for (int k = 0; k < 3; ++k) {
+      g->ab_box_d[6 * pv + k] = mn[k] - 1E-3;
+      g->ab_box_d[6 * pv + 3 + k] = mx[k] + 1E-3;
+    }
+    for (int k = 0; k < 6; ++k) g->ab_box[6 * pv + k] = (float)g->ab_box_d[6 * pv + k];
+  }
   return VGB_OK;
 }
 
@@ -390,7 +433,21 @@ vgb_status vgb_geometry_close(vgb_geometry *g) {
     if ((s = upload(zero, &g->dev.nav_flags, &g->dev.bytes)) != VGB_OK) return s;
   }
   if ((s = upload(g->pl_box, &g->dev.pl_box, &g->dev.bytes)) != VGB_OK) return s;
+  if ((s = upload(g->ab_box, &g->dev.ab_box, &g->dev.bytes)) != VGB_OK) return s;
   g->closed = true;
+  return VGB_OK;
+}
+
+vgb_status vgb_abbox_compute(const vgb_geometry *g, int32_t placed, double *lower_upper) {
+  if (!g || !lower_upper) return set_error(VGB_EINVAL, "vgb_abbox_compute: NULL argument");
+  if (placed < 0 || placed >= (int32_t)g->placed.size())
+    return set_error(VGB_EINVAL, "vgb_abbox_compute: unknown placed volume %d", placed);
+  vgb_geometry *gm = const_cast<vgb_geometry *>(g);
+  if (!g->closed) {
+    vgb_status s = prepare_tables(gm);
+    if (s != VGB_OK) return s;
+  }
+  for (int k = 0; k < 6; ++k) lower_upper[k] = g->ab_box_d[6 * (size_t)placed + k];
   return VGB_OK;
 }
 

@@ -72,6 +72,7 @@ struct DeviceImage {
   int32_t *daughters = nullptr;
   uint32_t *nav_flags = nullptr;  // navigation error bits (VGB_NAV_ERR_*)
   float *pl_box = nullptr;        // per placed: enclosing box in the mother's frame
+  float *ab_box = nullptr;        // per placed: ABBoxManager's aligned box (float), mother frame
   int64_t bytes = 0;
 };
 
@@ -90,9 +91,12 @@ struct vgb_geometry {
   std::vector<vgb::NavXform> nav_raw;  // per Transformation3D, for the navigator
   std::vector<float> bbox;             // per unplaced: 6 floats, enclosing box (own frame)
   std::vector<float> pl_box;           // per placed: 6 floats, enclosing box (mother frame)
+  std::vector<double> ab_box_d;        // per placed: ABBoxManager::ComputeABBox (lower, upper)
+  std::vector<float> ab_box;           // the same boxes rounded to float, as navigated
   uint32_t type_mask = 0;              // bit t set when a shape of type t exists
   int32_t world = -1;
   int32_t max_depth = 0;
+  int32_t max_daughters = 0;  // the most daughters of any logical volume
   bool closed = false;
   int device = -1;
   vgb::DeviceImage dev;
@@ -118,6 +122,9 @@ vgb_status prepare_tables(vgb_geometry *g);
 // Axis-aligned box (min xyz, max xyz) in the shape's own frame that encloses
 // the shape; false for unknown types.
 bool shape_bbox(const vgb_geometry *g, int32_t unplaced, double box[6]);
+// The reference's Extent of a shape record (lower and upper corner in its own
+// frame, VPlacedVolume::Extent, volumes/PlacedVolume.h:260); false for unknown types.
+bool reference_extent(int type, const double *rec, double lo[3], double hi[3]);
 // Appends a shape record to the parameter pool (16-byte aligned).
 vgb_status add_unplaced(vgb_geometry *g, int type, const void *rec, size_t bytes, int32_t extra,
                         int32_t *id);

@@ -35,6 +35,7 @@ struct NavGeom {
   const LogicalRec *logicals;   // daughter range per logical volume
   const int32_t *daughters;     // CSR over logicals
   const float *pl_box;          // per placed: enclosing box in the mother's frame (6 floats)
+  const float *ab_box;          // per placed: ABBoxManager's aligned box, float (6 floats)
   int32_t world;
   int32_t max_depth;            // levels of the deepest path
 };
@@ -86,6 +87,10 @@ struct WarpLanes {
   static VGB_D uint32_t ballot(bool b) { return __ballot_sync(0xffffffffu, b); }
   static VGB_D double shfl_xor(double v, int m) { return __shfl_xor_sync(0xffffffffu, v, m); }
   static VGB_D int shfl_xor(int v, int m) { return __shfl_xor_sync(0xffffffffu, v, m); }
+  static VGB_D float shfl_xor(float v, int m) { return __shfl_xor_sync(0xffffffffu, v, m); }
+  static VGB_D double shfl_up(double v, int d) { return __shfl_up_sync(0xffffffffu, v, d); }
+  static VGB_D uint32_t lanes_below() { return (1u << lane()) - 1u; }
+  static VGB_D void sync() { __syncwarp(); }
 };
 #endif
 struct OneLane {
@@ -94,6 +99,10 @@ struct OneLane {
   static VGB_HD uint32_t ballot(bool b) { return b ? 1u : 0u; }
   static VGB_HD double shfl_xor(double v, int) { return v; }
   static VGB_HD int shfl_xor(int v, int) { return v; }
+  static VGB_HD float shfl_xor(float v, int) { return v; }
+  static VGB_HD double shfl_up(double v, int) { return v; }
+  static VGB_HD uint32_t lanes_below() { return 0u; }
+  static VGB_HD void sync() {}
 };
 
 VGB_HD int nav_lowbit(uint32_t b) {
@@ -108,6 +117,14 @@ VGB_HD int nav_highbit(uint32_t b) {
   return 31 - __clz(b);
 #else
   return 31 - __builtin_clz(b);
+#endif
+}
+
+VGB_HD int nav_popc(uint32_t b) {
+#ifdef __CUDA_ARCH__
+  return __popc(b);
+#else
+  return __builtin_popcount(b);
 #endif
 }
 

@@ -6,7 +6,7 @@
 // launch picks the smallest set that covers the geometry.
 #include <cstring>
 
-#include "navigation.cuh"
+#include "abbox.cuh"
 
 using namespace vgb;
 
@@ -40,6 +40,7 @@ NavGeom nav_geom(const vgb_geometry *g) {
   G.logicals = g->dev.logicals;
   G.daughters = g->dev.daughters;
   G.pl_box = g->dev.pl_box;
+  G.ab_box = g->dev.ab_box;
   G.world = g->world;
   G.max_depth = g->max_depth;
   return G;
@@ -141,22 +142,103 @@ __global__ void __launch_bounds__(kNavBlock)
   }
 }
 
+// ABBoxNavigator kernels: the same loops with the box-culled step; each warp
+// keeps its hit list in dynamic shared memory (cap hits, and the rank-sorted
+// copy of a list of up to 16 beside them).  Volumes with more than kAbMaxCap
+// daughters fall back to the one-by-one walk when a ray hits more boxes.
+constexpr int kAbMaxCap = 6144;
+extern __shared__ AbCand vgb_ab_lists[];
+
+template <uint32_t kMask>
+__global__ void __launch_bounds__(kNavBlock)
+    k_abbox_step(const NavGeom G, int32_t cap, int64_t n, const double *x, const double *y, const double *z,
+                 const double *dx, const double *dy, const double *dz, const unsigned char *cur,
+                 unsigned char *next, int64_t stride, const double *pstep, double *step_out,
+                 double *safety_out, uint32_t *flags) {
+  using Nav = ABBoxNavigator<WarpLanes, kMask>;
+  AbCand *buf = vgb_ab_lists + (threadIdx.x / 32) * (cap + kAbSortThreshold);
+  const int64_t warps = (int64_t)gridDim.x * kNavWarps;
+  for (int64_t i = (int64_t)blockIdx.x * kNavWarps + threadIdx.x / 32; i < n; i += warps) {
+    NavPath c, nx;
+    nav_load(c, NavStateRef{const_cast<unsigned char *>(cur) + i * stride});
+    const V3<double> p = {x[i], y[i], z[i]};
+    const V3<double> d = {dx[i], dy[i], dz[i]};
+    double st = 0., sf = 0.;
+    bool ok = true;
+    nx = c;
+    if (c.level > 0) {
+      const DXform m = nav_top_matrix(G, c);
+      const V3<double> lp = xf_point(m, p);
+      const V3<double> ld = xf_dir(m, d);
+      if (safety_out) sf = Nav::safety(G, c, lp);
+      ok = Nav::step(G, c, nx, lp, ld, pstep[i], st, buf, cap);
+    }
+    if (WarpLanes::lane() == 0) {
+      if (!ok) nav_raise(flags, VGB_NAV_ERR_DEPTH);
+      nav_store(nx, NavStateRef{next + i * stride}, G.max_depth);
+      step_out[i] = st;
+      if (safety_out) safety_out[i] = sf;
+    }
+  }
+}
+
+template <uint32_t kMask>
+__global__ void __launch_bounds__(kNavBlock)
+    k_abbox_trace(const NavGeom G, int32_t cap, int64_t n, const double *x, const double *y, const double *z,
+                  const double *dx, const double *dy, const double *dz, double pstep,
+                  int32_t max_steps, int32_t *next_ids, double *steps, double *safeties,
+                  int32_t *nsteps, uint32_t *flags) {
+  using Nav = ABBoxNavigator<WarpLanes, kMask>;
+  AbCand *buf = vgb_ab_lists + (threadIdx.x / 32) * (cap + kAbSortThreshold);
+  const int64_t warps = (int64_t)gridDim.x * kNavWarps;
+  const bool lane0 = WarpLanes::lane() == 0;
+  for (int64_t i = (int64_t)blockIdx.x * kNavWarps + threadIdx.x / 32; i < n; i += warps) {
+    V3<double> p = {x[i], y[i], z[i]};
+    const V3<double> d = {dx[i], dy[i], dz[i]};
+    NavPath cur, nxt;
+    bool ok = Navigator<WarpLanes, kMask>::locate_from_world(G, cur, p);
+    int32_t k = 0;
+    while (ok && cur.level > 0 && k < max_steps) {
+      const DXform m = nav_top_matrix(G, cur);
+      const V3<double> lp = xf_point(m, p);
+      const V3<double> ld = xf_dir(m, d);
+      const double sf = Nav::safety(G, cur, lp);
+      double st = 0.;
+      ok = Nav::step(G, cur, nxt, lp, ld, pstep, st, buf, cap);
+      if (!ok) break;
+      if (lane0) {
+        const int64_t r = i * (int64_t)max_steps + k;
+        if (next_ids) next_ids[r] = nxt.top();
+        if (steps) steps[r] = st;
+        if (safeties) safeties[r] = sf;
+      }
+      p = {p.x + d.x * st, p.y + d.y * st, p.z + d.z * st};
+      cur = nxt;
+      ++k;
+    }
+    if (lane0) {
+      if (!ok) nav_raise(flags, VGB_NAV_ERR_DEPTH);
+      nsteps[i] = ok ? k : -1;
+    }
+  }
+}
+
 // Launches K<kMask, kScreen> for the smallest shape set covering the geometry;
 // kScreen (the float screen of the FP32+refine form) when precision asks for it.
 template <template <uint32_t, bool> class K, class... A>
-vgb_status nav_launch(const vgb_geometry *g, int64_t n, cudaStream_t s, int precision,
+vgb_status nav_launch(const vgb_geometry *g, int64_t n, cudaStream_t s, int precision, size_t smem,
                       A... args) {
   const int grid = nav_grid(n);
   const bool small = (g->type_mask & ~kNavMaskBoxTubeTrd) == 0;
   const bool screen = precision == VGB_PREC_FP32_REFINE;
   if (small && screen)
-    K<kNavMaskBoxTubeTrd, true>::launch(grid, s, args...);
+    K<kNavMaskBoxTubeTrd, true>::launch(grid, smem, s, args...);
   else if (small)
-    K<kNavMaskBoxTubeTrd, false>::launch(grid, s, args...);
+    K<kNavMaskBoxTubeTrd, false>::launch(grid, smem, s, args...);
   else if (screen)
-    K<kNavMaskAll, true>::launch(grid, s, args...);
+    K<kNavMaskAll, true>::launch(grid, smem, s, args...);
   else
-    K<kNavMaskAll, false>::launch(grid, s, args...);
+    K<kNavMaskAll, false>::launch(grid, smem, s, args...);
   count_launch();
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_error(e, "navigation kernel launch");
@@ -164,20 +246,43 @@ vgb_status nav_launch(const vgb_geometry *g, int64_t n, cudaStream_t s, int prec
 }
 
 template <uint32_t M, bool> struct LocateK {
-  template <class... A> static void launch(int grid, cudaStream_t s, A... a) {
+  template <class... A> static void launch(int grid, size_t, cudaStream_t s, A... a) {
     k_nav_locate<M><<<grid, kNavBlock, 0, s>>>(a...);
   }
 };
 template <uint32_t M, bool S> struct StepK {
-  template <class... A> static void launch(int grid, cudaStream_t s, A... a) {
+  template <class... A> static void launch(int grid, size_t, cudaStream_t s, A... a) {
     k_nav_step<M, S><<<grid, kNavBlock, 0, s>>>(a...);
   }
 };
 template <uint32_t M, bool S> struct TraceK {
-  template <class... A> static void launch(int grid, cudaStream_t s, A... a) {
+  template <class... A> static void launch(int grid, size_t, cudaStream_t s, A... a) {
     k_nav_trace<M, S><<<grid, kNavBlock, 0, s>>>(a...);
   }
 };
+
+template <uint32_t M, bool> struct AbStepK {
+  template <class... A> static void launch(int grid, size_t smem, cudaStream_t s, A... a) {
+    cudaFuncSetAttribute(k_abbox_step<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_abbox_step<M><<<grid, kNavBlock, smem, s>>>(a...);
+  }
+};
+template <uint32_t M, bool> struct AbTraceK {
+  template <class... A> static void launch(int grid, size_t smem, cudaStream_t s, A... a) {
+    cudaFuncSetAttribute(k_abbox_trace<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_abbox_trace<M><<<grid, kNavBlock, smem, s>>>(a...);
+  }
+};
+
+// Hit-list capacity per warp: the most daughters of any volume (so every list
+// fits and is ordered as the reference orders it), rounded up to 32 and kept
+// within kAbMaxCap; dynamic shared memory of a block for it.
+int abbox_cap(const vgb_geometry *g) {
+  int cap = (g->max_daughters + 31) / 32 * 32;
+  if (cap < 32) cap = 32;
+  return cap > kAbMaxCap ? kAbMaxCap : cap;
+}
+size_t abbox_smem(int cap) { return (size_t)kNavWarps * (cap + kAbSortThreshold) * sizeof(AbCand); }
 
 vgb_status check_nav_geometry(const vgb_geometry *g, const char *fn) {
   if (!g) return set_error(VGB_EINVAL, "%s: geometry is NULL", fn);
@@ -290,7 +395,7 @@ vgb_status vgb_nav_locate(const vgb_geometry *g, int64_t n, const double *x, con
   if (n == 0) return VGB_OK;
   if (!is_device_ptr(x) || !is_device_ptr(y) || !is_device_ptr(z))
     return set_error(VGB_EINVAL, "vgb_nav_locate: points must be device memory");
-  return nav_launch<LocateK>(g, n, (cudaStream_t)stream, VGB_PREC_FP64, nav_geom(g), n, x, y, z,
+  return nav_launch<LocateK>(g, n, (cudaStream_t)stream, VGB_PREC_FP64, 0, nav_geom(g), n, x, y, z,
                              states->dev,
                              states->stride, g->dev.nav_flags);
 }
@@ -316,7 +421,7 @@ vgb_status vgb_nav_find_next_boundary_and_step(const vgb_geometry *g, int64_t n,
     if (!is_device_ptr(p)) return set_error(VGB_EINVAL, "%s: arrays must be device memory", fn);
   if (safety && !is_device_ptr(safety))
     return set_error(VGB_EINVAL, "%s: safety must be device memory or NULL", fn);
-  return nav_launch<StepK>(g, n, (cudaStream_t)stream, precision, nav_geom(g), n, x, y, z, dx,
+  return nav_launch<StepK>(g, n, (cudaStream_t)stream, precision, 0, nav_geom(g), n, x, y, z, dx,
                            dy, dz,
                            (const unsigned char *)cur->dev, next->dev, cur->stride, pstep, step,
                            safety, g->dev.nav_flags);
@@ -340,10 +445,60 @@ vgb_status vgb_nav_trace(const vgb_geometry *g, int64_t n, const double *x, cons
   for (const void *p : opt)
     if (p && !is_device_ptr(p))
       return set_error(VGB_EINVAL, "%s: records must be device memory or NULL", fn);
-  return nav_launch<TraceK>(g, n, (cudaStream_t)stream, precision, nav_geom(g), n, x, y, z, dx,
+  return nav_launch<TraceK>(g, n, (cudaStream_t)stream, precision, 0, nav_geom(g), n, x, y, z, dx,
                             dy, dz,
                             pstep, max_steps, next_ids, steps, safeties, nsteps,
                             g->dev.nav_flags);
+}
+
+vgb_status vgb_abbox_nav_find_next_boundary_and_step(const vgb_geometry *g, int64_t n,
+                                                     const double *x, const double *y,
+                                                     const double *z, const double *dx,
+                                                     const double *dy, const double *dz,
+                                                     const vgb_navpool *cur, vgb_navpool *next,
+                                                     const double *pstep, double *step,
+                                                     double *safety, void *stream) {
+  const char *fn = "vgb_abbox_nav_find_next_boundary_and_step";
+  vgb_status s = check_nav_geometry(g, fn);
+  if (s != VGB_OK) return s;
+  if (!cur || !next || cur == next || n < 0 || n > cur->n || n > next->n ||
+      cur->max_depth != g->max_depth || next->max_depth != g->max_depth)
+    return set_error(VGB_EINVAL, "%s: need two distinct pools of the geometry's depth", fn);
+  if (n == 0) return VGB_OK;
+  const void *ptrs[] = {x, y, z, dx, dy, dz, pstep, step};
+  for (const void *p : ptrs)
+    if (!is_device_ptr(p)) return set_error(VGB_EINVAL, "%s: arrays must be device memory", fn);
+  if (safety && !is_device_ptr(safety))
+    return set_error(VGB_EINVAL, "%s: safety must be device memory or NULL", fn);
+  const int cap = abbox_cap(g);
+  return nav_launch<AbStepK>(g, n, (cudaStream_t)stream, VGB_PREC_FP64, abbox_smem(cap),
+                             nav_geom(g), (int32_t)cap, n, x, y, z,
+                             dx, dy, dz, (const unsigned char *)cur->dev, next->dev, cur->stride,
+                             pstep, step, safety, g->dev.nav_flags);
+}
+
+vgb_status vgb_abbox_nav_trace(const vgb_geometry *g, int64_t n, const double *x, const double *y,
+                               const double *z, const double *dx, const double *dy,
+                               const double *dz, double pstep, int32_t max_steps,
+                               int32_t *next_ids, double *steps, double *safeties,
+                               int32_t *nsteps, void *stream) {
+  const char *fn = "vgb_abbox_nav_trace";
+  vgb_status s = check_nav_geometry(g, fn);
+  if (s != VGB_OK) return s;
+  if (n < 0 || max_steps < 0) return set_error(VGB_EINVAL, "%s: n or max_steps < 0", fn);
+  if (n == 0) return VGB_OK;
+  const void *ptrs[] = {x, y, z, dx, dy, dz, nsteps};
+  for (const void *p : ptrs)
+    if (!is_device_ptr(p)) return set_error(VGB_EINVAL, "%s: arrays must be device memory", fn);
+  const void *opt[] = {next_ids, steps, safeties};
+  for (const void *p : opt)
+    if (p && !is_device_ptr(p))
+      return set_error(VGB_EINVAL, "%s: records must be device memory or NULL", fn);
+  const int cap = abbox_cap(g);
+  return nav_launch<AbTraceK>(g, n, (cudaStream_t)stream, VGB_PREC_FP64, abbox_smem(cap),
+                              nav_geom(g), (int32_t)cap, n, x, y, z,
+                              dx, dy, dz, pstep, max_steps, next_ids, steps, safeties, nsteps,
+                              g->dev.nav_flags);
 }
 
 vgb_status vgb_nav_error_flags(const vgb_geometry *g, uint32_t *flags) {

@@ -173,6 +173,7 @@ NavGeom server_geom(const vgb_geometry *g) {
   G.logicals = g->dev.logicals;
   G.daughters = g->dev.daughters;
   G.pl_box = g->dev.pl_box;
+  G.ab_box = g->dev.ab_box;
   G.world = g->world;
   G.max_depth = g->max_depth;
   return G;

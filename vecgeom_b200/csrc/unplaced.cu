@@ -577,6 +577,103 @@ bool shape_bbox(const vgb_geometry *g, int32_t u, double b[6]) {
   }
 }
 
+// UnplacedTube::Extent (source/UnplacedTube.cpp:244-295): the full box, cut
+// back on the sides whose axis direction (phi = 0, 90, 180, 270 deg) lies
+// outside the phi section.
+static void tube_extent(const TubeP &t, double lo[3], double hi[3]) {
+  lo[0] = -t.rmax; lo[1] = -t.rmax; lo[2] = -t.z;
+  hi[0] = t.rmax; hi[1] = t.rmax; hi[2] = t.z;
+  if (t.dphi == 2. * kPi) return;
+  const double rin = 0.5 * (t.rmax + t.rmin);
+  auto out = [&](double x, double y) {
+    bool ci, co;
+    WedgeOps<double>::contains_inside<false>(t.wedge, x, y, ci, co);
+    return co;
+  };
+  const bool o0 = out(rin, 0.), o90 = out(0., rin), o180 = out(-rin, 0.), o270 = out(0., -rin);
+  if (!(o0 || o90 || o180 || o270)) return;
+  const double cx = t.rmax * std::cos(t.sphi), dx = t.rmax * std::cos(t.sphi + t.dphi);
+  const double cy = t.rmax * std::sin(t.sphi), dy = t.rmax * std::sin(t.sphi + t.dphi);
+  if (o0) hi[0] = vmax(cx, dx);
+  if (o90) hi[1] = vmax(cy, dy);
+  if (o180) lo[0] = vmin(cx, dx);
+  if (o270) lo[1] = vmin(cy, dy);
+  if (t.dphi >= kPi) return;
+  const double ax = t.rmin * std::cos(t.sphi), bx = t.rmin * std::cos(t.sphi + t.dphi);
+  const double ay = t.rmin * std::sin(t.sphi), by = t.rmin * std::sin(t.sphi + t.dphi);
+  double v = vmax(ax, bx);
+  hi[0] = v > hi[0] ? v : hi[0];
+  v = vmax(ay, by);
+  hi[1] = v > hi[1] ? v : hi[1];
+  v = vmin(ax, bx);
+  lo[0] = v < lo[0] ? v : lo[0];
+  v = vmin(ay, by);
+  lo[1] = v < lo[1] ? v : lo[1];
+}
+
+bool reference_extent(int type, const double *rec, double lo[3], double hi[3]) {
+  auto set = [&](double x0, double y0, double z0, double x1, double y1, double z1) {
+    lo[0] = x0; lo[1] = y0; lo[2] = z0;
+    hi[0] = x1; hi[1] = y1; hi[2] = z1;
+    return true;
+  };
+  switch (type) {
+    case VGB_SHAPE_BOX: {  // source/UnplacedBox.cpp:29-34
+      const BoxP &p = *reinterpret_cast<const BoxP *>(rec);
+      return set(-p.d[0], -p.d[1], -p.d[2], p.d[0], p.d[1], p.d[2]);
+    }
+    case VGB_SHAPE_TUBE:
+      tube_extent(*reinterpret_cast<const TubeP *>(rec), lo, hi);
+      return true;
+    case VGB_SHAPE_CONE: {  // volumes/UnplacedCone.h:324-328
+      const ConeP &p = *reinterpret_cast<const ConeP *>(rec);
+      const double m = p.rmax1 > p.rmax2 ? p.rmax1 : p.rmax2;
+      return set(-m, -m, -p.dz, m, m, p.dz);
+    }
+    case VGB_SHAPE_SPHERE: {  // source/UnplacedSphere.cpp:174-179
+      const SphereP &p = *reinterpret_cast<const SphereP *>(rec);
+      return set(-p.rmax, -p.rmax, -p.rmax, p.rmax, p.rmax, p.rmax);
+    }
+    case VGB_SHAPE_TORUS:  // volumes/UnplacedTorus.h:178-180: the bounding tube's
+      tube_extent(reinterpret_cast<const TorusP *>(rec)->btube, lo, hi);
+      return true;
+    case VGB_SHAPE_TRD: {
+      // volumes/UnplacedTrd.h:147-150; the upper x bound reads fDY1 where fDX1
+      // is meant, kept as the reference computes it
+      const TrdP &p = *reinterpret_cast<const TrdP *>(rec);
+      return set(-vmax(p.dx1, p.dx2), -vmax(p.dy1, p.dy2), -p.dz, vmax(p.dy1, p.dx2),
+                 vmax(p.dy1, p.dy2), p.dz);
+    }
+    case VGB_SHAPE_POLYCONE: {  // source/UnplacedPolycone.cpp:755-774
+      const PolyconeP &p = *reinterpret_cast<const PolyconeP *>(rec);
+      const PolySec *sec = reinterpret_cast<const PolySec *>(rec + p.sec_off);
+      const double *zs = rec + p.zs_off;
+      double m = 0.;
+      for (int i = 0; i < p.nsec; ++i) {
+        if (m < sec[i].cone.rmax1) m = sec[i].cone.rmax1;
+        if (m < sec[i].cone.rmax2) m = sec[i].cone.rmax2;
+      }
+      return set(-m, -m, zs[0], m, m, zs[p.nsec]);
+    }
+    case VGB_SHAPE_POLYHEDRON: {  // source/UnplacedPolyhedron.cpp:342-347
+      const PolyhedronP &p = *reinterpret_cast<const PolyhedronP *>(rec);
+      tube_extent(p.btube, lo, hi);
+      lo[2] += p.btube_offset;
+      hi[2] += p.btube_offset;
+      return true;
+    }
+    case VGB_SHAPE_BOOLEAN: {
+      // source/UnplacedBooleanVolume.cpp:94-121: a subtraction's extent is its
+      // left component's, in the component's own frame (the placement of the
+      // component is not applied)
+      const BooleanP &p = *reinterpret_cast<const BooleanP *>(rec);
+      return reference_extent(p.left.type, rec + p.left.rec_off, lo, hi);
+    }
+    default:
+      return false;
+  }
+}
+
 }  // namespace vgb
 
 extern "C" {

@@ -380,6 +380,43 @@ class SimpleNavigator:
         return out.value
 
 
+class ABBoxNavigator(SimpleNavigator):
+    """navigation/ABBoxNavigator.h over device batches: the step culls and
+    orders the daughters by ABBoxManager's aligned boxes; LocatePoint and the
+    safety are SimpleNavigator's (the reference's ABBoxNavigator uses them)."""
+
+    def FindNextBoundaryAndStep(self, points: SOA3D, dirs: SOA3D, cur: NavStatePool,
+                                nxt: NavStatePool, pstep, step, safety=None,
+                                stream=None) -> None:
+        g = self.geometry
+        for a in (pstep, step, safety):
+            _check_dtype(a, "f8")
+        check(g.L.vgb_abbox_nav_find_next_boundary_and_step(
+            g.handle, points.size(), _addr(points.x), _addr(points.y), _addr(points.z),
+            _addr(dirs.x), _addr(dirs.y), _addr(dirs.z), cur.handle, nxt.handle, _addr(pstep),
+            _addr(step), _addr(safety), _stream(stream)))
+
+    def Trace(self, points: SOA3D, dirs: SOA3D, pstep: float, max_steps: int, nsteps,
+              next_ids=None, steps=None, safeties=None, stream=None) -> None:
+        """Steps every track to the world exit (see vgb_abbox_nav_trace)."""
+        g = self.geometry
+        _check_dtype(nsteps, "i4")
+        _check_dtype(next_ids, "i4")
+        check(g.L.vgb_abbox_nav_trace(
+            g.handle, points.size(), _addr(points.x), _addr(points.y), _addr(points.z),
+            _addr(dirs.x), _addr(dirs.y), _addr(dirs.z), float(pstep), int(max_steps),
+            _addr(next_ids), _addr(steps), _addr(safeties), _addr(nsteps), _stream(stream)))
+
+
+def ComputeABBox(geometry: "Geometry", placed) -> np.ndarray:
+    """ABBoxManager::ComputeABBox: (lower xyz, upper xyz) of a placed volume's
+    aligned box in its mother's frame."""
+    out = np.zeros(6)
+    pid = placed.id if hasattr(placed, "id") else int(placed)
+    check(geometry.L.vgb_abbox_compute(geometry.handle, pid, out.ctypes.data))
+    return out
+
+
 # ---------------------------------------------------------------------------
 # baskets: many placed volumes in one persistent launch (vgb_basket_*)
 # ---------------------------------------------------------------------------

@@ -417,6 +417,9 @@ class VgbBuilder:
     def trd(self, dx1, dx2, dy1, dy2, dz):
         return self.g.UnplacedTrd(dx1, dx2, dy1, dy2, dz)
 
+    def shape(self, spec: ShapeSpec):
+        return build_unplaced(self.g, spec)
+
     def transform(self, tx=0., ty=0., tz=0., phi=0., theta=0., psi=0.):
         return self.g.Transformation3D(tx, ty, tz, phi, theta, psi)
 
@@ -468,6 +471,74 @@ def build_detector(b, spec: DetectorSpec | None = None) -> list:
     b.set_world(world)
     b.close()
     return placed
+
+
+def zoo_specs(exclude=()) -> list:
+    """The shapes of the mixed navigation geometry: the box, tube/cone/sphere,
+    torus/polycone/polyhedron/box-tube workloads and a trd, less the kinds in
+    `exclude`."""
+    specs = ([config1_box()] + list(config2_shapes().values()) + list(config3_shapes().values())
+             + [trd_spec(20., 10., 25., 15., 30.)])
+    return [s for s in specs if s.kind not in exclude]
+
+
+def build_zoo(b, specs: list, seed: int = SEED_BASE + 9) -> list:
+    """Mixed-shape navigation geometry: a world box (half 1000 mm) with a 3x3x3
+    grid of cells 600 mm apart.  Cell c holds specs[c % len(specs)] placed with
+    a random Euler rotation (degrees) and an offset of up to 20 mm; every third
+    cell instead holds a box container (half 160 mm, its own rotation) with the
+    shape inside it (offset up to 5 mm) and a small trd in a corner, so paths
+    are up to three levels deep.  Every shape reaches less than 135 mm from its
+    centre, so nothing overlaps.  Returns the placed volumes in creation (= id)
+    order."""
+    rng = np.random.default_rng(seed)
+    placed = []
+    world_lv = b.logical("world", b.box(1000., 1000., 1000.))
+    world = b.place(world_lv, b.transform())
+    placed.append(world)
+    lvs = [b.logical(f"zoo{k}", b.shape(sp)) for k, sp in enumerate(specs)]
+    small_lv = b.logical("zoo_trd", b.trd(6., 4., 8., 5., 10.))
+    box_u = b.box(160., 160., 160.)
+
+    def rot():
+        return tuple(float(a) for a in rng.uniform(0., 360., 3))
+
+    c = 0
+    for i in (-600., 0., 600.):
+        for j in (-600., 0., 600.):
+            for k in (-600., 0., 600.):
+                off = rng.uniform(-20., 20., 3)
+                lv = lvs[c % len(lvs)]
+                if c % 3 == 2:
+                    cont = b.logical(f"cont{c}", box_u)
+                    placed.append(b.place_daughter(cont, lv, b.transform(*(off / 4.), *rot())))
+                    placed.append(b.place_daughter(cont, small_lv,
+                                                   b.transform(140., 140., -140., *rot())))
+                    placed.append(b.place_daughter(world_lv, cont,
+                                                   b.transform(i, j, k, *rot())))
+                else:
+                    placed.append(b.place_daughter(world_lv, lv,
+                                                   b.transform(i + off[0], j + off[1], k + off[2],
+                                                               *rot())))
+                c += 1
+    b.set_world(world)
+    b.close()
+    return placed
+
+
+def zoo_tracks(n: int, seed: int):
+    """n tracks: a third from near the cell centres (inside or near the shapes),
+    the rest from uniform points of the world's inner 900 mm; isotropic
+    directions."""
+    rng = np.random.default_rng(seed)
+    n0 = n // 3
+    cells = np.array([(i, j, k) for i in (-600., 0., 600.) for j in (-600., 0., 600.)
+                      for k in (-600., 0., 600.)])
+    pick = cells[rng.integers(0, len(cells), n0)] + rng.uniform(-30., 30., (n0, 3))
+    rest = rng.uniform(-900., 900., (n - n0, 3))
+    p = np.concatenate([pick, rest])
+    d = isotropic(rng, n)
+    return tuple(np.ascontiguousarray(p[:, a]) for a in range(3)), d
 
 
 def isotropic_tracks(n: int, seed: int):
