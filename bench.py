@@ -363,13 +363,42 @@ def run_baskets(args):
 # served navigation: continuous batching of Poisson-arriving track baskets
 # ---------------------------------------------------------------------------
 
+def nav_cpu_baseline(pts, dirs, max_steps, n_simple=16384, n_abbox=4096):
+    """The reference's navigators on the host cores over the first tracks of
+    the trace workload (oracle/_ref, the reference built from its sources):
+    SimpleNavigator on every core (one navigator and state pair per thread),
+    ABBoxNavigator on one (its ABBoxManager shares one hit list)."""
+    import oracle
+    from vecgeom_b200 import workloads as W
+    if not oracle.RefLib.available():
+        return None
+    ref = oracle.RefLib()
+    W.build_detector(oracle.RefBuilder(ref))
+    threads = os.cpu_count() or 1
+    sub = lambda a, k: tuple(np.ascontiguousarray(v[:k]) for v in a)  # noqa: E731
+    t0 = time.perf_counter()
+    _, _, _, nst = oracle.ref_nav_trace(ref, sub(pts, n_simple), sub(dirs, n_simple), 1e30,
+                                        max_steps, threads)
+    simple = float(nst.sum()) / (time.perf_counter() - t0)
+    t0 = time.perf_counter()
+    _, _, _, nst_ab = oracle.ref_abbox_nav_trace(ref, sub(pts, n_abbox), sub(dirs, n_abbox), 1e30,
+                                                 max_steps)
+    abbox = float(nst_ab.sum()) / (time.perf_counter() - t0)
+    return {"value": round(simple, 1), "unit": "steps/s", "cores": threads, "kind": "reference",
+            "sample": f"first {n_simple} trace tracks, SimpleNavigator, {threads} threads",
+            "abbox_single_thread": {"value": round(abbox, 1), "unit": "steps/s",
+                                    "sample": f"first {n_abbox} trace tracks, ABBoxNavigator, "
+                                              "1 thread"}}
+
+
 def run_nav(args):
     """Layered detector (14,011 placed volumes).  Requests of 1-16384 tracks
     (log-uniform sizes) from the origin, isotropic, arrive as a Poisson stream
     at ~80% of the measured saturated throughput; each track steps (safety +
     FindNextBoundaryAndStep) until it leaves the world or 64 steps.  The served
     run uses --precision; the other form is served with the same arrivals for
-    comparison, and the raw trace throughput of both forms is reported."""
+    comparison, and the raw trace throughput of both forms and of
+    ABBoxNavigator is reported."""
     import torch
     import vecgeom_b200 as V
     from vecgeom_b200 import workloads as W
@@ -449,16 +478,23 @@ def run_nav(args):
     P, D = V.SOA3D(*(dev(a) for a in pts)), V.SOA3D(*(dev(a) for a in dirs))
     nst = torch.zeros(n, dtype=torch.int32, device="cuda")
     nav = V.SimpleNavigator(g)
+    abnav = V.ABBoxNavigator(g)
     trace = {}
-    for name, pr in (("fp64", V.PREC_FP64), ("fp32r", V.PREC_FP32_REFINE)):
+    for name, pr in (("fp64", V.PREC_FP64), ("fp32r", V.PREC_FP32_REFINE), ("abbox", None)):
+        def run():
+            if pr is None:
+                abnav.Trace(P, D, 1e30, max_steps, nst)
+            else:
+                nav.Trace(P, D, 1e30, max_steps, nst, precision=pr)
         for _ in range(2):
-            nav.Trace(P, D, 1e30, max_steps, nst, precision=pr)
+            run()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        nav.Trace(P, D, 1e30, max_steps, nst, precision=pr)
+        run()
         e1.record()
         torch.cuda.synchronize()
         trace[name] = round(int(nst.sum()) / (e0.elapsed_time(e1) * 1e-3), 1)
+    cpu = nav_cpu_baseline(pts, dirs, max_steps)
     tag = "fp64" if prec_main == V.PREC_FP64 else "fp32+refine"
     line = {"metric": f"nav steps/s ({tag}, served) with p50/p99 request latency",
             "value": round(steps / wall, 1), "unit": "steps/s", "n_gpus": 1,
@@ -480,6 +516,7 @@ def run_nav(args):
             "other_precision": {"precision": "fp32+refine" if other else "fp64",
                                 "steps_per_s": round(o_steps / o_wall, 1), "latency_ms": o_lat},
             "trace_steps_per_s": trace,
+            "cpu_baseline": cpu,
             "e2e": {"value": round(steps / wall, 1), "unit": "steps/s",
                     "h2d_bytes_per_step": int(48 * sizes.sum() / nreq),
                     "d2h_bytes_per_step": int(36 * sizes.sum() / nreq)},

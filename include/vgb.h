@@ -346,6 +346,22 @@ vgb_status vgb_nav_find_next_boundary_and_step(const vgb_geometry *g, int64_t n,
                                                double *step, double *safety, int32_t precision,
                                                void *stream);
 
+/* The basket form of SimpleNavigator::FindNextBoundaryAndStep
+ * (navigation/SimpleNavigator.h:637-743) with GetSafeties (:599-632): per track
+ * the current volume's DistanceToOut with its node index, every daughter's
+ * DistanceToInMinimize (volumes/ShapeImplementationHelper.h:637-658) and the
+ * relocation pushed 1e-9 past the boundary.  distance[i] is the step (pstep[i]
+ * when the geometry is further), nextnode[i] the reference's next-node
+ * workspace entry (daughter position, -1 leaving, -2 staying; may be NULL) and
+ * safety[i] GetSafeties' value (may be NULL).  The reference takes the
+ * volume of a basket's first track for all of its tracks; here every track
+ * uses its own state, which is the same for a basket of one volume. */
+vgb_status vgb_nav_find_next_boundary_and_step_basket(
+    const vgb_geometry *g, int64_t n, const double *x, const double *y, const double *z,
+    const double *dx, const double *dy, const double *dz, const vgb_navpool *cur,
+    vgb_navpool *next, const double *pstep, double *distance, double *safety, int32_t *nextnode,
+    void *stream);
+
 /* Transport of n straight tracks from their start points to the world exit:
  * LocatePoint from the world, then per step GetSafety, FindNextBoundaryAndStep
  * and point += direction * step, until the state is outside or max_steps steps

@@ -135,6 +135,8 @@ class RefLib:
         L.vgref_placed_id.argtypes = [_vp]
         L.vgref_nav_trace.restype = _i
         L.vgref_nav_trace.argtypes = [_i64] + [_vp] * 6 + [_d, _i] + [_vp] * 4 + [_i]
+        L.vgref_nav_basket_step.restype = _i
+        L.vgref_nav_basket_step.argtypes = [_i64] + [_vp] * 7 + [_i] + [_vp] * 8
         L.vgref_abbox_compute.restype = None
         L.vgref_abbox_compute.argtypes = [_vp, _vp]
         L.vgref_abbox_nav_trace.restype = _i
@@ -265,6 +267,22 @@ def ref_abbox_nav_trace(ref: RefLib, pts, dirs, pstep: float, max_steps: int):
     ref.L.vgref_abbox_nav_trace(n, _p(x), _p(y), _p(z), _p(dx), _p(dy), _p(dz), pstep, max_steps,
                                 _p(ids), _p(steps), _p(saf), _p(nst))
     return ids, steps, saf, nst
+
+
+def ref_nav_basket_step(ref: RefLib, pts, dirs, pstep, prior: int) -> dict:
+    """SimpleNavigator's basket step over the current reference world (see
+    ref_driver.cpp vgref_nav_basket_step): start points after `prior` single
+    steps, then per track distance, safety, next node, new top id, boundary."""
+    x, y, z = (np.ascontiguousarray(a, np.float64) for a in pts)
+    dx, dy, dz = (np.ascontiguousarray(a, np.float64) for a in dirs)
+    ps = np.ascontiguousarray(pstep, np.float64)
+    n = len(x)
+    out = {k: np.zeros(n) for k in ("px", "py", "pz", "distance", "safety")}
+    out.update({k: np.zeros(n, np.int32) for k in ("nextnode", "newtop", "boundary")})
+    ref.L.vgref_nav_basket_step(n, _p(x), _p(y), _p(z), _p(dx), _p(dy), _p(dz), _p(ps), prior,
+                                *(_p(out[k]) for k in ("px", "py", "pz", "distance", "safety",
+                                                       "nextnode", "newtop", "boundary")))
+    return out
 
 
 def ref_abbox(ref: RefLib, placed) -> np.ndarray:

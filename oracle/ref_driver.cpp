@@ -33,6 +33,8 @@
 #include <algorithm>
 #include <cstdint>
 #include <cstring>
+#include <limits>
+#include <map>
 #include <thread>
 #include <vector>
 
@@ -282,6 +284,86 @@ int vgref_nav_trace(int64_t ntracks, const double *x, const double *y, const dou
     pool.emplace_back(work, b, e);
   }
   for (auto &th : pool) th.join();
+  return 0;
+}
+
+// Basket navigation (navigation/SimpleNavigator.h:599-743).  Every track is
+// located from the world and moved by `prior` scalar steps (GetSafety is not
+// needed for that; FindNextBoundaryAndStep and p += d * step, as the trace
+// does); the tracks that are then inside are grouped into baskets by Top()
+// volume, in track order, and each basket takes one basket
+// FindNextBoundaryAndStep (SOA3D containers) and one GetSafeties.  Per track:
+// distance, safety, next-node workspace entry, the new state's Top() id (-1
+// outside) and boundary flag; tracks outside before the basket step get -7 ids
+// and NaN values.  The points the basket step starts from are written to
+// px/py/pz.
+int vgref_nav_basket_step(int64_t n, const double *x, const double *y, const double *z,
+                          const double *dx, const double *dy, const double *dz,
+                          const double *pstep, int prior, double *px, double *py, double *pz,
+                          double *dist, double *safety, int *nextnode, int *newtop,
+                          int *boundary) {
+  const int depth = GeoManager::Instance().getMaxDepth();
+  VPlacedVolume const *world = GeoManager::Instance().GetWorld();
+  SimpleNavigator nav;
+  std::vector<NavigationState *> cur((size_t)n), nxt((size_t)n);
+  NavigationState *tmp = NavigationState::MakeInstance(depth);
+  for (int64_t i = 0; i < n; ++i) {
+    cur[i] = NavigationState::MakeInstance(depth);
+    nxt[i] = NavigationState::MakeInstance(depth);
+    Vector3D<Precision> p(x[i], y[i], z[i]);
+    Vector3D<Precision> d(dx[i], dy[i], dz[i]);
+    nav.LocatePoint(world, p, *cur[i], true);
+    for (int k = 0; k < prior && !cur[i]->IsOutside(); ++k) {
+      double step = 0;
+      tmp->Clear();
+      nav.FindNextBoundaryAndStep(p, d, *cur[i], *tmp, 1e30, step);
+      p = p + d * step;
+      tmp->CopyTo(cur[i]);
+    }
+    px[i] = p.x();
+    py[i] = p.y();
+    pz[i] = p.z();
+    dist[i] = safety[i] = std::numeric_limits<double>::quiet_NaN();
+    nextnode[i] = newtop[i] = boundary[i] = -7;
+  }
+  std::map<VPlacedVolume const *, std::vector<int64_t>> baskets;
+  for (int64_t i = 0; i < n; ++i)
+    if (!cur[i]->IsOutside()) baskets[cur[i]->Top()].push_back(i);
+  for (auto &kv : baskets) {
+    const std::vector<int64_t> &ix = kv.second;
+    const size_t m = ix.size();
+    SOA3D<Precision> gp(m), gd(m), lp(m), ld(m);
+    std::vector<NavigationState *> cs(m), ns(m);
+    // the basket step leaves a distance untouched where a shape kernel does not
+    // write it; start from kInfinity as the batch calls here do
+    std::vector<double> ps(m), ds(m, kInfinity), sf(m);
+    std::vector<int> nn(m);
+    for (size_t k = 0; k < m; ++k) {
+      const int64_t i = ix[k];
+      gp.set(k, px[i], py[i], pz[i]);
+      gd.set(k, dx[i], dy[i], dz[i]);
+      cs[k] = cur[i];
+      ns[k] = nxt[i];
+      ps[k] = pstep[i];
+    }
+    nav.FindNextBoundaryAndStep(gp, gd, lp, ld, cs.data(), ns.data(), ps.data(), sf.data(),
+                                ds.data(), nn.data());
+    SOA3D<Precision> work(m);
+    nav.GetSafeties(gp, cs.data(), work, sf.data());
+    for (size_t k = 0; k < m; ++k) {
+      const int64_t i = ix[k];
+      dist[i] = ds[k];
+      safety[i] = sf[k];
+      nextnode[i] = nn[k];
+      newtop[i] = ns[k]->IsOutside() ? -1 : ns[k]->Top()->id();
+      boundary[i] = ns[k]->IsOnBoundary() ? 1 : 0;
+    }
+  }
+  for (int64_t i = 0; i < n; ++i) {
+    NavigationState::ReleaseInstance(cur[i]);
+    NavigationState::ReleaseInstance(nxt[i]);
+  }
+  NavigationState::ReleaseInstance(tmp);
   return 0;
 }
 

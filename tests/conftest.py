@@ -4,7 +4,8 @@ import sys
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-for p in (ROOT, os.path.dirname(os.path.abspath(__file__))):
+HERE = os.path.dirname(os.path.abspath(__file__))
+for p in (ROOT, HERE, os.path.join(HERE, "golden")):
     if p not in sys.path:
         sys.path.insert(0, p)
 

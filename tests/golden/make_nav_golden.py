@@ -11,6 +11,8 @@ per step (oracle/ref_driver.cpp vgref_nav_trace / vgref_abbox_nav_trace).
     zoo.npz             mixed-shape geometry without the sphere and the torus,
                         SimpleNavigator
     zoo_abbox.npz       the same without the polyhedron too, ABBoxNavigator
+    basket.npz          layered detector, SimpleNavigator's basket step and
+                        GetSafeties after 0-3 single steps
     row_abbox.npz       300 boxes on a line, ABBoxNavigator (hit lists longer
                         than the GPU kernel's shared list)
     zoo_boxes.npz       ABBoxManager::ComputeABBox of every placed volume of the
@@ -139,6 +141,44 @@ def reference_boxes(ref, geometry: str) -> np.ndarray:
     return np.array([oracle.ref_abbox(ref, p) for p in placed])
 
 
+def basket_inputs(n: int = 512):
+    """Points spread over the detector with isotropic directions; half the
+    tracks propose a physical step U(0, 50) mm, the rest 1e30."""
+    rng = np.random.default_rng(SEED + 6)
+    pts = (rng.uniform(-1100., 1100., n), rng.uniform(-1100., 1100., n),
+           rng.uniform(-1300., 1300., n))
+    _, dirs = W.isotropic_tracks(n, SEED + 7)
+    pstep = np.where(np.arange(n) % 2 == 0, rng.uniform(0., 50., n), 1e30)
+    return pts, dirs, pstep
+
+
+BASKET_PRIORS = (0, 1, 2, 3)
+
+
+def reference_basket(ref, pts, dirs, pstep, priors=BASKET_PRIORS, geometry="detector"):
+    """The reference's basket step after each number of prior steps; new top
+    ids mapped to list positions."""
+    rb = oracle.RefBuilder(ref)
+    placed = build_geometry(rb, geometry)
+    to_ours = {int(r): k for k, r in enumerate(rb.ids(placed))}
+    out = {}
+    for prior in priors:
+        r = oracle.ref_nav_basket_step(ref, pts, dirs, pstep, prior)
+        r["newtop"] = np.array([to_ours[int(i)] if i >= 0 else int(i) for i in r["newtop"]],
+                               np.int32)
+        for k, v in r.items():
+            out[f"{k}_{prior}"] = v
+    return out
+
+
+def _basket(pts, dirs, pstep, priors, geometry):
+    return reference_basket(oracle.RefLib(), pts, dirs, pstep, priors, geometry)
+
+
+def reference_basket_isolated(pts, dirs, pstep, priors=BASKET_PRIORS, geometry="detector"):
+    return isolated(_basket, pts, dirs, pstep, priors, geometry)
+
+
 def _traced(pts, dirs, max_steps, nthreads, geometry, navigator):
     return reference_trace(oracle.RefLib(), pts, dirs, max_steps, nthreads, geometry, navigator)
 
@@ -181,6 +221,12 @@ def main() -> None:
                             steps=steps, safeties=saf, nsteps=nst, geometry=geometry,
                             navigator=navigator)
         print("wrote", os.path.relpath(path, ROOT), "mean steps", float(nst.mean()))
+    pts, dirs, pstep = basket_inputs()
+    rec = reference_basket_isolated(pts, dirs, pstep)
+    path = os.path.join(out, "basket.npz")
+    np.savez_compressed(path, x=pts[0], y=pts[1], z=pts[2], dx=dirs[0], dy=dirs[1], dz=dirs[2],
+                        pstep=pstep, priors=np.array(BASKET_PRIORS), **rec)
+    print("wrote", os.path.relpath(path, ROOT))
     boxes = reference_boxes_isolated("zoo_all")
     path = os.path.join(out, "zoo_boxes.npz")
     np.savez_compressed(path, boxes=boxes)

@@ -80,7 +80,7 @@ extern "C" int hc_nav_trace(vgb_geometry *g, int64_t n, const double *x, const d
   if (prepare_tables(g) != VGB_OK) return -1;
   const NavGeom G = {g->params.data(),    g->unplaced.data(), g->placed.data(),
                      g->xforms.data(),    g->nav_raw.data(),  g->logicals.data(),
-                     g->daughters.data(), g->pl_box.data(),   g->ab_box.data(), g->world,
+                     g->daughters.data(), g->pl_box.data(),   g->ab_box.data(), g->ab_slot.data(), g->world,
                      g->max_depth};
   if (screen) return trace_host<Navigator<OneLane, kNavMaskAll, true>>(G, n, x, y, z, dx, dy, dz, pstep,
                                                                        max_steps, next_ids, steps,
@@ -132,7 +132,7 @@ extern "C" int hc_abbox_trace(vgb_geometry *g, int64_t n, const double *x, const
   if (prepare_tables(g) != VGB_OK || cap < 1) return -1;
   const NavGeom G = {g->params.data(),    g->unplaced.data(), g->placed.data(),
                      g->xforms.data(),    g->nav_raw.data(),  g->logicals.data(),
-                     g->daughters.data(), g->pl_box.data(),   g->ab_box.data(), g->world,
+                     g->daughters.data(), g->pl_box.data(),   g->ab_box.data(), g->ab_slot.data(), g->world,
                      g->max_depth};
   using Nav = ABBoxNavigator<OneLane, kNavMaskAll>;
   std::vector<AbCand> buf((size_t)cap + kAbSortThreshold);
@@ -180,6 +180,52 @@ extern "C" int hc_abbox_sort_check(const float *b, int32_t n, int32_t *ours, int
   for (int i = 0; i < n; ++i) {
     ours[i] = a[i].d;
     std_order[i] = h[i].first;
+  }
+  return 0;
+}
+
+// The basket step (Navigator::step_basket) with one lane, after `prior`
+// single-track steps from the located start point (the same sequence as the
+// reference driver's vgref_nav_basket_step); outputs per track as there.
+extern "C" int hc_nav_basket(vgb_geometry *g, int64_t n, const double *x, const double *y,
+                             const double *z, const double *dx, const double *dy,
+                             const double *dz, const double *pstep, int32_t prior, double *px,
+                             double *py, double *pz, double *dist, double *safety,
+                             int32_t *nextnode, int32_t *newtop, int32_t *boundary) {
+  if (prepare_tables(g) != VGB_OK) return -1;
+  const NavGeom G = {g->params.data(),    g->unplaced.data(), g->placed.data(),
+                     g->xforms.data(),    g->nav_raw.data(),  g->logicals.data(),
+                     g->daughters.data(), g->pl_box.data(),   g->ab_box.data(), g->ab_slot.data(),
+                     g->world,            g->max_depth};
+  using Nav = Navigator<OneLane, kNavMaskAll>;
+  for (int64_t i = 0; i < n; ++i) {
+    V3<double> p = {x[i], y[i], z[i]};
+    const V3<double> d = {dx[i], dy[i], dz[i]};
+    NavPath cur, nxt;
+    if (!Nav::locate_from_world(G, cur, p)) return -2;
+    for (int k = 0; k < prior && cur.level > 0; ++k) {
+      const DXform m = nav_top_matrix(G, cur);
+      double st = 0.;
+      if (!Nav::step(G, cur, nxt, xf_point(m, p), xf_dir(m, d), 1e30, st)) return -2;
+      p = {p.x + d.x * st, p.y + d.y * st, p.z + d.z * st};
+      cur = nxt;
+    }
+    px[i] = p.x;
+    py[i] = p.y;
+    pz[i] = p.z;
+    dist[i] = safety[i] = Lim<double>::quiet_nan();
+    nextnode[i] = newtop[i] = boundary[i] = -7;
+    if (cur.level == 0) continue;
+    const DXform m = nav_top_matrix(G, cur);
+    const V3<double> lp = xf_point(m, p), ld = xf_dir(m, d);
+    safety[i] = Nav::safety(G, cur, lp);
+    double st = 0.;
+    int32_t node = 0;
+    if (!Nav::step_basket(G, cur, nxt, lp, ld, pstep[i], st, node)) return -2;
+    dist[i] = st;
+    nextnode[i] = node;
+    newtop[i] = nxt.top();
+    boundary[i] = nxt.boundary ? 1 : 0;
   }
   return 0;
 }

@@ -34,6 +34,8 @@ def load_hostcheck():
             f.restype = res
             f.argtypes = args
     vp = ctypes.c_void_p
+    L.hc_nav_basket.restype = ctypes.c_int
+    L.hc_nav_basket.argtypes = [vp, ctypes.c_int64] + [vp] * 7 + [ctypes.c_int32] + [vp] * 8
     for fn in ("hc_nav_trace", "hc_abbox_trace"):
         getattr(L, fn).restype = ctypes.c_int
         getattr(L, fn).argtypes = ([vp, ctypes.c_int64] + [vp] * 6 + [ctypes.c_double,
@@ -120,3 +122,32 @@ def assert_traces_equal(got, want, max_steps, what=""):
         same = (a == b) | (np.isnan(a) & np.isnan(b)) if a.dtype.kind == "f" else a == b
         k = np.flatnonzero(~same)
         assert len(k) == 0, f"{what}: {name} differ at {len(k)} records, first {k[:5].tolist()}"
+
+
+BASKET_KEYS = ("px", "py", "pz", "distance", "safety", "nextnode", "newtop", "boundary")
+
+
+def host_basket(L, geometry: str, pts, dirs, pstep, prior: int) -> dict:
+    """hc_nav_basket: the basket step after `prior` single steps (host build)."""
+    g, placed = build(L, geometry, close=False)
+    n = len(pts[0])
+    out = {k: np.zeros(n) for k in BASKET_KEYS[:5]}
+    out.update({k: np.zeros(n, np.int32) for k in BASKET_KEYS[5:]})
+    a = lambda v: np.ascontiguousarray(v).ctypes.data  # noqa: E731
+    rc = L.hc_nav_basket(g.handle, n, *(a(v) for v in pts), *(a(v) for v in dirs),
+                         a(np.ascontiguousarray(pstep, np.float64)), prior,
+                         *(a(out[k]) for k in BASKET_KEYS))
+    assert rc == 0
+    pos = {int(p.id): k for k, p in enumerate(placed)}
+    out["newtop"] = np.array([pos[int(i)] if i >= 0 else int(i) for i in out["newtop"]],
+                             np.int32)
+    return out
+
+
+def assert_basket_equal(got: dict, want: dict, what=""):
+    """Every field bit for bit (NaN marks tracks outside before the step)."""
+    for k in BASKET_KEYS:
+        a, b = np.asarray(got[k]), np.asarray(want[k])
+        same = (a == b) | (np.isnan(a) & np.isnan(b)) if a.dtype.kind == "f" else a == b
+        bad = np.flatnonzero(~same)
+        assert len(bad) == 0, f"{what}: {k} differs for tracks {bad[:6].tolist()}"

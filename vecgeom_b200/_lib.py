@@ -110,6 +110,7 @@ SIGNATURES = {
     "vgb_nav_find_next_boundary_and_step": (ctypes.c_int, [_vp, _i64] + [_vp] * 11 + [_i32, _vp]),
     "vgb_nav_trace": (ctypes.c_int, [_vp, _i64] + [_vp] * 6 + [_dbl, _i32] + [_vp] * 4
                       + [_i32, _vp]),
+    "vgb_nav_find_next_boundary_and_step_basket": (ctypes.c_int, [_vp, _i64] + [_vp] * 13),
     "vgb_abbox_nav_find_next_boundary_and_step": (ctypes.c_int, [_vp, _i64] + [_vp] * 12),
     "vgb_abbox_nav_trace": (ctypes.c_int, [_vp, _i64] + [_vp] * 6 + [_dbl, _i32] + [_vp] * 5),
     "vgb_abbox_compute": (ctypes.c_int, [_vp, _i32, _vp]),

@@ -158,7 +158,7 @@ VGB_HD void ab_insert(AbCand *a, int lo, int i, bool guarded) {
 
 constexpr int kAbSortThreshold = 16;
 
-VGB_HD void ab_sort_like_libstdcxx(AbCand *a, int n) {
+VGB_HD_NOINLINE void ab_sort_like_libstdcxx(AbCand *a, int n) {
   if (n < 2 || n >= (1 << 16)) return;
   int lg = 0;
   while ((n >> (lg + 1)) != 0) ++lg;
@@ -216,20 +216,25 @@ VGB_HD AbRay ab_ray(const V3<double> &p, const V3<double> &d) {
 
 // BoxImplementation::IntersectCachedKernel2<kScalarFloat, float>
 // (volumes/kernel/BoxImplementation.h:337-384) with t0 = 0 and t1 = +inf on a
-// box stored as lower (0..2) and upper (3..5) corner: the entry distance, or
+// box stored as lower and upper corner (two float4): the entry distance, or
 // +inf when the ray misses.
-VGB_HD float ab_intersect(const float *box, const AbRay &r) {
+VGB_HD float ab_intersect(const float4 *box, const AbRay &r) {
   const float inf = Lim<float>::inf();
-  float tmin = (box[3 * r.sign[0]] - r.p[0]) * r.inv[0];
-  float tymax = (box[3 * (1 - r.sign[1]) + 1] - r.p[1]) * r.inv[1];
+  const float4 lo = box[0], hi = box[1];
+  // corners[sign] and corners[1 - sign] of the reference, per axis
+  const float xn = r.sign[0] ? hi.x : lo.x, xf = r.sign[0] ? lo.x : hi.x;
+  const float yn = r.sign[1] ? hi.y : lo.y, yf = r.sign[1] ? lo.y : hi.y;
+  const float zn = r.sign[2] ? hi.z : lo.z, zf = r.sign[2] ? lo.z : hi.z;
+  float tmin = (xn - r.p[0]) * r.inv[0];
+  float tymax = (yf - r.p[1]) * r.inv[1];
   if (tmin > tymax) return inf;
-  float tmax = (box[3 * (1 - r.sign[0])] - r.p[0]) * r.inv[0];
-  const float tymin = (box[3 * r.sign[1] + 1] - r.p[1]) * r.inv[1];
+  float tmax = (xf - r.p[0]) * r.inv[0];
+  const float tymin = (yn - r.p[1]) * r.inv[1];
   if (tymin > tmax) return inf;
   tmin = vmax(tmin, tymin);
   tmax = vmin(tmax, tymax);
-  const float tzmin = (box[3 * r.sign[2] + 2] - r.p[2]) * r.inv[2];
-  const float tzmax = (box[3 * (1 - r.sign[2]) + 2] - r.p[2]) * r.inv[2];
+  const float tzmin = (zn - r.p[2]) * r.inv[2];
+  const float tzmax = (zf - r.p[2]) * r.inv[2];
   if ((tmin > tzmax) || (tzmin > tmax)) return inf;
   tmin = vmax(tmin, tzmin);
   tmax = vmin(tmax, tzmax);
@@ -250,8 +255,9 @@ template <class L, uint32_t kMask> struct ABBoxNavigator {
 
   // Steps 2 and 3 above: updates step (entering with the mother's) and hit
   // (the daughter position, -1 for the mother).  buf holds cap + 16 entries.
-  static VGB_HD void walk(const NavGeom &G, const int32_t *dl, int nd, const V3<R> &lp,
-                          const V3<R> &ld, R &step, int &hit, AbCand *buf, int cap) {
+  static VGB_HD void walk(const NavGeom &G, const int32_t *dl, const float4 *boxes, int nd,
+                          const V3<R> &lp, const V3<R> &ld, R &step, int &hit, AbCand *buf,
+                          int cap) {
     const AbRay ray = ab_ray(lp, ld);
     const float finf = Lim<float>::inf();
     L::sync();
@@ -259,7 +265,7 @@ template <class L, uint32_t kMask> struct ABBoxNavigator {
     for (int base = 0; base < nd; base += L::N) {
       const int d = base + L::lane();
       float b = finf;
-      if (d < nd) b = ab_intersect(G.ab_box + 6 * (int64_t)dl[d], ray);
+      if (d < nd) b = ab_intersect(boxes + 2 * d, ray);
       const bool keep = b < finf;
       const uint32_t bal = L::ballot(keep);
       if (keep) {
@@ -270,7 +276,7 @@ template <class L, uint32_t kMask> struct ABBoxNavigator {
     }
     if (m == 0) return;
     if (m > cap) {
-      walk_one_by_one(G, dl, nd, lp, ld, ray, step, hit);
+      walk_one_by_one(G, dl, boxes, nd, lp, ld, ray, step, hit);
       return;
     }
     L::sync();
@@ -343,8 +349,10 @@ template <class L, uint32_t kMask> struct ABBoxNavigator {
 
   // The same walk for lists longer than the buffer: the next candidate is the
   // smallest (b, index) above the last one among the hits the step can reach.
-  static VGB_HD void walk_one_by_one(const NavGeom &G, const int32_t *dl, int nd, const V3<R> &lp,
-                                     const V3<R> &ld, const AbRay &ray, R &step, int &hit) {
+  static VGB_HD_NOINLINE void walk_one_by_one(const NavGeom &G, const int32_t *dl,
+                                              const float4 *boxes, int nd, const V3<R> &lp,
+                                              const V3<R> &ld, const AbRay &ray, R &step,
+                                              int &hit) {
     const float finf = Lim<float>::inf();
     R t = step;
     int h = hit;
@@ -352,7 +360,7 @@ template <class L, uint32_t kMask> struct ABBoxNavigator {
     for (;;) {
       AbCand best = {finf, 0x7fffffff};
       for (int d = L::lane(); d < nd; d += L::N) {
-        const float b = ab_intersect(G.ab_box + 6 * (int64_t)dl[d], ray);
+        const float b = ab_intersect(boxes + 2 * d, ray);
         if (!(b < finf) || t < (R)b) continue;
         const AbCand c = {b, d};
         if (ab_less(last, c) && ab_less(c, best)) best = c;
@@ -393,7 +401,7 @@ template <class L, uint32_t kMask> struct ABBoxNavigator {
     const int32_t nd = lr.dcount;
     const int32_t *dl = G.daughters + lr.dfirst;
     int hit = -1;
-    if (nd > 0) walk(G, dl, nd, lp, ld, step, hit, buf, cap);
+    if (nd > 0) walk(G, dl, G.ab_slot + 2 * (int64_t)lr.dfirst, nd, lp, ld, step, hit, buf, cap);
 
     next = cur;
     if (step > pstep) {

@@ -163,6 +163,7 @@ vgb_status vgb_geometry_destroy(vgb_geometry *g) {
     cudaFree(g->dev.nav_flags);
     cudaFree(g->dev.pl_box);
     cudaFree(g->dev.ab_box);
+    cudaFree(g->dev.ab_slot);
     cudaFree(g->dev.placed);
     cudaFree(g->dev.logicals);
     cudaFree(g->dev.daughters);
@@ -395,6 +396,13 @@ vgb_status vgb::prepare_tables(vgb_geometry *g) {
     }
     for (int k = 0; k < 6; ++k) g->ab_box[6 * pv + k] = (float)g->ab_box_d[6 * pv + k];
   }
+  // the navigator reads the boxes of a volume's daughters in daughter order
+  g->ab_slot.assign(2 * g->daughters.size(), float4{0.f, 0.f, 0.f, 0.f});
+  for (size_t k = 0; k < g->daughters.size(); ++k) {
+    const float *b = &g->ab_box[6 * (size_t)g->daughters[k]];
+    g->ab_slot[2 * k] = float4{b[0], b[1], b[2], 0.f};
+    g->ab_slot[2 * k + 1] = float4{b[3], b[4], b[5], 0.f};
+  }
   return VGB_OK;
 }
 
@@ -434,6 +442,7 @@ vgb_status vgb_geometry_close(vgb_geometry *g) {
   }
   if ((s = upload(g->pl_box, &g->dev.pl_box, &g->dev.bytes)) != VGB_OK) return s;
   if ((s = upload(g->ab_box, &g->dev.ab_box, &g->dev.bytes)) != VGB_OK) return s;
+  if ((s = upload(g->ab_slot, &g->dev.ab_slot, &g->dev.bytes)) != VGB_OK) return s;
   g->closed = true;
   return VGB_OK;
 }

@@ -73,6 +73,7 @@ struct DeviceImage {
   uint32_t *nav_flags = nullptr;  // navigation error bits (VGB_NAV_ERR_*)
   float *pl_box = nullptr;        // per placed: enclosing box in the mother's frame
   float *ab_box = nullptr;        // per placed: ABBoxManager's aligned box (float), mother frame
+  float4 *ab_slot = nullptr;      // per daughter slot (CSR order): the same box as 2 float4
   int64_t bytes = 0;
 };
 
@@ -93,6 +94,7 @@ struct vgb_geometry {
   std::vector<float> pl_box;           // per placed: 6 floats, enclosing box (mother frame)
   std::vector<double> ab_box_d;        // per placed: ABBoxManager::ComputeABBox (lower, upper)
   std::vector<float> ab_box;           // the same boxes rounded to float, as navigated
+  std::vector<float4> ab_slot;         // per daughter slot: (lower, 0), (upper, 0)
   uint32_t type_mask = 0;              // bit t set when a shape of type t exists
   int32_t world = -1;
   int32_t max_depth = 0;

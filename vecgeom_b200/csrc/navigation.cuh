@@ -36,6 +36,7 @@ struct NavGeom {
   const int32_t *daughters;     // CSR over logicals
   const float *pl_box;          // per placed: enclosing box in the mother's frame (6 floats)
   const float *ab_box;          // per placed: ABBoxManager's aligned box, float (6 floats)
+  const float4 *ab_slot;        // per daughter slot (CSR order): lower, upper as float4
   int32_t world;
   int32_t max_depth;            // levels of the deepest path
 };
@@ -448,6 +449,58 @@ template <class L, uint32_t kMask, bool kScreen = false> struct Navigator {
     }
     (void)bi;
     return best;
+  }
+
+  // The basket form of FindNextBoundaryAndStep (:637-743) for one track: the
+  // mother's DistanceToOut with its node index (-1 leaves within pstep, -2
+  // stays; volumes/ShapeImplementationHelper.h:676-692), every daughter's
+  // DistanceToInMinimize (:637-658: a strictly smaller distance takes the
+  // daughter's index), then the relocation with a 1e-9 push.  Unlike the
+  // single-track form there is no special case for a negative or infinite
+  // distance.  The lanes share the daughters as in step().
+  static VGB_HD bool step_basket(const NavGeom &G, const NavPath &cur, NavPath &next,
+                                 const V3<R> &lp, const V3<R> &ld, R pstep, R &dist_out,
+                                 int32_t &node_out) {
+    const int32_t cv = cur.top();
+    const R mother = S::distance_to_out(G, cv, lp, ld, pstep);
+    const LogicalRec &lr = G.logicals[G.placed[cv].logical];
+    const int32_t nd = lr.dcount;
+    const int32_t *dl = G.daughters + lr.dfirst;
+    R best = mother;
+    int bi = mother < pstep ? -1 : -2;
+    R mine = mother;
+    int mi = 0x7fffffff;
+    for (int d = L::lane(); d < nd; d += L::N) {
+      const R dd = S::distance_to_in(G, dl[d], lp, ld, mother);
+      if (dd < mine) {
+        mine = dd;
+        mi = d;
+      }
+    }
+    nav_min_reduce<L>(mine, mi);
+    if (mine < best) {
+      best = mine;
+      bi = mi;
+    }
+    dist_out = best;
+    node_out = bi;
+    next = cur;
+    if (best > pstep) {
+      dist_out = pstep;
+      next.boundary = false;
+      return true;
+    }
+    next.boundary = true;
+    const R s9 = best + (R)1e-9;
+    V3<R> np = {ld.x * s9, ld.y * s9, ld.z * s9};
+    np = {np.x + lp.x, np.y + lp.y, np.z + lp.z};
+    if (bi > -1) {
+      const int32_t nv = dl[bi];
+      if (next.level >= kNavMaxLevels) return false;
+      next.push(nv);
+      return descend<true>(G, next, nv, nav_generic_point(G.raw[G.placed[nv].raw_xform], np), -1);
+    }
+    return relocate_from_path(G, next, np);
   }
 
   // FindNextBoundaryAndStep (:340-470).  `next` is updated in place from `cur`.

@@ -41,6 +41,7 @@ NavGeom nav_geom(const vgb_geometry *g) {
   G.daughters = g->dev.daughters;
   G.pl_box = g->dev.pl_box;
   G.ab_box = g->dev.ab_box;
+  G.ab_slot = g->dev.ab_slot;
   G.world = g->world;
   G.max_depth = g->max_depth;
   return G;
@@ -97,6 +98,41 @@ __global__ void __launch_bounds__(kNavBlock)
       nav_store(nx, NavStateRef{next + i * stride}, G.max_depth);
       step_out[i] = st;
       if (safety_out) safety_out[i] = sf;
+    }
+  }
+}
+
+// basket form of the step (SimpleNavigator.h:637-743) with GetSafeties (:599-632)
+template <uint32_t kMask, bool>
+__global__ void __launch_bounds__(kNavBlock)
+    k_nav_basket(const NavGeom G, int64_t n, const double *x, const double *y, const double *z,
+                 const double *dx, const double *dy, const double *dz, const unsigned char *cur,
+                 unsigned char *next, int64_t stride, const double *pstep, double *dist_out,
+                 double *safety_out, int32_t *node_out, uint32_t *flags) {
+  using Nav = Navigator<WarpLanes, kMask>;
+  const int64_t warps = (int64_t)gridDim.x * kNavWarps;
+  for (int64_t i = (int64_t)blockIdx.x * kNavWarps + threadIdx.x / 32; i < n; i += warps) {
+    NavPath c, nx;
+    nav_load(c, NavStateRef{const_cast<unsigned char *>(cur) + i * stride});
+    const V3<double> p = {x[i], y[i], z[i]};
+    const V3<double> d = {dx[i], dy[i], dz[i]};
+    double st = 0., sf = 0.;
+    int32_t node = -2;
+    bool ok = true;
+    nx = c;
+    if (c.level > 0) {
+      const DXform m = nav_top_matrix(G, c);
+      const V3<double> lp = xf_point(m, p);
+      const V3<double> ld = xf_dir(m, d);
+      if (safety_out) sf = Nav::safety(G, c, lp);
+      ok = Nav::step_basket(G, c, nx, lp, ld, pstep[i], st, node);
+    }
+    if (WarpLanes::lane() == 0) {
+      if (!ok) nav_raise(flags, VGB_NAV_ERR_DEPTH);
+      nav_store(nx, NavStateRef{next + i * stride}, G.max_depth);
+      dist_out[i] = st;
+      if (safety_out) safety_out[i] = sf;
+      if (node_out) node_out[i] = node;
     }
   }
 }
@@ -253,6 +289,11 @@ template <uint32_t M, bool> struct LocateK {
 template <uint32_t M, bool S> struct StepK {
   template <class... A> static void launch(int grid, size_t, cudaStream_t s, A... a) {
     k_nav_step<M, S><<<grid, kNavBlock, 0, s>>>(a...);
+  }
+};
+template <uint32_t M, bool S> struct BasketK {
+  template <class... A> static void launch(int grid, size_t, cudaStream_t s, A... a) {
+    k_nav_basket<M, S><<<grid, kNavBlock, 0, s>>>(a...);
   }
 };
 template <uint32_t M, bool S> struct TraceK {
@@ -425,6 +466,28 @@ vgb_status vgb_nav_find_next_boundary_and_step(const vgb_geometry *g, int64_t n,
                            dy, dz,
                            (const unsigned char *)cur->dev, next->dev, cur->stride, pstep, step,
                            safety, g->dev.nav_flags);
+}
+
+vgb_status vgb_nav_find_next_boundary_and_step_basket(
+    const vgb_geometry *g, int64_t n, const double *x, const double *y, const double *z,
+    const double *dx, const double *dy, const double *dz, const vgb_navpool *cur,
+    vgb_navpool *next, const double *pstep, double *distance, double *safety, int32_t *nextnode,
+    void *stream) {
+  const char *fn = "vgb_nav_find_next_boundary_and_step_basket";
+  vgb_status s = check_nav_geometry(g, fn);
+  if (s != VGB_OK) return s;
+  if (!cur || !next || cur == next || n < 0 || n > cur->n || n > next->n ||
+      cur->max_depth != g->max_depth || next->max_depth != g->max_depth)
+    return set_error(VGB_EINVAL, "%s: need two distinct pools of the geometry's depth", fn);
+  if (n == 0) return VGB_OK;
+  const void *ptrs[] = {x, y, z, dx, dy, dz, pstep, distance};
+  for (const void *p : ptrs)
+    if (!is_device_ptr(p)) return set_error(VGB_EINVAL, "%s: arrays must be device memory", fn);
+  if ((safety && !is_device_ptr(safety)) || (nextnode && !is_device_ptr(nextnode)))
+    return set_error(VGB_EINVAL, "%s: safety / nextnode must be device memory or NULL", fn);
+  return nav_launch<BasketK>(g, n, (cudaStream_t)stream, VGB_PREC_FP64, 0, nav_geom(g), n, x, y,
+                             z, dx, dy, dz, (const unsigned char *)cur->dev, next->dev,
+                             cur->stride, pstep, distance, safety, nextnode, g->dev.nav_flags);
 }
 
 vgb_status vgb_nav_trace(const vgb_geometry *g, int64_t n, const double *x, const double *y,

@@ -174,6 +174,7 @@ NavGeom server_geom(const vgb_geometry *g) {
   G.daughters = g->dev.daughters;
   G.pl_box = g->dev.pl_box;
   G.ab_box = g->dev.ab_box;
+  G.ab_slot = g->dev.ab_slot;
   G.world = g->world;
   G.max_depth = g->max_depth;
   return G;

@@ -361,6 +361,20 @@ class SimpleNavigator:
             _addr(dirs.x), _addr(dirs.y), _addr(dirs.z), cur.handle, nxt.handle, _addr(pstep),
             _addr(step), _addr(safety), precision, _stream(stream)))
 
+    def FindNextBoundaryAndStepBasket(self, points: SOA3D, dirs: SOA3D, cur: NavStatePool,
+                                      nxt: NavStatePool, pstep, distances, safeties=None,
+                                      nextnodes=None, stream=None) -> None:
+        """The basket interface (SimpleNavigator.h:637-743 with GetSafeties);
+        see vgb_nav_find_next_boundary_and_step_basket."""
+        g = self.geometry
+        for a in (pstep, distances, safeties):
+            _check_dtype(a, "f8")
+        _check_dtype(nextnodes, "i4")
+        check(g.L.vgb_nav_find_next_boundary_and_step_basket(
+            g.handle, points.size(), _addr(points.x), _addr(points.y), _addr(points.z),
+            _addr(dirs.x), _addr(dirs.y), _addr(dirs.z), cur.handle, nxt.handle, _addr(pstep),
+            _addr(distances), _addr(safeties), _addr(nextnodes), _stream(stream)))
+
     def Trace(self, points: SOA3D, dirs: SOA3D, pstep: float, max_steps: int, nsteps,
               next_ids=None, steps=None, safeties=None, precision: int = L.PREC_FP64,
               stream=None) -> None:
