@@ -14,6 +14,18 @@
 
 namespace vgb {
 
+// A polar-angle cut c the kernels compare theta = atan2(rho, z) with, and its
+// sine and cosine (mode 1: c < 0, below every theta; mode 2: c above pi).
+struct ThetaCut {
+  double c, sn, cs;
+  int32_t mode;
+  int32_t pad;
+};
+// the cuts: Inside's (fSTheta -/+ half tolerance, eTheta -/+ half tolerance)
+// and DistanceToIn's (tolSTheta, tolETheta, tolSTheta + kAngTolerance,
+// tolETheta - kAngTolerance), each the double value the reference compares with
+enum { kCutInS0, kCutInS1, kCutInE0, kCutInE1, kCutTolS, kCutTolE, kCutTolS2, kCutTolE2, kCuts };
+
 // UnplacedSphere / USphere cached values (volumes/UnplacedSphere.h:25-215,
 // source/UnplacedSphere.cpp:24-95, USolids/src/USphere.cc:30-60).
 struct SphereP {
@@ -29,10 +41,55 @@ struct SphereP {
   int32_t fullTheta;  // fFullThetaSphere
   int32_t full;       // fFullSphere (what IsFullPhiSphere() returns)
   int32_t pad;
+  ThetaCut cut[kCuts];
 };
 
 template <class R> struct SphereOps {
   static constexpr double kHalfAngTol = 0.5 * kAngTolerance;
+
+  // The reference compares polar angles theta = atan2(rho, z) with fixed cuts.
+  // z sin c - rho cos c = r sin(c - theta) decides such a comparison without
+  // atan2 when theta is more than ~3e-15 rad from the cut (the margin covers
+  // the rounding of this expression and of sin c, cos c, rho), well beyond the
+  // error of atan2 itself (2 ulp, < 1e-15 rad), so the outcome is the one the
+  // atan2 comparison gives.  Nearer the cut the comparison evaluates atan2.
+  // -1: theta < c, +1: theta > c, 0: undecided.
+  static VGB_HD int cut_side(R rho, R z, const ThetaCut &k) {
+    if (k.mode == 1) return 1;
+    if (k.mode == 2) return -1;
+    const R f = z * (R)k.sn - rho * (R)k.cs;
+    const R m = (R)4e-15 * (fabs(z) + rho);
+    return f > m ? -1 : (f < -m ? 1 : 0);
+  }
+  // theta = atan2(rho, z), evaluated only when a comparison needs its value
+  struct PolarAngle {
+    R rho, z, t;
+    bool known;
+    VGB_HD PolarAngle(R rho_, R z_) : rho(rho_), z(z_), t(0), known(false) {}
+    VGB_HD R value() {
+      if (!known) {
+        t = atan2(rho, z);
+        known = true;
+      }
+      return t;
+    }
+    VGB_HD bool lt(const ThetaCut &k) {
+      const int sd = cut_side(rho, z, k);
+      return sd ? sd < 0 : value() < (R)k.c;
+    }
+    VGB_HD bool le(const ThetaCut &k) {
+      const int sd = cut_side(rho, z, k);
+      return sd ? sd < 0 : value() <= (R)k.c;
+    }
+    VGB_HD bool gt(const ThetaCut &k) {
+      const int sd = cut_side(rho, z, k);
+      return sd ? sd > 0 : value() > (R)k.c;
+    }
+    VGB_HD bool ge(const ThetaCut &k) {
+      const int sd = cut_side(rho, z, k);
+      return sd ? sd > 0 : value() >= (R)k.c;
+    }
+  };
 
   // :804-880 GenericKernelForContainsAndInside (both flags always computed)
   static VGB_HD void kernel(const SphereP &s, const V3<R> &p, bool &cin, bool &cout) {
@@ -55,10 +112,10 @@ template <class R> struct SphereOps {
       if (cout) return;
     }
     if (!s.fullTheta) {
-      const R pTheta = atan2(sqrt(p.x * p.x + p.y * p.y), p.z);
-      const R fST = (R)s.stheta, eT = (R)s.stheta + (R)s.dtheta;
-      cin &= (pTheta <= eT - ht) && (pTheta >= fST + ht);
-      cout |= (pTheta < fST - ht) || (pTheta > eT + ht);
+      // pTheta = atan2(sqrt(x^2 + y^2), z) against stheta -/+ ht, eTheta -/+ ht
+      PolarAngle th(sqrt(p.x * p.x + p.y * p.y), p.z);
+      cin &= th.le(s.cut[kCutInE0]) && th.ge(s.cut[kCutInS1]);
+      cout |= th.lt(s.cut[kCutInS0]) || th.gt(s.cut[kCutInE1]);
     }
   }
 
@@ -86,7 +143,6 @@ template <class R> struct SphereOps {
   static VGB_HD R dti_core(const SphereP &s, const V3<R> &p, const V3<R> &v) {
     const R inf = Lim<R>::inf();
     R snxt = inf;
-    R tolSTheta = 0, tolETheta = 0;
     const R dRmax = (R)100. * (R)s.rmax;
     const R halfCarTol = (R)(kTolerance * 0.5);
     const R halfAngTol = (R)kHalfAngTol;
@@ -97,33 +153,25 @@ template <class R> struct SphereOps {
     const R tolIRMin2 = (fRmin + halfRminTol) * (fRmin + halfRminTol);
     const R tolORMax2 = (fRmax + halfTol) * (fRmax + halfTol);
     const R tolIRMax2 = (fRmax - halfTol) * (fRmax - halfTol);
-    const R kAng = (R)kAngTolerance;
     const R eTheta = (R)s.eTheta, fSTheta = (R)s.stheta;
     const R piby2 = (R)(kPi / 2);
-    R xi, yi, zi, rhoi, rhoi2, radi2, iTheta, sd, c, d2, t1, t2, b, d;
+    R xi, yi, zi, rhoi, rhoi2, radi2, sd, c, d2, t1, t2, b, d;
 
     const R rho2 = p.x * p.x + p.y * p.y;
     const R rad2 = rho2 + p.z * p.z;
-    // polar angle of the point, computed on first use (only the theta-cone
-    // branches read it; the value is the reference's atan2(sqrt(rho2), z))
-    R pThetaV = 0;
-    bool pThetaSet = false;
-    auto pTheta = [&]() {
-      if (!pThetaSet) {
-        pThetaV = atan2(sqrt(rho2), p.z);
-        pThetaSet = true;
-      }
-      return pThetaV;
-    };
+    // polar angle of the point, the reference's atan2(sqrt(rho2), z); only
+    // compared with the cuts (PolarAngle)
+    PolarAngle pTheta(sqrt(rho2), p.z);
     const R pDotV2d = p.x * v.x + p.y * v.y;
     const R pDotV3d = pDotV2d + p.z * v.z;
-    if (!s.fullTheta) {
-      tolSTheta = fSTheta - halfAngTol;
-      tolETheta = eTheta + halfAngTol;
-    }
-    auto theta_in = [&](R th) { return (th >= tolSTheta) && (th <= tolETheta); };
+    // theta of (rho, z) within [tolSTheta, tolETheta]
+    auto theta_in = [&](R rh, R zz) {
+      PolarAngle th(rh, zz);
+      return th.ge(s.cut[kCutTolS]) && th.le(s.cut[kCutTolE]);
+    };
+    // pTheta within [tolSTheta + kAng, tolETheta - kAng]
     auto strictly_theta = [&]() {
-      return (pTheta() >= tolSTheta + kAng) && (pTheta() <= tolETheta - kAng);
+      return pTheta.ge(s.cut[kCutTolS2]) && pTheta.le(s.cut[kCutTolE2]);
     };
 
     // outer sphere (:667-760)
@@ -148,8 +196,7 @@ template <class R> struct SphereOps {
             if (psi_ok(s, xi, yi, rhoi, s.cosHDPhiOT)) {
               if (!s.fullTheta) {
                 zi = p.z + sd * v.z;
-                iTheta = atan2(rhoi, zi);
-                if (theta_in(iTheta)) return sd;
+                if (theta_in(rhoi, zi)) return sd;
               } else {
                 return sd;
               }
@@ -157,8 +204,7 @@ template <class R> struct SphereOps {
           } else {
             if (!s.fullTheta) {
               zi = p.z + sd * v.z;
-              iTheta = atan2(rhoi, zi);
-              if (theta_in(iTheta)) return sd;
+              if (theta_in(rhoi, zi)) return sd;
             } else {
               return sd;
             }
@@ -219,8 +265,7 @@ template <class R> struct SphereOps {
             if (psi_ok(s, xi, yi, rhoi, s.cosHDPhiOT)) {
               if (!s.fullTheta) {
                 zi = p.z + sd * v.z;
-                iTheta = atan2(rhoi, zi);
-                if (theta_in(iTheta)) snxt = sd;
+                if (theta_in(rhoi, zi)) snxt = sd;
               } else {
                 snxt = sd;
               }
@@ -228,8 +273,7 @@ template <class R> struct SphereOps {
           } else {
             if (!s.fullTheta) {
               zi = p.z + sd * v.z;
-              iTheta = atan2(rhoi, zi);
-              if (theta_in(iTheta)) snxt = sd;
+              if (theta_in(rhoi, zi)) snxt = sd;
             } else {
               snxt = sd;
             }
@@ -267,8 +311,7 @@ template <class R> struct SphereOps {
         const bool half_ok = plane == 0 ? (side <= 0) : (side >= 0);
         if ((radi2 <= tolORMax2) && (radi2 >= tolORMin2) && half_ok) {
           if (!s.fullTheta) {
-            iTheta = atan2(sqrt(rhoi2), zi);
-            if (theta_in(iTheta) && half_ok) snxt = sd;
+            if (theta_in(sqrt(rhoi2), zi) && half_ok) snxt = sd;
           } else {
             snxt = sd;
           }
@@ -297,7 +340,7 @@ template <class R> struct SphereOps {
         }
       };
       const R tanS2 = (R)s.tanSTheta2, tanE2 = (R)s.tanETheta2;
-      if (pTheta() < tolSTheta) {
+      if (pTheta.lt(s.cut[kCutTolS])) {
         t1 = (R)1 - v.z * v.z * ((R)1 + tanS2);
         t2 = pDotV2d - p.z * v.z * tanS2;
         if (t1 != 0) {
@@ -326,7 +369,7 @@ template <class R> struct SphereOps {
             }
           }
         }
-      } else if (pTheta() > tolETheta) {
+      } else if (pTheta.gt(s.cut[kCutTolE])) {
         t1 = (R)1 - v.z * v.z * ((R)1 + tanE2);
         t2 = pDotV2d - p.z * v.z * tanE2;
         if (t1 != 0) {
@@ -355,7 +398,7 @@ template <class R> struct SphereOps {
             }
           }
         }
-      } else if ((pTheta() < tolSTheta + kAng) && (fSTheta > halfAngTol)) {
+      } else if (pTheta.lt(s.cut[kCutTolS2]) && (fSTheta > halfAngTol)) {
         t2 = pDotV2d - p.z * v.z * tanS2;
         if ((t2 >= 0 && tolIRMin2 < rad2 && rad2 < tolIRMax2 && s.stheta < kPi / 2) ||
             (t2 < 0 && tolIRMin2 < rad2 && rad2 < tolIRMax2 && s.stheta > kPi / 2) ||
@@ -377,7 +420,7 @@ template <class R> struct SphereOps {
             if ((sd >= halfCarTol) && (sd < snxt) && (s.stheta < kPi / 2)) accept(sd, fSTheta);
           }
         }
-      } else if ((pTheta() > tolETheta - kAng) && (s.eTheta < kPi - kAngTolerance)) {
+      } else if (pTheta.gt(s.cut[kCutTolE2]) && (s.eTheta < kPi - kAngTolerance)) {
         t2 = pDotV2d - p.z * v.z * tanE2;
         if (((t2 < 0) && (s.eTheta < kPi / 2) && (tolIRMin2 < rad2) && (rad2 < tolIRMax2)) ||
             ((t2 >= 0) && (s.eTheta > kPi / 2) && (tolIRMin2 < rad2) && (rad2 < tolIRMax2)) ||

@@ -175,6 +175,21 @@ SphereP make_sphere(double rmin, double rmax, double sphi, double dphi, double s
   s.fullPhi = fullPhi;
   s.fullTheta = fullTheta;
   s.full = full;
+  // the polar-angle cuts the kernels compare with, as the kernels compute them
+  // (Inside: stheta -/+ ht, stheta + dtheta -/+ ht; DistanceToIn: tolSTheta =
+  // stheta - ht, tolETheta = eTheta + ht, and those moved inwards by kAngTol)
+  const double ht = 0.5 * kAngTol;
+  const double eT = fSTheta + fDTheta;
+  const double tolS = fSTheta - ht, tolE = s.eTheta + ht;
+  const double cuts[kCuts] = {fSTheta - ht, fSTheta + ht, eT - ht, eT + ht,
+                              tolS,         tolE,         tolS + kAngTol, tolE - kAngTol};
+  for (int k = 0; k < kCuts; ++k) {
+    ThetaCut &c = s.cut[k];
+    c.c = cuts[k];
+    c.sn = std::sin(cuts[k]);
+    c.cs = std::cos(cuts[k]);
+    c.mode = cuts[k] < 0 ? 1 : (cuts[k] > kPi ? 2 : 0);
+  }
   return s;
 }
 
