@@ -1,8 +1,9 @@
-"""Sphere polar-angle cuts: points and rays placed 0 to 1e-11 rad from every
+"""Sphere angle cuts: points and rays placed 0 to 1e-11 rad from every
 theta cut the kernels compare with (stheta -/+ the half angular tolerance,
 eTheta -/+ it).  The kernels decide such comparisons from z sin c - rho cos c
 and evaluate atan2 only within ~3e-15 rad of a cut; these cases sit on both
-sides of that margin.
+sides of that margin.  Points near phi = 0 check the phi test, which a
+full-phi sphere with a theta cut decides without atan2 away from that seam.
 
   * CPU: the host build of the shape arithmetic against the reference (Inside,
     Contains) and against USolids' USphere::DistanceToIn (the in-tree sphere
@@ -60,6 +61,25 @@ def cut_cases(spec, seed):
     return pts, rays, off
 
 
+def seam_points(spec, seed):
+    """Points of the radial shell at phi = 0 + offsets (the phi test of a
+    full-phi sphere with a theta cut only matters within its half tolerance,
+    5e-10 rad, of phi = 0), on both sides of x = 0, and on the z axis."""
+    p = spec.params
+    rng = np.random.default_rng(seed)
+    dphi = np.array([0., 1e-12, -1e-12, 1e-10, -1e-10, 4e-10, -4e-10, 6e-10, -6e-10, 1e-9, -1e-9,
+                     9e-9, -9e-9, 1.1e-8, -1.1e-8, 2e-8, -2e-8, math.pi / 2, math.pi, -math.pi])
+    st, et = p["stheta"], p["stheta"] + p["dtheta"]
+    th = np.repeat(np.linspace(st + 0.05, et - 0.05, 4), len(dphi))
+    ph = np.tile(dphi, 4)
+    r = rng.uniform(p["rmin"] + 1., p["rmax"] - 1., len(th))
+    x, y, z = r * np.sin(th) * np.cos(ph), r * np.sin(th) * np.sin(ph), r * np.cos(th)
+    axis = np.array([p["rmin"] + 2., p["rmax"] - 2., -(p["rmin"] + 2.)])
+    return (np.concatenate([x, np.zeros(3), -np.zeros(3)]),
+            np.concatenate([y, np.zeros(3), np.zeros(3)]),
+            np.concatenate([z, axis, axis]))
+
+
 def reference(spec, pts, rays):
     ref = oracle.RefLib()
     pv = ref.placed(oracle.ref_unplaced(ref, spec))
@@ -79,6 +99,44 @@ def test_host_theta_cuts_match_reference(hc, name):  # noqa: F811
     assert_exact(host_run(hc, g, pv, 0, pts), want["contains"], "Contains")
     assert_exact(host_run(hc, g, pv, 1, pts), want["inside"], "Inside")
     assert_distances(host_run(hc, g, pv, 2, *rays, step), want["dti"], "DistanceToIn")
+
+
+@pytest.mark.skipif(not HAVE_REF, reason="oracle/_ref not built")
+@pytest.mark.parametrize("name", list(SPECS))
+def test_host_phi_seam_matches_reference(hc, name):  # noqa: F811
+    spec = SPECS[name]
+    pts = seam_points(spec, 12)
+    ref = oracle.RefLib()
+    rpv = ref.placed(oracle.ref_unplaced(ref, spec))
+    g = Geometry(library=hc)
+    pv = g.LogicalVolume("s", W.build_unplaced(g, spec)).Place(g.Transformation3D())
+    assert_exact(host_run(hc, g, pv, 0, pts), ref.batch(rpv, 0, pts), "Contains")
+    assert_exact(host_run(hc, g, pv, 1, pts), ref.batch(rpv, 1, pts), "Inside")
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not HAVE_REF, reason="oracle/_ref not built")
+@pytest.mark.parametrize("name", list(SPECS))
+def test_gpu_phi_seam_matches_reference(name):
+    import torch
+    import vecgeom_b200 as V
+    spec = SPECS[name]
+    pts = seam_points(spec, 12)
+    ref = oracle.RefLib()
+    rpv = ref.placed(oracle.ref_unplaced(ref, spec))
+    g = V.Geometry()
+    pv = g.LogicalVolume("s", W.build_unplaced(g, spec)).Place(g.Transformation3D())
+    g.SetWorld(pv)
+    g.CloseGeometry()
+    n = len(pts[0])
+    P = V.SOA3D(*(torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in pts))
+    c = torch.zeros(n, dtype=torch.uint8, device="cuda")
+    i = torch.zeros(n, dtype=torch.int32, device="cuda")
+    pv.Contains(P, c)
+    pv.Inside(P, i)
+    torch.cuda.synchronize()
+    assert_exact(c.cpu().numpy(), ref.batch(rpv, 0, pts), "Contains")
+    assert_exact(i.cpu().numpy(), ref.batch(rpv, 1, pts), "Inside")
 
 
 @pytest.mark.gpu

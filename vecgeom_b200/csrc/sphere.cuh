@@ -102,7 +102,13 @@ template <class R> struct SphereOps {
     cout = (rad2 <= tolRMin * tolRMin) || (rad2 >= tolRMax * tolRMax);
     if (cout) return;
     const R ht = (R)kHalfAngTol;
-    if (!s.full) {
+    // A full-phi sphere with a theta cut still runs the phi test (fFullSphere
+    // is false).  With fSPhi = 0 and fDPhi = 2 pi the test only changes the
+    // result for points within the half tolerance of phi = 0 (they lose
+    // kInside); a point with x < 0, or with |y| > 1e-8 |x| (more than 1e-8 rad
+    // from phi = 0), keeps cin and cout as they are without atan2.
+    const bool phi_far = s.fullPhi && ((p.x < 0) || (fabs(p.y) > (R)1e-8 * fabs(p.x)));
+    if (!s.full && !phi_far) {
       R pPhi = atan2(p.y, p.x);
       const R fSPhi = (R)s.sphi, ePhi = (R)s.sphi + (R)s.dphi;
       if (pPhi < fSPhi - ht) pPhi = pPhi + (R)(2. * kPi);
@@ -563,7 +569,7 @@ template <class R> struct SphereOps {
     const R rad = sqrt(rad2);
     const R pDotV3d = p.x * v.x + p.y * v.y + p.z * v.z;
     const R rxy2 = p.x * p.x + p.y * p.y;
-    R snxt = inf, b = 0, delta = 0, xnew = 0, ynew = 0, znew = 0, phi0 = 0, ddp = 0;
+    R snxt = inf, b = 0, delta = 0, xnew = 0, ynew = 0, znew = 0;
     R sn1 = inf, rn1 = inf, sn2 = inf, rn2;
     const R fPhi1 = (R)s.sphi, fPhi2 = (R)s.ePhi;
     const R fRmin = (R)s.rmin, fRmax = (R)s.rmax;
@@ -575,6 +581,15 @@ template <class R> struct SphereOps {
     const R sr = vmin(rn1, rn2);
 
     const bool isFullPhiSphere = s.full;
+    // the phi test of a theta-cone candidate: atan2(y, x) - fPhi1 moved into
+    // [0, 2 pi) against fPhi2 - fPhi1.  For a full-phi sphere (fPhi1 = 0,
+    // fPhi2 = 2 pi) every angle passes, NaN excepted.
+    auto in_phi_range = [&](R x, R y) {
+      if (s.fullPhi) return !(x != x || y != y);
+      R d = atan2(y, x) - fPhi1;
+      if (d < zero) d = d + (R)(2 * kPi);
+      return d <= (fPhi2 - fPhi1);
+    };
     if (!s.fullTheta) {
       // one theta cone; returns true if the point leaves through it at once
       auto theta_cone = [&](bool first, R &snside) -> bool {
@@ -617,10 +632,7 @@ template <class R> struct SphereOps {
           } else {
             xnew = pt.x + snxt * v.x;
             ynew = pt.y + snxt * v.y;
-            phi0 = atan2(ynew, xnew);
-            ddp = phi0 - fPhi1;
-            if (ddp < zero) ddp = ddp + (R)(2 * kPi);
-            if (ddp <= (fPhi2 - fPhi1)) snside = snxt;
+            if (in_phi_range(xnew, ynew)) snside = snxt;
           }
         }
         // second root: the reference tests sn > toler (end cone) / sn > toler2
@@ -635,10 +647,7 @@ template <class R> struct SphereOps {
             } else {
               xnew = pt.x + snxt * v.x;
               ynew = pt.y + snxt * v.y;
-              phi0 = atan2(ynew, xnew);
-              ddp = phi0 - fPhi1;
-              if (ddp < zero) ddp = ddp + (R)(2 * kPi);
-              if (ddp <= (fPhi2 - fPhi1)) snside = snxt;
+              if (in_phi_range(xnew, ynew)) snside = snxt;
             }
           }
         }
