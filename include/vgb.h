@@ -75,7 +75,9 @@ typedef enum {
   VGB_SHAPE_POLYCONE = 6,
   VGB_SHAPE_POLYHEDRON = 7,
   VGB_SHAPE_BOOLEAN = 8,
-  VGB_SHAPE_TRD = 9
+  VGB_SHAPE_TRD = 9,
+  VGB_SHAPE_ORB = 10,
+  VGB_SHAPE_PARALLELEPIPED = 11
 } vgb_shape_type;
 
 /* volumes/UnplacedBooleanVolume.h:10-14 */
@@ -130,6 +132,12 @@ vgb_status vgb_unplaced_polyhedron(vgb_geometry *g, double phi_start_deg, double
 /* volumes/UnplacedTrd.h:73 */
 vgb_status vgb_unplaced_trd(vgb_geometry *g, double dx1, double dx2, double dy1, double dy2,
                             double dz, int32_t *id);
+/* volumes/UnplacedOrb.h:45 */
+vgb_status vgb_unplaced_orb(vgb_geometry *g, double r, int32_t *id);
+/* volumes/UnplacedParallelepiped.h:34 (half-lengths; alpha, theta, phi in degrees) */
+vgb_status vgb_unplaced_parallelepiped(vgb_geometry *g, double x, double y, double z,
+                                       double alpha_deg, double theta_deg, double phi_deg,
+                                       int32_t *id);
 /* volumes/UnplacedBooleanVolume.h:46 (left/right are placed-volume ids) */
 vgb_status vgb_unplaced_boolean(vgb_geometry *g, int32_t op, int32_t left_placed,
                                 int32_t right_placed, int32_t *id);

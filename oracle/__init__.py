@@ -110,6 +110,10 @@ class RefLib:
             f = getattr(L, name)
             f.restype = _vp
             f.argtypes = [_d] * argn
+        L.vgref_orb.restype = _vp
+        L.vgref_orb.argtypes = [_d]
+        L.vgref_parallelepiped.restype = _vp
+        L.vgref_parallelepiped.argtypes = [_d] * 6
         L.vgref_polycone.restype = _vp
         L.vgref_polycone.argtypes = [_d, _d, _i, _vp, _vp, _vp]
         L.vgref_polyhedron.restype = _vp
@@ -312,6 +316,10 @@ def ref_unplaced(ref: RefLib, spec):
         return L.vgref_torus(p["rmin"], p["rmax"], p["rtor"], p["sphi"], p["dphi"])
     if k == "trd":
         return L.vgref_trd(p["dx1"], p["dx2"], p["dy1"], p["dy2"], p["dz"])
+    if k == "orb":
+        return L.vgref_orb(p["r"])
+    if k == "parallelepiped":
+        return L.vgref_parallelepiped(p["x"], p["y"], p["z"], p["alpha"], p["theta"], p["phi"])
     if k in ("polycone", "polyhedron"):
         z, rmin, rmax = (np.ascontiguousarray(p[a], np.float64) for a in ("z", "rmin", "rmax"))
         ref._keep += [z, rmin, rmax]

@@ -6,8 +6,8 @@
 // the golden fixtures in tests/golden/) and by bench.py's CPU-baseline leg.
 //
 // Every entry point builds or calls the reference's own objects:
-//   - shapes: Unplaced{Box,Tube,Cone,Sphere,Torus,Polycone,Polyhedron,Trd,
-//     BooleanVolume} constructors (volumes/Unplaced*.h),
+//   - shapes: Unplaced{Box,Tube,Cone,Sphere,Torus,Polycone,Polyhedron,Trd,Orb,
+//     Parallelepiped,BooleanVolume} constructors (volumes/Unplaced*.h),
 //   - placement: LogicalVolume::Place / PlaceDaughter (source/LogicalVolume.cpp:60-102),
 //   - batch ops: the VPlacedVolume SOA3D virtuals (volumes/PlacedVolume.h:145-250),
 //   - navigation: SimpleNavigator (navigation/SimpleNavigator.h:204-743).
@@ -24,6 +24,8 @@
 #include "volumes/Polycone.h"
 #include "volumes/Polyhedron.h"
 #include "volumes/Trd.h"
+#include "volumes/Orb.h"
+#include "volumes/Parallelepiped.h"
 #include "volumes/BooleanVolume.h"
 #include "management/GeoManager.h"
 #include "navigation/NavigationState.h"
@@ -151,6 +153,17 @@ void *vgref_polyhedron(double phistart_deg, double phidelta_deg, int nsides, int
                        const double *z, const double *rmin, const double *rmax) {
   std::vector<double> zz(z, z + nz);
   return new UnplacedPolyhedron(phistart_deg, phidelta_deg, nsides, nz, zz.data(), rmin, rmax);
+}
+// UnplacedOrb(r) computes its tolerance from a member not yet initialised
+// (volumes/UnplacedOrb.h:27-35, source/UnplacedOrb.cpp:33-44); SetRadius, the
+// reference's own setter, recomputes the cached values with it initialised.
+void *vgref_orb(double r) {
+  UnplacedOrb *o = new UnplacedOrb(r);
+  o->SetRadius(r);
+  return o;
+}
+void *vgref_parallelepiped(double x, double y, double z, double alpha, double theta, double phi) {
+  return new UnplacedParallelepiped(x, y, z, alpha, theta, phi);
 }
 void *vgref_trd(double x1, double x2, double y1, double y2, double z) {
   return new UnplacedTrd(x1, x2, y1, y2, z);

@@ -125,7 +125,8 @@ from vecgeom_b200.workloads import build_unplaced as vgb_unplaced  # noqa: E402,
 
 
 def shape_specs() -> dict:
-    """The shapes of the parity tests: the benchmark shapes plus a trd."""
+    """The shapes of the parity tests: the benchmark shapes plus a trd, an orb
+    and parallelepipeds."""
     from vecgeom_b200 import workloads as W
     s = {"box": W.box_spec(10., 20., 30.)}
     s.update(W.config2_shapes())
@@ -146,6 +147,11 @@ def shape_specs() -> dict:
                                         [0., 5., 8., 0., 12.], [20., 25., 30., 18., 30.])
     # components with their own placements (the right one with 6e-17 entries the
     # specialised transform drops and the generic one keeps)
+    s["orb"] = W.orb_spec(25.)
+    s["orbsmall"] = W.orb_spec(0.7)
+    s["parallelepiped"] = W.parallelepiped_spec(20., 30., 40., 30., 20., 40.)
+    s["parallelepipedneg"] = W.parallelepiped_spec(15., 10., 25., -45., 35., 200.)
+    s["parallelepipedbox"] = W.parallelepiped_spec(12., 8., 5., 0., 0., 0.)
     s["boolsubxf"] = W.boolsub_spec((30., 30., 30.), 15., 40., left_place=(2., -1., 3., 0., 0., 15.),
                                     right_place=(5., 0., -4., 0., 90., 0.))
     return s

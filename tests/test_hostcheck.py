@@ -24,7 +24,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 SO = os.path.join(ROOT, "_build", "hostcheck", "libvgb_hostcheck.so")
 GOLDEN = sorted(glob.glob(os.path.join(HERE, "golden", "*.npz")))
-HOST_SHAPES = {"box", "tube", "cone", "sphere", "trd", "torus", "polycone", "polyhedron",
+HOST_SHAPES = {"box", "tube", "cone", "sphere", "trd", "torus", "polycone", "polyhedron", "orb",
+               "parallelepiped",
                "boolsub"}
 
 

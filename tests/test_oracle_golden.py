@@ -33,7 +33,8 @@ def spec_from_meta(meta):
     ctor = {"box": W.box_spec, "tube": W.tube_spec, "cone": W.cone_spec,
             "sphere": W.sphere_spec, "torus": W.torus_spec, "trd": W.trd_spec,
             "polycone": W.polycone_spec, "polyhedron": W.polyhedron_spec,
-            "boolsub": W.boolsub_spec}[k]
+            "boolsub": W.boolsub_spec, "orb": W.orb_spec,
+            "parallelepiped": W.parallelepiped_spec}[k]
     return ctor(**p)
 
 

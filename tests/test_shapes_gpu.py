@@ -19,7 +19,8 @@ from test_oracle_golden import load_case, spec_from_meta
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 GOLDEN = sorted(glob.glob(os.path.join(HERE, "golden", "*.npz")))
-VGB_SHAPES = {"box", "tube", "cone", "sphere", "trd", "torus", "polycone", "polyhedron", "boolsub"}
+VGB_SHAPES = {"box", "tube", "cone", "sphere", "trd", "torus", "polycone", "polyhedron", "boolsub",
+              "orb", "parallelepiped"}
 
 pytestmark = pytest.mark.gpu
 

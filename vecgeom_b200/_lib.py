@@ -66,6 +66,8 @@ SIGNATURES = {
     "vgb_unplaced_polycone": (ctypes.c_int, [_vp, _dbl, _dbl, _i32, _vp, _vp, _vp, _pi32]),
     "vgb_unplaced_polyhedron": (ctypes.c_int, [_vp, _dbl, _dbl, _i32, _i32, _vp, _vp, _vp, _pi32]),
     "vgb_unplaced_trd": (ctypes.c_int, [_vp] + [_dbl] * 5 + [_pi32]),
+    "vgb_unplaced_orb": (ctypes.c_int, [_vp, _dbl, _pi32]),
+    "vgb_unplaced_parallelepiped": (ctypes.c_int, [_vp] + [_dbl] * 6 + [_pi32]),
     "vgb_unplaced_boolean": (ctypes.c_int, [_vp, _i32, _i32, _i32, _pi32]),
     "vgb_transformation": (ctypes.c_int, [_vp] + [_dbl] * 6 + [_pi32]),
     "vgb_transformation_matrix": (ctypes.c_int, [_vp, _dbl, _dbl, _dbl, _vp, _pi32]),

@@ -58,7 +58,9 @@ constexpr int kBoolMaxRounds = 4096;
   X(VGB_SHAPE_TRD, vgb::TrdOps, vgb::TrdP)                    \
   X(VGB_SHAPE_TORUS, vgb::TorusOps, vgb::TorusP)              \
   X(VGB_SHAPE_POLYCONE, vgb::PolyconeOps, vgb::PolyconeP)    \
-  X(VGB_SHAPE_POLYHEDRON, vgb::PolyhedronOps, vgb::PolyhedronP)
+  X(VGB_SHAPE_POLYHEDRON, vgb::PolyhedronOps, vgb::PolyhedronP)      \
+  X(VGB_SHAPE_ORB, vgb::OrbOps, vgb::OrbP)                            \
+  X(VGB_SHAPE_PARALLELEPIPED, vgb::ParaOps, vgb::ParaP)
 
 template <class P> VGB_HD P comp_params(const double *rec) {
   return bind_params(*reinterpret_cast<const P *>(rec), rec);

@@ -363,13 +363,20 @@ vgb_status vgb::prepare_tables(vgb_geometry *g) {
   // (base/Transformation3D.h:598-632), their min / max (std::min, std::max, in
   // the reference's corner order) widened by 1e-3; InitABBoxes
   // (:185-262) keeps a float copy for the navigator's hit test
+  g->abbox_ok = true;
   g->ab_box_d.assign(6 * g->placed.size(), 0.);
   g->ab_box.assign(6 * g->placed.size(), 0.f);
   for (size_t pv = 0; pv < g->placed.size(); ++pv) {
     const UnplacedRec &u = g->unplaced[g->placed[pv].unplaced];
     double lo[3], hi[3];
-    if (!reference_extent(u.type, g->params.data() + u.param_off, lo, hi))
-      return set_error(VGB_EINVAL, "vgb_geometry_close: no extent for shape type %d", u.type);
+    if (!reference_extent(u.type, g->params.data() + u.param_off, lo, hi)) {
+      // the reference's VPlacedVolume::Extent asserts for this shape
+      // (volumes/PlacedVolume.h:260-263); its volumes get no box and the ABBox
+      // navigator refuses the geometry
+      g->abbox_ok = false;
+      for (int k = 0; k < 6; ++k) g->ab_box_d[6 * pv + k] = std::numeric_limits<double>::quiet_NaN();
+      continue;
+    }
     const RawXform &x = g->raw_xforms[g->placed[pv].raw_xform];
     const double delta[3] = {hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2]};
     double mn[3], mx[3];
@@ -456,6 +463,11 @@ vgb_status vgb_abbox_compute(const vgb_geometry *g, int32_t placed, double *lowe
     vgb_status s = prepare_tables(gm);
     if (s != VGB_OK) return s;
   }
+  const UnplacedRec &u = g->unplaced[g->placed[placed].unplaced];
+  double lo[3], hi[3];
+  if (!reference_extent(u.type, g->params.data() + u.param_off, lo, hi))
+    return set_error(VGB_ENOTSUP, "vgb_abbox_compute: shape type %d has no Extent in the reference",
+                     u.type);
   for (int k = 0; k < 6; ++k) lower_upper[k] = g->ab_box_d[6 * (size_t)placed + k];
   return VGB_OK;
 }

@@ -95,6 +95,7 @@ struct vgb_geometry {
   std::vector<double> ab_box_d;        // per placed: ABBoxManager::ComputeABBox (lower, upper)
   std::vector<float> ab_box;           // the same boxes rounded to float, as navigated
   std::vector<float4> ab_slot;         // per daughter slot: (lower, 0), (upper, 0)
+  bool abbox_ok = true;                // every placed volume's shape has an Extent
   uint32_t type_mask = 0;              // bit t set when a shape of type t exists
   int32_t world = -1;
   int32_t max_depth = 0;

@@ -524,6 +524,9 @@ vgb_status vgb_abbox_nav_find_next_boundary_and_step(const vgb_geometry *g, int6
   const char *fn = "vgb_abbox_nav_find_next_boundary_and_step";
   vgb_status s = check_nav_geometry(g, fn);
   if (s != VGB_OK) return s;
+  if (!g->abbox_ok)
+    return set_error(VGB_ENOTSUP, "%s: a volume's shape has no Extent (parallelepiped), so no "
+                     "aligned box", fn);
   if (!cur || !next || cur == next || n < 0 || n > cur->n || n > next->n ||
       cur->max_depth != g->max_depth || next->max_depth != g->max_depth)
     return set_error(VGB_EINVAL, "%s: need two distinct pools of the geometry's depth", fn);
@@ -548,6 +551,9 @@ vgb_status vgb_abbox_nav_trace(const vgb_geometry *g, int64_t n, const double *x
   const char *fn = "vgb_abbox_nav_trace";
   vgb_status s = check_nav_geometry(g, fn);
   if (s != VGB_OK) return s;
+  if (!g->abbox_ok)
+    return set_error(VGB_ENOTSUP, "%s: a volume's shape has no Extent (parallelepiped), so no "
+                     "aligned box", fn);
   if (n < 0 || max_steps < 0) return set_error(VGB_EINVAL, "%s: n or max_steps < 0", fn);
   if (n == 0) return VGB_OK;
   const void *ptrs[] = {x, y, z, dx, dy, dz, nsteps};

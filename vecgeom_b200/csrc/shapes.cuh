@@ -11,6 +11,8 @@
 #include "torus.cuh"
 #include "polycone.cuh"
 #include "polyhedron.cuh"
+#include "orb.cuh"
+#include "parallelepiped.cuh"
 
 struct vgb_geometry;
 

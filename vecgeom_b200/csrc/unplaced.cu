@@ -193,6 +193,40 @@ SphereP make_sphere(double rmin, double rmax, double sphi, double dphi, double s
   return s;
 }
 
+// UnplacedOrb(r) (source/UnplacedOrb.cpp:33-44) reads frTolerance in its
+// initialiser list before that member is initialised (members are initialised
+// in declaration order, volumes/UnplacedOrb.h:27-35), so the tolerance it
+// computes is undefined (garbage memory made it huge in some runs here).  This
+// takes the values the reference's own SetRadius (:52-60) computes, with
+// frTolerance = 1e-9: fRTolerance = Max(1e-9, fepsilon * fR).
+OrbP make_orb(double r) {
+  OrbP o;
+  std::memset(&o, 0, sizeof(o));
+  const double fepsilon = 2e-11, frTolerance = 1e-9;
+  o.r = r;
+  o.rTolerance = vmax(frTolerance, fepsilon * r);
+  o.rTolI = r - o.rTolerance;
+  o.rTolO = r + o.rTolerance;
+  return o;
+}
+
+// UnplacedParallelepiped(x, y, z, alpha, theta, phi), angles in degrees
+// (source/UnplacedParallelepiped.cpp:24-65); ctx / cty as the safeties compute
+// them (ParallelepipedImplementation.h:270-276)
+ParaP make_parallelepiped(double x, double y, double z, double alpha, double theta, double phi) {
+  ParaP a;
+  std::memset(&a, 0, sizeof(a));
+  a.dims.d[0] = x;
+  a.dims.d[1] = y;
+  a.dims.d[2] = z;
+  a.tanAlpha = std::tan(kDegToRad * alpha);
+  a.tanThetaCosPhi = std::tan(kDegToRad * theta) * std::cos(kDegToRad * phi);
+  a.tanThetaSinPhi = std::tan(kDegToRad * theta) * std::sin(kDegToRad * phi);
+  a.ctx = 1.0 / std::sqrt(1. + a.tanAlpha * a.tanAlpha + a.tanThetaCosPhi * a.tanThetaCosPhi);
+  a.cty = 1.0 / std::sqrt(1. + a.tanThetaSinPhi * a.tanThetaSinPhi);
+  return a;
+}
+
 // UnplacedTrd::calculateCached (volumes/UnplacedTrd.h:38-51)
 TrdP make_trd(double dx1, double dx2, double dy1, double dy2, double dz) {
   TrdP t;
@@ -541,6 +575,18 @@ bool shape_bbox(const vgb_geometry *g, int32_t u, double b[6]) {
       const TrdP &p = *reinterpret_cast<const TrdP *>(rec);
       return sym(std::max(p.dx1, p.dx2), std::max(p.dy1, p.dy2), p.dz);
     }
+    case VGB_SHAPE_ORB: {
+      const OrbP &p = *reinterpret_cast<const OrbP *>(rec);
+      return sym(p.rTolO, p.rTolO, p.rTolO);
+    }
+    case VGB_SHAPE_PARALLELEPIPED: {
+      // the box's corners mapped back through the shear
+      const ParaP &p = *reinterpret_cast<const ParaP *>(rec);
+      const double z = p.dims.d[2], y = std::fabs(p.dims.d[1]) + std::fabs(p.tanThetaSinPhi) * z;
+      const double x = std::fabs(p.dims.d[0]) + std::fabs(p.tanThetaCosPhi) * z +
+                       std::fabs(p.tanAlpha) * y;
+      return sym(x, y, z);
+    }
     case VGB_SHAPE_POLYCONE: {
       const PolyconeP &p = *reinterpret_cast<const PolyconeP *>(rec);
       const PolySec *sec = reinterpret_cast<const PolySec *>(rec + p.sec_off);
@@ -649,6 +695,10 @@ bool reference_extent(int type, const double *rec, double lo[3], double hi[3]) {
       const SphereP &p = *reinterpret_cast<const SphereP *>(rec);
       return set(-p.rmax, -p.rmax, -p.rmax, p.rmax, p.rmax, p.rmax);
     }
+    case VGB_SHAPE_ORB: {  // source/UnplacedOrb.cpp:69-74
+      const OrbP &p = *reinterpret_cast<const OrbP *>(rec);
+      return set(-p.r, -p.r, -p.r, p.r, p.r, p.r);
+    }
     case VGB_SHAPE_TORUS:  // volumes/UnplacedTorus.h:178-180: the bounding tube's
       tube_extent(reinterpret_cast<const TorusP *>(rec)->btube, lo, hi);
       return true;
@@ -745,6 +795,23 @@ vgb_status vgb_unplaced_trd(vgb_geometry *g, double dx1, double dx2, double dy1,
     return set_error(VGB_EINVAL, "vgb_unplaced_trd: invalid half-lengths");
   TrdP t = make_trd(dx1, dx2, dy1, dy2, dz);
   return add_unplaced(g, VGB_SHAPE_TRD, &t, sizeof(t), 0, id);
+}
+
+vgb_status vgb_unplaced_orb(vgb_geometry *g, double r, int32_t *id) {
+  VGB_CHECK_OPEN(g);
+  if (!(r > 0)) return set_error(VGB_EINVAL, "vgb_unplaced_orb: radius must be > 0");
+  OrbP o = make_orb(r);
+  return add_unplaced(g, VGB_SHAPE_ORB, &o, sizeof(o), 0, id);
+}
+
+vgb_status vgb_unplaced_parallelepiped(vgb_geometry *g, double x, double y, double z,
+                                       double alpha_deg, double theta_deg, double phi_deg,
+                                       int32_t *id) {
+  VGB_CHECK_OPEN(g);
+  if (!(x > 0 && y > 0 && z > 0))
+    return set_error(VGB_EINVAL, "vgb_unplaced_parallelepiped: half-lengths must be > 0");
+  ParaP a = make_parallelepiped(x, y, z, alpha_deg, theta_deg, phi_deg);
+  return add_unplaced(g, VGB_SHAPE_PARALLELEPIPED, &a, sizeof(a), 0, id);
 }
 
 vgb_status vgb_unplaced_sphere(vgb_geometry *g, double rmin, double rmax, double sphi,

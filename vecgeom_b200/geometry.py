@@ -244,6 +244,13 @@ class Geometry:
     def UnplacedTrd(self, dx1, dx2, dy1, dy2, dz) -> int:
         return self._id(self.L.vgb_unplaced_trd, dx1, dx2, dy1, dy2, dz)
 
+    def UnplacedOrb(self, r) -> int:
+        return self._id(self.L.vgb_unplaced_orb, r)
+
+    def UnplacedParallelepiped(self, x, y, z, alpha, theta, phi) -> int:
+        """Half-lengths and the three angles in degrees, as the reference takes them."""
+        return self._id(self.L.vgb_unplaced_parallelepiped, x, y, z, alpha, theta, phi)
+
     def UnplacedBooleanVolume(self, op: int, left: PlacedVolume, right: PlacedVolume) -> int:
         return self._id(self.L.vgb_unplaced_boolean, op, left.id, right.id)
 

@@ -31,7 +31,8 @@ def isotropic(rng: np.random.Generator, n: int):
 @dataclass
 class ShapeSpec:
     """One unplaced shape: constructor arguments plus sampling helpers."""
-    kind: str                       # box, tube, cone, sphere, torus, polycone, polyhedron, boolsub, trd
+    kind: str                       # box, tube, cone, sphere, torus, polycone, polyhedron, boolsub,
+                                    # trd, orb, parallelepiped
     params: dict
     half: tuple                     # half extents of the axis-aligned bounding box
     center: tuple = (0., 0., 0.)
@@ -100,6 +101,29 @@ def torus_spec(rmin, rmax, rtor, sphi, dphi) -> ShapeSpec:
     R = rtor + rmax
     return ShapeSpec("torus", dict(rmin=rmin, rmax=rmax, rtor=rtor, sphi=sphi, dphi=dphi),
                      (R, R, rmax), contains=contains)
+
+
+def orb_spec(r) -> ShapeSpec:
+    def contains(x, y, z):
+        return x * x + y * y + z * z <= r * r
+    return ShapeSpec("orb", dict(r=r), (r, r, r), contains=contains)
+
+
+def parallelepiped_spec(x, y, z, alpha, theta, phi) -> ShapeSpec:
+    """Half-lengths x, y, z; alpha, theta, phi in degrees (the reference's
+    UnplacedParallelepiped arguments)."""
+    ta = math.tan(math.radians(alpha))
+    tt = math.tan(math.radians(theta))
+    tcp, tsp = tt * math.cos(math.radians(phi)), tt * math.sin(math.radians(phi))
+
+    def contains(px, py, pz):
+        ly = py - tsp * pz
+        lx = px - (tcp * pz + ta * ly)
+        return (np.abs(lx) <= x) & (np.abs(ly) <= y) & (np.abs(pz) <= z)
+    hy = y + abs(tsp) * z
+    hx = x + abs(tcp) * z + abs(ta) * hy
+    return ShapeSpec("parallelepiped", dict(x=x, y=y, z=z, alpha=alpha, theta=theta, phi=phi),
+                     (hx, hy, z), contains=contains)
 
 
 def trd_spec(dx1, dx2, dy1, dy2, dz) -> ShapeSpec:
@@ -350,6 +374,11 @@ def build_unplaced(geom, spec: ShapeSpec) -> int:
         return geom.UnplacedTorus(p["rmin"], p["rmax"], p["rtor"], p["sphi"], p["dphi"])
     if k == "trd":
         return geom.UnplacedTrd(p["dx1"], p["dx2"], p["dy1"], p["dy2"], p["dz"])
+    if k == "orb":
+        return geom.UnplacedOrb(p["r"])
+    if k == "parallelepiped":
+        return geom.UnplacedParallelepiped(p["x"], p["y"], p["z"], p["alpha"], p["theta"],
+                                           p["phi"])
     if k == "polycone":
         return geom.UnplacedPolycone(p["sphi"], p["dphi"], p["rmin"], p["rmax"], p["z"])
     if k == "polyhedron":
