@@ -77,7 +77,8 @@ typedef enum {
   VGB_SHAPE_BOOLEAN = 8,
   VGB_SHAPE_TRD = 9,
   VGB_SHAPE_ORB = 10,
-  VGB_SHAPE_PARALLELEPIPED = 11
+  VGB_SHAPE_PARALLELEPIPED = 11,
+  VGB_SHAPE_PARABOLOID = 12
 } vgb_shape_type;
 
 /* volumes/UnplacedBooleanVolume.h:10-14 */
@@ -138,6 +139,9 @@ vgb_status vgb_unplaced_orb(vgb_geometry *g, double r, int32_t *id);
 vgb_status vgb_unplaced_parallelepiped(vgb_geometry *g, double x, double y, double z,
                                        double alpha_deg, double theta_deg, double phi_deg,
                                        int32_t *id);
+/* UnplacedParaboloid(rlo, rhi, dz), source/UnplacedParaboloid.cpp:45-67 */
+vgb_status vgb_unplaced_paraboloid(vgb_geometry *g, double rlo, double rhi, double dz,
+                                   int32_t *id);
 /* volumes/UnplacedBooleanVolume.h:46 (left/right are placed-volume ids) */
 vgb_status vgb_unplaced_boolean(vgb_geometry *g, int32_t op, int32_t left_placed,
                                 int32_t right_placed, int32_t *id);

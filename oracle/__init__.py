@@ -114,6 +114,8 @@ class RefLib:
         L.vgref_orb.argtypes = [_d]
         L.vgref_parallelepiped.restype = _vp
         L.vgref_parallelepiped.argtypes = [_d] * 6
+        L.vgref_paraboloid.restype = _vp
+        L.vgref_paraboloid.argtypes = [_d] * 3
         L.vgref_polycone.restype = _vp
         L.vgref_polycone.argtypes = [_d, _d, _i, _vp, _vp, _vp]
         L.vgref_polyhedron.restype = _vp
@@ -318,6 +320,8 @@ def ref_unplaced(ref: RefLib, spec):
         return L.vgref_trd(p["dx1"], p["dx2"], p["dy1"], p["dy2"], p["dz"])
     if k == "orb":
         return L.vgref_orb(p["r"])
+    if k == "paraboloid":
+        return L.vgref_paraboloid(p["rlo"], p["rhi"], p["dz"])
     if k == "parallelepiped":
         return L.vgref_parallelepiped(p["x"], p["y"], p["z"], p["alpha"], p["theta"], p["phi"])
     if k in ("polycone", "polyhedron"):

@@ -7,7 +7,7 @@
 //
 // Every entry point builds or calls the reference's own objects:
 //   - shapes: Unplaced{Box,Tube,Cone,Sphere,Torus,Polycone,Polyhedron,Trd,Orb,
-//     Parallelepiped,BooleanVolume} constructors (volumes/Unplaced*.h),
+//     Parallelepiped,Paraboloid,BooleanVolume} constructors (volumes/Unplaced*.h),
 //   - placement: LogicalVolume::Place / PlaceDaughter (source/LogicalVolume.cpp:60-102),
 //   - batch ops: the VPlacedVolume SOA3D virtuals (volumes/PlacedVolume.h:145-250),
 //   - navigation: SimpleNavigator (navigation/SimpleNavigator.h:204-743).
@@ -26,6 +26,7 @@
 #include "volumes/Trd.h"
 #include "volumes/Orb.h"
 #include "volumes/Parallelepiped.h"
+#include "volumes/Paraboloid.h"
 #include "volumes/BooleanVolume.h"
 #include "management/GeoManager.h"
 #include "navigation/NavigationState.h"
@@ -164,6 +165,9 @@ void *vgref_orb(double r) {
 }
 void *vgref_parallelepiped(double x, double y, double z, double alpha, double theta, double phi) {
   return new UnplacedParallelepiped(x, y, z, alpha, theta, phi);
+}
+void *vgref_paraboloid(double rlo, double rhi, double dz) {
+  return new UnplacedParaboloid(rlo, rhi, dz);
 }
 void *vgref_trd(double x1, double x2, double y1, double y2, double z) {
   return new UnplacedTrd(x1, x2, y1, y2, z);

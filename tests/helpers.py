@@ -152,6 +152,9 @@ def shape_specs() -> dict:
     s["parallelepiped"] = W.parallelepiped_spec(20., 30., 40., 30., 20., 40.)
     s["parallelepipedneg"] = W.parallelepiped_spec(15., 10., 25., -45., 35., 200.)
     s["parallelepipedbox"] = W.parallelepiped_spec(12., 8., 5., 0., 0., 0.)
+    s["paraboloid"] = W.paraboloid_spec(10., 30., 40.)
+    s["paraboloidinv"] = W.paraboloid_spec(25., 5., 20.)
+    s["paraboloidtip"] = W.paraboloid_spec(0., 15., 30.)
     s["boolsubxf"] = W.boolsub_spec((30., 30., 30.), 15., 40., left_place=(2., -1., 3., 0., 0., 15.),
                                     right_place=(5., 0., -4., 0., 90., 0.))
     return s

@@ -34,7 +34,7 @@ def spec_from_meta(meta):
             "sphere": W.sphere_spec, "torus": W.torus_spec, "trd": W.trd_spec,
             "polycone": W.polycone_spec, "polyhedron": W.polyhedron_spec,
             "boolsub": W.boolsub_spec, "orb": W.orb_spec,
-            "parallelepiped": W.parallelepiped_spec}[k]
+            "parallelepiped": W.parallelepiped_spec, "paraboloid": W.paraboloid_spec}[k]
     return ctor(**p)
 
 

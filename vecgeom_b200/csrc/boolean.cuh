@@ -60,7 +60,8 @@ constexpr int kBoolMaxRounds = 4096;
   X(VGB_SHAPE_POLYCONE, vgb::PolyconeOps, vgb::PolyconeP)    \
   X(VGB_SHAPE_POLYHEDRON, vgb::PolyhedronOps, vgb::PolyhedronP)      \
   X(VGB_SHAPE_ORB, vgb::OrbOps, vgb::OrbP)                            \
-  X(VGB_SHAPE_PARALLELEPIPED, vgb::ParaOps, vgb::ParaP)
+  X(VGB_SHAPE_PARALLELEPIPED, vgb::ParaOps, vgb::ParaP)               \
+  X(VGB_SHAPE_PARABOLOID, vgb::ParaboloidOps, vgb::ParaboloidP)
 
 template <class P> VGB_HD P comp_params(const double *rec) {
   return bind_params(*reinterpret_cast<const P *>(rec), rec);

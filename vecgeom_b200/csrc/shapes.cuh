@@ -13,6 +13,7 @@
 #include "polyhedron.cuh"
 #include "orb.cuh"
 #include "parallelepiped.cuh"
+#include "paraboloid.cuh"
 
 struct vgb_geometry;
 

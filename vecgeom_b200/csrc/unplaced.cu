@@ -227,6 +227,26 @@ ParaP make_parallelepiped(double x, double y, double z, double alpha, double the
   return a;
 }
 
+// UnplacedParaboloid(rlo, rhi, dz) -> SetRloAndRhiAndDz
+// (source/UnplacedParaboloid.cpp:90-128) and ComputeBoundingBox (:242-245)
+ParaboloidP make_paraboloid(double rlo, double rhi, double dz) {
+  ParaboloidP q;
+  std::memset(&q, 0, sizeof(q));
+  q.rlo = rlo;
+  q.rhi = rhi;
+  q.rlo2 = rlo * rlo;
+  q.rhi2 = rhi * rhi;
+  q.dz = dz;
+  const double dd = 1. / (q.rhi2 - q.rlo2);
+  q.a = 2. * dz * dd;
+  q.b = -dz * (q.rlo2 + q.rhi2) * dd;
+  q.ainv = 1 / q.a;
+  q.a2 = q.a * q.a;
+  q.tolOz = dz + kHalfTolerance;
+  q.dx = vmax(rhi, rlo);
+  return q;
+}
+
 // UnplacedTrd::calculateCached (volumes/UnplacedTrd.h:38-51)
 TrdP make_trd(double dx1, double dx2, double dy1, double dy2, double dz) {
   TrdP t;
@@ -579,6 +599,10 @@ bool shape_bbox(const vgb_geometry *g, int32_t u, double b[6]) {
       const OrbP &p = *reinterpret_cast<const OrbP *>(rec);
       return sym(p.rTolO, p.rTolO, p.rTolO);
     }
+    case VGB_SHAPE_PARABOLOID: {
+      const ParaboloidP &p = *reinterpret_cast<const ParaboloidP *>(rec);
+      return sym(p.dx, p.dx, p.dz);
+    }
     case VGB_SHAPE_PARALLELEPIPED: {
       // the box's corners mapped back through the shear
       const ParaP &p = *reinterpret_cast<const ParaP *>(rec);
@@ -694,6 +718,10 @@ bool reference_extent(int type, const double *rec, double lo[3], double hi[3]) {
     case VGB_SHAPE_SPHERE: {  // source/UnplacedSphere.cpp:174-179
       const SphereP &p = *reinterpret_cast<const SphereP *>(rec);
       return set(-p.rmax, -p.rmax, -p.rmax, p.rmax, p.rmax, p.rmax);
+    }
+    case VGB_SHAPE_PARABOLOID: {  // source/UnplacedParaboloid.cpp:169-176
+      const ParaboloidP &p = *reinterpret_cast<const ParaboloidP *>(rec);
+      return set(-p.dx, -p.dx, -p.dz, p.dx, p.dx, p.dz);
     }
     case VGB_SHAPE_ORB: {  // source/UnplacedOrb.cpp:69-74
       const OrbP &p = *reinterpret_cast<const OrbP *>(rec);
@@ -812,6 +840,17 @@ vgb_status vgb_unplaced_parallelepiped(vgb_geometry *g, double x, double y, doub
     return set_error(VGB_EINVAL, "vgb_unplaced_parallelepiped: half-lengths must be > 0");
   ParaP a = make_parallelepiped(x, y, z, alpha_deg, theta_deg, phi_deg);
   return add_unplaced(g, VGB_SHAPE_PARALLELEPIPED, &a, sizeof(a), 0, id);
+}
+
+vgb_status vgb_unplaced_paraboloid(vgb_geometry *g, double rlo, double rhi, double dz,
+                                   int32_t *id) {
+  VGB_CHECK_OPEN(g);
+  // the reference prints an error and keeps zeros for these
+  // (source/UnplacedParaboloid.cpp:93-96); here they are refused
+  if (!(rlo >= 0 && rhi >= 0 && dz > 0 && rhi != rlo))
+    return set_error(VGB_EINVAL, "vgb_unplaced_paraboloid: need rlo, rhi >= 0, rlo != rhi, dz > 0");
+  ParaboloidP q = make_paraboloid(rlo, rhi, dz);
+  return add_unplaced(g, VGB_SHAPE_PARABOLOID, &q, sizeof(q), 0, id);
 }
 
 vgb_status vgb_unplaced_sphere(vgb_geometry *g, double rmin, double rmax, double sphi,

@@ -251,6 +251,9 @@ class Geometry:
         """Half-lengths and the three angles in degrees, as the reference takes them."""
         return self._id(self.L.vgb_unplaced_parallelepiped, x, y, z, alpha, theta, phi)
 
+    def UnplacedParaboloid(self, rlo, rhi, dz) -> int:
+        return self._id(self.L.vgb_unplaced_paraboloid, rlo, rhi, dz)
+
     def UnplacedBooleanVolume(self, op: int, left: PlacedVolume, right: PlacedVolume) -> int:
         return self._id(self.L.vgb_unplaced_boolean, op, left.id, right.id)
 

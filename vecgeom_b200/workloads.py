@@ -32,7 +32,7 @@ def isotropic(rng: np.random.Generator, n: int):
 class ShapeSpec:
     """One unplaced shape: constructor arguments plus sampling helpers."""
     kind: str                       # box, tube, cone, sphere, torus, polycone, polyhedron, boolsub,
-                                    # trd, orb, parallelepiped
+                                    # trd, orb, parallelepiped, paraboloid
     params: dict
     half: tuple                     # half extents of the axis-aligned bounding box
     center: tuple = (0., 0., 0.)
@@ -124,6 +124,16 @@ def parallelepiped_spec(x, y, z, alpha, theta, phi) -> ShapeSpec:
     hx = x + abs(tcp) * z + abs(ta) * hy
     return ShapeSpec("parallelepiped", dict(x=x, y=y, z=z, alpha=alpha, theta=theta, phi=phi),
                      (hx, hy, z), contains=contains)
+
+
+def paraboloid_spec(rlo, rhi, dz) -> ShapeSpec:
+    a = 2. * dz / (rhi * rhi - rlo * rlo)
+    b = -dz * (rlo * rlo + rhi * rhi) / (rhi * rhi - rlo * rlo)
+
+    def contains(x, y, z):
+        return (np.abs(z) <= dz) & (z >= a * (x * x + y * y) + b)
+    h = max(rlo, rhi)
+    return ShapeSpec("paraboloid", dict(rlo=rlo, rhi=rhi, dz=dz), (h, h, dz), contains=contains)
 
 
 def trd_spec(dx1, dx2, dy1, dy2, dz) -> ShapeSpec:
@@ -376,6 +386,8 @@ def build_unplaced(geom, spec: ShapeSpec) -> int:
         return geom.UnplacedTrd(p["dx1"], p["dx2"], p["dy1"], p["dy2"], p["dz"])
     if k == "orb":
         return geom.UnplacedOrb(p["r"])
+    if k == "paraboloid":
+        return geom.UnplacedParaboloid(p["rlo"], p["rhi"], p["dz"])
     if k == "parallelepiped":
         return geom.UnplacedParallelepiped(p["x"], p["y"], p["z"], p["alpha"], p["theta"],
                                            p["phi"])
