@@ -332,13 +332,13 @@ def ref_unplaced(ref: RefLib, spec):
                                     rmin.ctypes.data, rmax.ctypes.data)
         return L.vgref_polyhedron(p["phi_start_deg"], p["phi_delta_deg"], p["sides"], len(z),
                                   z.ctypes.data, rmin.ctypes.data, rmax.ctypes.data)
-    if k == "boolsub":
+    if k in ("boolsub", "boolunion", "boolinter"):
         bx, by, bz = p["box_half"]
         ident = (0., 0., 0., 0., 0., 0.)
         left = ref.placed(L.vgref_box(bx, by, bz), *p.get("left_place", ident), label="sub_box")
         right = ref.placed(L.vgref_tube(0., p["tube_rmax"], p["tube_dz"], 0., 2 * math.pi),
                            *p.get("right_place", ident), label="sub_tube")
-        return L.vgref_boolean(2, left, right)
+        return L.vgref_boolean({"boolunion": 0, "boolinter": 1, "boolsub": 2}[k], left, right)
     raise ValueError(k)
 
 

@@ -155,6 +155,18 @@ def shape_specs() -> dict:
     s["paraboloid"] = W.paraboloid_spec(10., 30., 40.)
     s["paraboloidinv"] = W.paraboloid_spec(25., 5., 20.)
     s["paraboloidtip"] = W.paraboloid_spec(0., 15., 30.)
+    s["boolunion"] = W.boolean_spec("boolunion", (20., 20., 20.), 12., 35.,
+                                    right_place=(8., 0., 0., 0., 0., 0.))
+    # (a union's left component stays at identity: the reference's union
+    # DistanceToOut hands the left component the boolean-frame point, and with
+    # a placed left component its walk does not end)
+    s["boolunionxf"] = W.boolean_spec("boolunion", (15., 25., 10.), 10., 30.,
+                                      right_place=(-5., 0., 2., 20., 90., 30.))
+    s["boolinter"] = W.boolean_spec("boolinter", (20., 20., 20.), 15., 30.,
+                                    right_place=(6., 0., 0., 0., 0., 0.))
+    s["boolinterxf"] = W.boolean_spec("boolinter", (25., 20., 15.), 18., 40.,
+                                      left_place=(2., -1., 3., 0., 0., 15.),
+                                      right_place=(0., 2., 0., 0., 90., 30.))
     s["boolsubxf"] = W.boolsub_spec((30., 30., 30.), 15., 40., left_place=(2., -1., 3., 0., 0., 15.),
                                     right_place=(5., 0., -4., 0., 90., 0.))
     return s

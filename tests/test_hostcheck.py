@@ -26,7 +26,7 @@ SO = os.path.join(ROOT, "_build", "hostcheck", "libvgb_hostcheck.so")
 GOLDEN = sorted(glob.glob(os.path.join(HERE, "golden", "*.npz")))
 HOST_SHAPES = {"box", "tube", "cone", "sphere", "trd", "torus", "polycone", "polyhedron", "orb",
                "parallelepiped", "paraboloid",
-               "boolsub"}
+               "boolsub", "boolunion", "boolinter"}
 
 
 @pytest.fixture(scope="module")

@@ -20,7 +20,7 @@ from test_oracle_golden import load_case, spec_from_meta
 HERE = os.path.dirname(os.path.abspath(__file__))
 GOLDEN = sorted(glob.glob(os.path.join(HERE, "golden", "*.npz")))
 VGB_SHAPES = {"box", "tube", "cone", "sphere", "trd", "torus", "polycone", "polyhedron", "boolsub",
-              "orb", "parallelepiped", "paraboloid"}
+              "orb", "parallelepiped", "paraboloid", "boolunion", "boolinter"}
 
 pytestmark = pytest.mark.gpu
 

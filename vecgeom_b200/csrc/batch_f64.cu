@@ -63,9 +63,9 @@ static vgb_status launch_fused(const P &prm, const DXform &X, const FusedIO &io,
 // switch over primitive shapes for every other pair.
 template <class F> static vgb_status with_boolean_ops(const BooleanP &b, F &&f) {
   const int lt = b.left.type, rt = b.right.type;
-  if (lt == VGB_SHAPE_BOX && rt == VGB_SHAPE_TUBE) return f(BoolSubBoxTube<double>{});
-  if (lt == VGB_SHAPE_BOX && rt == VGB_SHAPE_BOX) return f(BoolSubBoxBox<double>{});
-  return f(BoolSubOps<double>{});
+  if (lt == VGB_SHAPE_BOX && rt == VGB_SHAPE_TUBE) return f(BoolBoxTube<double>{});
+  if (lt == VGB_SHAPE_BOX && rt == VGB_SHAPE_BOX) return f(BoolBoxBox<double>{});
+  return f(BoolOps<double>{});
 }
 
 static BooleanP boolean_params(const vgb_geometry *g, int32_t unplaced) {

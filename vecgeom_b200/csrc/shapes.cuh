@@ -64,4 +64,4 @@ vgb_status finalize_shapes(vgb_geometry *g);
 // (type, ops template, parameter record) of every shape with batch kernels
 #define VGB_FOR_EACH_SHAPE(X)                                 \
   VGB_FOR_EACH_PRIMITIVE(X)                                   \
-  X(VGB_SHAPE_BOOLEAN, vgb::BoolSubOps, vgb::BooleanP)
+  X(VGB_SHAPE_BOOLEAN, vgb::BoolOps, vgb::BooleanP)

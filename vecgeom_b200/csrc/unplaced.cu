@@ -635,26 +635,32 @@ bool shape_bbox(const vgb_geometry *g, int32_t u, double b[6]) {
       return true;
     }
     case VGB_SHAPE_BOOLEAN: {
-      // the left component's box, moved into the boolean's frame
+      // the components' boxes moved into the boolean's frame: the left one
+      // encloses a subtraction or an intersection, both enclose a union
       const BooleanP &p = *reinterpret_cast<const BooleanP *>(rec);
-      if (p.left.xf.flags & kXfQuirk16A) return false;  // not a rigid motion
-      const int32_t loff = r.param_off + p.left.rec_off;
-      int32_t left = -1;
-      for (size_t k = 0; k < g->unplaced.size(); ++k)
-        if (g->unplaced[k].param_off == loff) left = (int32_t)k;
-      double lb[6];
-      if (left < 0 || !shape_bbox(g, left, lb)) return false;
       b[0] = b[1] = b[2] = 1e300;
       b[3] = b[4] = b[5] = -1e300;
-      for (int c = 0; c < 8; ++c) {
-        const V3<double> l = {lb[(c & 1) ? 3 : 0], lb[(c & 2) ? 4 : 1], lb[(c & 4) ? 5 : 2]};
-        const V3<double> m = xf_inverse_point(p.left.xf, l);
-        const double v[3] = {m.x, m.y, m.z};
-        for (int k = 0; k < 3; ++k) {
-          b[k] = std::min(b[k], v[k]);
-          b[3 + k] = std::max(b[3 + k], v[k]);
+      auto add = [&](const BoolComp &c) {
+        if (c.xf.flags & kXfQuirk16A) return false;  // not a rigid motion
+        const int32_t off = r.param_off + c.rec_off;
+        int32_t u = -1;
+        for (size_t k = 0; k < g->unplaced.size(); ++k)
+          if (g->unplaced[k].param_off == off) u = (int32_t)k;
+        double cb[6];
+        if (u < 0 || !shape_bbox(g, u, cb)) return false;
+        for (int q = 0; q < 8; ++q) {
+          const V3<double> l = {cb[(q & 1) ? 3 : 0], cb[(q & 2) ? 4 : 1], cb[(q & 4) ? 5 : 2]};
+          const V3<double> m = xf_inverse_point(c.xf, l);
+          const double v[3] = {m.x, m.y, m.z};
+          for (int k = 0; k < 3; ++k) {
+            b[k] = std::min(b[k], v[k]);
+            b[3 + k] = std::max(b[3 + k], v[k]);
+          }
         }
-      }
+        return true;
+      };
+      if (!add(p.left)) return false;
+      if (p.op == VGB_BOOL_UNION && !add(p.right)) return false;
       return true;
     }
     default:
@@ -756,11 +762,26 @@ bool reference_extent(int type, const double *rec, double lo[3], double hi[3]) {
       return true;
     }
     case VGB_SHAPE_BOOLEAN: {
-      // source/UnplacedBooleanVolume.cpp:94-121: a subtraction's extent is its
-      // left component's, in the component's own frame (the placement of the
-      // component is not applied)
+      // source/UnplacedBooleanVolume.cpp:94-121: from the components' extents
+      // in their own frames (their placements are not applied): a
+      // subtraction's is its left component's, a union's the enclosing box of
+      // both, an intersection's their overlap (Min / Max of the bounds)
       const BooleanP &p = *reinterpret_cast<const BooleanP *>(rec);
-      return reference_extent(p.left.type, rec + p.left.rec_off, lo, hi);
+      double rlo[3], rhi[3];
+      if (!reference_extent(p.left.type, rec + p.left.rec_off, lo, hi)) return false;
+      if (!reference_extent(p.right.type, rec + p.right.rec_off, rlo, rhi)) return false;
+      if (p.op == VGB_BOOL_UNION) {
+        for (int k = 0; k < 3; ++k) {
+          lo[k] = vmin(lo[k], rlo[k]);
+          hi[k] = vmax(hi[k], rhi[k]);
+        }
+      } else if (p.op == VGB_BOOL_INTERSECTION) {
+        for (int k = 0; k < 3; ++k) {
+          lo[k] = vmax(lo[k], rlo[k]);
+          hi[k] = vmin(hi[k], rhi[k]);
+        }
+      }
+      return true;
     }
     default:
       return false;
@@ -902,9 +923,8 @@ vgb_status vgb_unplaced_tube(vgb_geometry *g, double rmin, double rmax, double d
 vgb_status vgb_unplaced_boolean(vgb_geometry *g, int32_t op, int32_t left_placed,
                                 int32_t right_placed, int32_t *id) {
   VGB_CHECK_OPEN(g);
-  if (op != VGB_BOOL_SUBTRACTION)
-    return set_error(VGB_ENOTSUP, "vgb_unplaced_boolean: only subtraction (op %d) is available",
-                     (int)VGB_BOOL_SUBTRACTION);
+  if (op != VGB_BOOL_SUBTRACTION && op != VGB_BOOL_UNION && op != VGB_BOOL_INTERSECTION)
+    return set_error(VGB_EINVAL, "vgb_unplaced_boolean: unknown operation %d", op);
   const int32_t np = (int32_t)g->placed.size();
   if (left_placed < 0 || left_placed >= np || right_placed < 0 || right_placed >= np)
     return set_error(VGB_EINVAL, "vgb_unplaced_boolean: unknown placed volume");

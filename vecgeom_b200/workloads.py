@@ -248,6 +248,29 @@ def boolsub_spec(box_half, tube_rmax, tube_dz, left_place=IDENTITY_PLACE,
     return ShapeSpec("boolsub", params, extent, contains=contains)
 
 
+# operation codes of UnplacedBooleanVolume (volumes/UnplacedBooleanVolume.h:10-14)
+BOOL_OPS = {"boolunion": 0, "boolinter": 1, "boolsub": 2}
+
+
+def boolean_spec(kind, box_half, tube_rmax, tube_dz, left_place=IDENTITY_PLACE,
+                 right_place=IDENTITY_PLACE) -> ShapeSpec:
+    """Box union / intersection with a full solid tube (kind "boolunion" or
+    "boolinter"), each component at its own placement."""
+    bx, by, bz = box_half
+
+    def contains(x, y, z):
+        lx, ly, lz = to_local(left_place, x, y, z)
+        inbox = (np.abs(lx) <= bx) & (np.abs(ly) <= by) & (np.abs(lz) <= bz)
+        rx, ry, rz = to_local(right_place, x, y, z)
+        intube = (rx * rx + ry * ry <= tube_rmax * tube_rmax) & (np.abs(rz) <= tube_dz)
+        return (inbox | intube) if kind == "boolunion" else (inbox & intube)
+    params = dict(box_half=box_half, tube_rmax=tube_rmax, tube_dz=tube_dz,
+                  left_place=list(left_place), right_place=list(right_place))
+    e = max(float(np.linalg.norm(box_half)) + float(np.linalg.norm(left_place[:3])),
+            float(np.hypot(tube_rmax, tube_dz)) + float(np.linalg.norm(right_place[:3])))
+    return ShapeSpec(kind, params, (e, e, e), contains=contains)
+
+
 # ---------------------------------------------------------------------------
 # point sets
 # ---------------------------------------------------------------------------
@@ -396,14 +419,14 @@ def build_unplaced(geom, spec: ShapeSpec) -> int:
     if k == "polyhedron":
         return geom.UnplacedPolyhedron(p["phi_start_deg"], p["phi_delta_deg"], p["sides"],
                                        p["z"], p["rmin"], p["rmax"])
-    if k == "boolsub":
+    if k in BOOL_OPS:
         bx, by, bz = p["box_half"]
         lb = geom.LogicalVolume("sub_box", geom.UnplacedBox(bx, by, bz))
         lt = geom.LogicalVolume("sub_tube", geom.UnplacedTube(0., p["tube_rmax"], p["tube_dz"],
                                                               0., 2 * math.pi))
         left = lb.Place(geom.Transformation3D(*p.get("left_place", IDENTITY_PLACE)))
         right = lt.Place(geom.Transformation3D(*p.get("right_place", IDENTITY_PLACE)))
-        return geom.UnplacedBooleanVolume(2, left, right)
+        return geom.UnplacedBooleanVolume(BOOL_OPS[k], left, right)
     raise ValueError(k)
 
 
