@@ -192,6 +192,39 @@ class Geometry {
                                   &id));
     return id;
   }
+  int UnplacedOrb(double r) {
+    int32_t id;
+    check(vgb_unplaced_orb(g_, r, &id));
+    return id;
+  }
+  // alpha, theta, phi in degrees (volumes/UnplacedParallelepiped.h:34)
+  int UnplacedParallelepiped(double x, double y, double z, double alpha, double theta,
+                             double phi) {
+    int32_t id;
+    check(vgb_unplaced_parallelepiped(g_, x, y, z, alpha, theta, phi, &id));
+    return id;
+  }
+  int UnplacedParaboloid(double rlo, double rhi, double dz) {
+    int32_t id;
+    check(vgb_unplaced_paraboloid(g_, rlo, rhi, dz, &id));
+    return id;
+  }
+  // theta, phi in radians (volumes/UnplacedTrapezoid.h:93-95)
+  int UnplacedTrapezoid(double dz, double theta, double phi, double dy1, double dx1, double dx2,
+                        double tan_alpha1, double dy2, double dx3, double dx4,
+                        double tan_alpha2) {
+    int32_t id;
+    check(vgb_unplaced_trapezoid(g_, dz, theta, phi, dy1, dx1, dx2, tan_alpha1, dy2, dx3, dx4,
+                                 tan_alpha2, &id));
+    return id;
+  }
+  // corners[24]: 8 corners (x, y, z), 0-3 at z = -dz, 4-7 at z = +dz
+  // (volumes/UnplacedTrapezoid.h:103)
+  int UnplacedTrapezoid(const double *corners) {
+    int32_t id;
+    check(vgb_unplaced_trapezoid_corners(g_, corners, &id));
+    return id;
+  }
   int UnplacedBooleanVolume(int op, const VPlacedVolume &left, const VPlacedVolume &right) {
     int32_t id;
     check(vgb_unplaced_boolean(g_, op, left.id(), right.id(), &id));

@@ -78,7 +78,8 @@ typedef enum {
   VGB_SHAPE_TRD = 9,
   VGB_SHAPE_ORB = 10,
   VGB_SHAPE_PARALLELEPIPED = 11,
-  VGB_SHAPE_PARABOLOID = 12
+  VGB_SHAPE_PARABOLOID = 12,
+  VGB_SHAPE_TRAPEZOID = 13
 } vgb_shape_type;
 
 /* volumes/UnplacedBooleanVolume.h:10-14 */
@@ -142,6 +143,16 @@ vgb_status vgb_unplaced_parallelepiped(vgb_geometry *g, double x, double y, doub
 /* UnplacedParaboloid(rlo, rhi, dz), source/UnplacedParaboloid.cpp:45-67 */
 vgb_status vgb_unplaced_paraboloid(vgb_geometry *g, double rlo, double rhi, double dz,
                                    int32_t *id);
+/* volumes/UnplacedTrapezoid.h:93-95, UnplacedTrapezoid(pDz, pTheta, pPhi, pDy1,
+   pDx1, pDx2, pTanAlpha1, pDy2, pDx3, pDx4, pTanAlpha2); theta, phi in radians */
+vgb_status vgb_unplaced_trapezoid(vgb_geometry *g, double dz, double theta, double phi,
+                                  double dy1, double dx1, double dx2, double tan_alpha1,
+                                  double dy2, double dx3, double dx4, double tan_alpha2,
+                                  int32_t *id);
+/* volumes/UnplacedTrapezoid.h:103, UnplacedTrapezoid(TrapCorners_t): corners[24] =
+   8 corners (x, y, z), 0-3 at z = -dz, 4-7 at z = +dz, in the reference's order */
+vgb_status vgb_unplaced_trapezoid_corners(vgb_geometry *g, const double *corners,
+                                          int32_t *id);
 /* volumes/UnplacedBooleanVolume.h:46 (left/right are placed-volume ids) */
 vgb_status vgb_unplaced_boolean(vgb_geometry *g, int32_t op, int32_t left_placed,
                                 int32_t right_placed, int32_t *id);

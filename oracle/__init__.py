@@ -116,6 +116,10 @@ class RefLib:
         L.vgref_parallelepiped.argtypes = [_d] * 6
         L.vgref_paraboloid.restype = _vp
         L.vgref_paraboloid.argtypes = [_d] * 3
+        L.vgref_trapezoid.restype = _vp
+        L.vgref_trapezoid.argtypes = [_d] * 11
+        L.vgref_trapezoid_corners.restype = _vp
+        L.vgref_trapezoid_corners.argtypes = [_vp]
         L.vgref_polycone.restype = _vp
         L.vgref_polycone.argtypes = [_d, _d, _i, _vp, _vp, _vp]
         L.vgref_polyhedron.restype = _vp
@@ -322,6 +326,12 @@ def ref_unplaced(ref: RefLib, spec):
         return L.vgref_orb(p["r"])
     if k == "paraboloid":
         return L.vgref_paraboloid(p["rlo"], p["rhi"], p["dz"])
+    if k == "trapezoid":
+        return L.vgref_trapezoid(p["dz"], p["theta"], p["phi"], p["dy1"], p["dx1"], p["dx2"],
+                                 p["tan_alpha1"], p["dy2"], p["dx3"], p["dx4"], p["tan_alpha2"])
+    if k == "trapezoidcorners":
+        c = np.ascontiguousarray(p["corners"], np.float64)
+        return L.vgref_trapezoid_corners(c.ctypes.data)
     if k == "parallelepiped":
         return L.vgref_parallelepiped(p["x"], p["y"], p["z"], p["alpha"], p["theta"], p["phi"])
     if k in ("polycone", "polyhedron"):

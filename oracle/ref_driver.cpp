@@ -7,7 +7,8 @@
 //
 // Every entry point builds or calls the reference's own objects:
 //   - shapes: Unplaced{Box,Tube,Cone,Sphere,Torus,Polycone,Polyhedron,Trd,Orb,
-//     Parallelepiped,Paraboloid,BooleanVolume} constructors (volumes/Unplaced*.h),
+//     Parallelepiped,Paraboloid,Trapezoid,BooleanVolume} constructors
+//     (volumes/Unplaced*.h),
 //   - placement: LogicalVolume::Place / PlaceDaughter (source/LogicalVolume.cpp:60-102),
 //   - batch ops: the VPlacedVolume SOA3D virtuals (volumes/PlacedVolume.h:145-250),
 //   - navigation: SimpleNavigator (navigation/SimpleNavigator.h:204-743).
@@ -27,6 +28,7 @@
 #include "volumes/Orb.h"
 #include "volumes/Parallelepiped.h"
 #include "volumes/Paraboloid.h"
+#include "volumes/Trapezoid.h"
 #include "volumes/BooleanVolume.h"
 #include "management/GeoManager.h"
 #include "navigation/NavigationState.h"
@@ -168,6 +170,15 @@ void *vgref_parallelepiped(double x, double y, double z, double alpha, double th
 }
 void *vgref_paraboloid(double rlo, double rhi, double dz) {
   return new UnplacedParaboloid(rlo, rhi, dz);
+}
+void *vgref_trapezoid(double dz, double theta, double phi, double dy1, double dx1, double dx2,
+                      double ta1, double dy2, double dx3, double dx4, double ta2) {
+  return new UnplacedTrapezoid(dz, theta, phi, dy1, dx1, dx2, ta1, dy2, dx3, dx4, ta2);
+}
+void *vgref_trapezoid_corners(const double *c) {
+  TrapCorners_t pt;
+  for (int k = 0; k < 8; ++k) pt[k] = Vector3D<Precision>(c[3 * k], c[3 * k + 1], c[3 * k + 2]);
+  return new UnplacedTrapezoid(pt);
 }
 void *vgref_trd(double x1, double x2, double y1, double y2, double z) {
   return new UnplacedTrd(x1, x2, y1, y2, z);

@@ -155,6 +155,16 @@ def shape_specs() -> dict:
     s["paraboloid"] = W.paraboloid_spec(10., 30., 40.)
     s["paraboloidinv"] = W.paraboloid_spec(25., 5., 20.)
     s["paraboloidtip"] = W.paraboloid_spec(0., 15., 30.)
+    # trapezoids: slanted (theta, phi, alpha; planar faces need equal alphas and
+    # (dx1 - dx2) / dy1 = (dx3 - dx4) / dy2), with negative angles, box-like
+    # (test/unit_tests/TestTrap.cpp:59 "Test Boxlike #1"), and from the corners
+    # of TestTrap.cpp:51-58 ("Test Trdlike #2")
+    s["trapezoid"] = W.trapezoid_spec(40., 0.3, 0.7, 20., 10., 15., 0.2, 30., 20., 27.5, 0.2)
+    s["trapezoidneg"] = W.trapezoid_spec(25., -0.4, 2.5, 10., 8., 6., -0.3, 15., 12., 9., -0.3)
+    s["trapezoidbox"] = W.trapezoid_spec(40., 0., 0., 30., 20., 20., 0., 30., 20., 20., 0.)
+    s["trapezoidtrd"] = W.trapezoid_corners_spec(
+        [(-10., -20., -40.), (10., -20., -40.), (-10., 20., -40.), (10., 20., -40.),
+         (-30., -40., 40.), (30., -40., 40.), (-30., 40., 40.), (30., 40., 40.)])
     s["boolunion"] = W.boolean_spec("boolunion", (20., 20., 20.), 12., 35.,
                                     right_place=(8., 0., 0., 0., 0., 0.))
     # (a union's left component stays at identity: the reference's union

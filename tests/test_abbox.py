@@ -3,8 +3,10 @@ against the reference, and SimpleNavigator on the mixed-shape geometry.
 
 Fixtures (tests/golden/make_nav_golden.py, written by the reference):
 detector_abbox / zoo_abbox / row_abbox (ABBoxNavigator traces), zoo
-(SimpleNavigator on the mixed-shape geometry), zoo_boxes (ComputeABBox of all
-nine shape types under random placements).  Records must match bit for bit:
+(SimpleNavigator on the mixed-shape geometry), zoo2 / zoo2_abbox (both
+navigators on the second mixed geometry: orb, parallelepiped, paraboloid,
+trapezoids, union, intersection), zoo_boxes (ComputeABBox of all nine shape
+types under random placements).  Records must match bit for bit:
   * CPU: the navigators of navigation.cuh / abbox.cuh built for the host, with
     the shared hit list large (sorted walk) and tiny (one-by-one walk);
   * GPU: vgb_abbox_nav_trace / vgb_abbox_nav_find_next_boundary_and_step and
@@ -24,7 +26,7 @@ from vecgeom_b200 import workloads as W
 from vecgeom_b200.geometry import ComputeABBox
 
 HAVE_REF = oracle.RefLib.available()
-FIXTURES = ["detector_abbox", "zoo_abbox", "row_abbox", "zoo"]
+FIXTURES = ["detector_abbox", "zoo_abbox", "row_abbox", "zoo", "zoo2", "zoo2_abbox"]
 
 
 def want_of(d):
@@ -59,6 +61,16 @@ def test_trd_extent_keeps_the_reference_typo(hc):
     g.SetWorld(world.Place(g.Transformation3D()))
     lo_hi = ComputeABBox(g, pv)
     assert lo_hi[0] == -30. - 1e-3 and lo_hi[3] == 10. + 1e-3  # max(dy1=5, dx2=10), not 30
+
+
+@pytest.mark.skipif(not HAVE_REF, reason="oracle/_ref not built")
+def test_abbox_boxes_match_reference_zoo2(hc):
+    """ComputeABBox of orb, paraboloid, trapezoids (their Extents), union and
+    intersection under random rotations."""
+    g, placed = build(hc, "zoo2_abbox", close=False)
+    got = np.array([ComputeABBox(g, p) for p in placed])
+    want = reference_boxes_isolated("zoo2_abbox")
+    assert np.array_equal(got, want)
 
 
 @pytest.mark.skipif(not HAVE_REF, reason="oracle/_ref not built")

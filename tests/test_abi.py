@@ -88,6 +88,12 @@ int main(int argc, char **) {
   if (argc > 5) {  // never taken: the calls only have to compile and link
     Geometry g;
     VPlacedVolume pv = g.Place(g.LogicalVolume("b", g.UnplacedBox(1, 2, 3)), g.Transformation3D());
+    double corners[24] = {0};
+    int shapes[] = {g.UnplacedOrb(1), g.UnplacedParallelepiped(1, 2, 3, 10, 20, 30),
+                    g.UnplacedParaboloid(1, 2, 3),
+                    g.UnplacedTrapezoid(4, 0.1, 0.2, 3, 2, 2, 0, 3, 2, 2, 0),
+                    g.UnplacedTrapezoid(corners)};
+    (void)shapes;
     double x[1] = {0}, out[1];
     SOA3D<double> p(x, x, x, 1);
     bool c[1];

@@ -25,7 +25,7 @@ ROOT = os.path.dirname(HERE)
 SO = os.path.join(ROOT, "_build", "hostcheck", "libvgb_hostcheck.so")
 GOLDEN = sorted(glob.glob(os.path.join(HERE, "golden", "*.npz")))
 HOST_SHAPES = {"box", "tube", "cone", "sphere", "trd", "torus", "polycone", "polyhedron", "orb",
-               "parallelepiped", "paraboloid",
+               "parallelepiped", "paraboloid", "trapezoid", "trapezoidcorners",
                "boolsub", "boolunion", "boolinter"}
 
 

@@ -45,6 +45,13 @@ TUBE3 = W.tube_spec(0., 50., 50., 0.5 * math.pi, 0.5 * math.pi)     # TestTube.c
 TUBE5 = W.tube_spec(50., 100., 50., 0., 1.5 * math.pi)              # TestTube.cpp:62
 TRD1 = W.trd_spec(20., 20., 30., 30., 40.)   # TestTrd.cpp:46
 TRD2 = W.trd_spec(10., 30., 20., 40., 40.)   # TestTrd.cpp:47
+TRAP1 = W.trapezoid_spec(40., 0., 0., 30., 20., 20., 0., 30., 20., 20., 0.)  # TestTrap.cpp:59
+TRAP2 = W.trapezoid_corners_spec([(-10., -20., -40.), (10., -20., -40.), (-10., 20., -40.),
+                                  (10., 20., -40.), (-30., -40., 40.), (30., -40., 40.),
+                                  (-30., 40., 40.), (30., 40., 40.)])  # TestTrap.cpp:51-65
+TRAP3 = W.trapezoid_spec(50., 0., 0., 50., 50., 50., math.pi / 4, 50., 50., 50., math.pi / 4)
+TRAP4 = W.trapezoid_spec(50., 0., 0., 50., 50., 50., -math.pi / 4, 50., 50., 50., -math.pi / 4)
+VYMZ = (0., R2, -R2)
 POLY = W.polycone_spec(0., 2 * math.pi, [-1., -0.5, 0.5, 2.], [0.1, 0., 0., 0.4],
                        [1., 2., 2., 1.5])    # TestVecGeomPolycone.cpp:29-41
 
@@ -95,6 +102,46 @@ CASES = [
     ("trd2 dto vx", TRD2, "distance_to_out", (0., 0., 0.), VX, 20., "TestTrd.cpp:283"),
     ("trd2 dto vy", TRD2, "distance_to_out", (0., 0., 0.), VY, 30., "TestTrd.cpp:287"),
     ("trd1 dti big x", TRD1, "distance_to_in", (100., 0., 0.), VMX, 80., "TestTrd.cpp:343"),
+    ("trap1 inside origin", TRAP1, "inside", (0., 0., 0.), None, kInside, "TestTrap.cpp:120"),
+    ("trap1 surface x", TRAP1, "inside", (20., 0., 0.), None, kSurface, "TestTrap.cpp:122"),
+    ("trap2 inside origin", TRAP2, "inside", (0., 0., 0.), None, kInside, "TestTrap.cpp:126"),
+    ("trap2 outside big z", TRAP2, "inside", (0., 0., 100.), None, kOutside, "TestTrap.cpp:127"),
+    ("trap2 surface y", TRAP2, "inside", (0., 30., 0.), None, kSurface, "TestTrap.cpp:129"),
+    ("trap1 safety out vx", TRAP1, "safety_to_out", (1., 0., 0.), None, 19., "TestTrap.cpp:251"),
+    ("trap2 safety out", TRAP2, "safety_to_out", (0., 0., 0.), None, 20 * COSA,
+     "TestTrap.cpp:258"),
+    ("trap2 safety out vz", TRAP2, "safety_to_out", (0., 0., 1.), None, 20 * COSA + SINA,
+     "TestTrap.cpp:264"),
+    ("trap1 dto vxy", TRAP1, "distance_to_out", (0., 0., 0.), VXY, math.sqrt(800.),
+     "TestTrap.cpp:282"),
+    ("trap1 dto z face back", TRAP1, "distance_to_out", (0., 0., 40.), VMZ, 80.,
+     "TestTrap.cpp:306"),
+    ("trap2 dto vx", TRAP2, "distance_to_out", (0., 0., 0.), VX, 20., "TestTrap.cpp:312"),
+    ("trap2 dto vxy", TRAP2, "distance_to_out", (0., 0., 0.), VXY, math.sqrt(800.),
+     "TestTrap.cpp:324"),
+    ("trap2 dto surface x", TRAP2, "distance_to_out", (20., 0., 0.), VX, 0., "TestTrap.cpp:327"),
+    ("trap1 safety in big", TRAP1, "safety_to_in", (100., 100., 100.), None, 80.,
+     "TestTrap.cpp:343"),
+    ("trap2 safety in big x", TRAP2, "safety_to_in", (100., 0., 0.), None, 80 * COSA,
+     "TestTrap.cpp:365"),
+    ("trap2 safety in big z", TRAP2, "safety_to_in", (0., 0., 100.), None, 60.,
+     "TestTrap.cpp:373"),
+    ("trap2 dti big y", TRAP2, "distance_to_in", (0., 100., 0.), VMY, 70., "TestTrap.cpp:402"),
+    ("trap2 dti miss", TRAP2, "distance_to_in", (100., 0., 0.), VXY, INF, "TestTrap.cpp:410"),
+    ("trap3 dti vy", TRAP3, "distance_to_in", (50., -50., 0.), VY, 50., "TestTrap.cpp:415"),
+    ("trap3 dti vmy", TRAP3, "distance_to_in", (50., -50., 0.), VMY, INF, "TestTrap.cpp:418"),
+    ("trap4 dti vy", TRAP4, "distance_to_in", (50., 50., 0.), VY, INF, "TestTrap.cpp:421"),
+    ("trap4 dti vmy", TRAP4, "distance_to_in", (50., 50., 0.), VMY, 50., "TestTrap.cpp:424"),
+    ("trap1 dti corner", TRAP1, "distance_to_in", (0., 40., 0.), VXMY, 10. * math.sqrt(2.),
+     "TestTrap.cpp:434"),
+    ("trap1 dti corner above", TRAP1, "distance_to_in", (0., 40., 50.), VXMY, INF,
+     "TestTrap.cpp:437"),
+    ("trap1 dti parallel z", TRAP1, "distance_to_in", (40., 60., 50.), VMZ, INF,
+     "TestTrap.cpp:448"),
+    ("trap1 dti vymz", TRAP1, "distance_to_in", (0., 0., 50.), VYMZ, 10. * math.sqrt(2.),
+     "TestTrap.cpp:451"),
+    ("trap1 dti vymz far", TRAP1, "distance_to_in", (0., 0., 80.), VYMZ, INF,
+     "TestTrap.cpp:454"),
     ("polycone contains origin", POLY, "contains", (0., 0., 0.), None, 1,
      "TestVecGeomPolycone.cpp:71"),
     ("polycone contains below", POLY, "contains", (0., 0., -2.), None, 0,

@@ -34,7 +34,9 @@ def spec_from_meta(meta):
             "sphere": W.sphere_spec, "torus": W.torus_spec, "trd": W.trd_spec,
             "polycone": W.polycone_spec, "polyhedron": W.polyhedron_spec,
             "boolsub": W.boolsub_spec, "orb": W.orb_spec,
-            "parallelepiped": W.parallelepiped_spec, "paraboloid": W.paraboloid_spec}.get(k)
+            "parallelepiped": W.parallelepiped_spec, "paraboloid": W.paraboloid_spec,
+            "trapezoid": W.trapezoid_spec,
+            "trapezoidcorners": W.trapezoid_corners_spec}.get(k)
     if ctor is None:
         return W.boolean_spec(k, **p)
     return ctor(**p)

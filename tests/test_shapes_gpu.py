@@ -20,7 +20,8 @@ from test_oracle_golden import load_case, spec_from_meta
 HERE = os.path.dirname(os.path.abspath(__file__))
 GOLDEN = sorted(glob.glob(os.path.join(HERE, "golden", "*.npz")))
 VGB_SHAPES = {"box", "tube", "cone", "sphere", "trd", "torus", "polycone", "polyhedron", "boolsub",
-              "orb", "parallelepiped", "paraboloid", "boolunion", "boolinter"}
+              "orb", "parallelepiped", "paraboloid", "boolunion", "boolinter", "trapezoid",
+              "trapezoidcorners"}
 
 pytestmark = pytest.mark.gpu
 
@@ -37,6 +38,13 @@ def dev(a):
 
 def host(t):
     return t.cpu().numpy()
+
+
+def spec_of_kind(kind):
+    """The parity shape named `kind`, else the first one of that kind."""
+    from helpers import shape_specs
+    specs = shape_specs()
+    return specs.get(kind) or next(s for s in specs.values() if s.kind == kind)
 
 
 def build_placed(spec, placement):
@@ -118,7 +126,7 @@ def test_large_seeded_vs_reference(kind):
     oracle/_ref is built, else against the C restatement."""
     from helpers import shape_specs
     from vecgeom_b200 import workloads as W
-    spec = shape_specs()[kind]
+    spec = spec_of_kind(kind)
     wl = W.make_workload(spec, 1 << 16, W.SEED_BASE + 17)
     g, pv = build_placed(spec, "generic")
     pts = (wl.x, wl.y, wl.z)
@@ -161,7 +169,7 @@ def test_minimize_node_and_placed_forms(kind):
     import vecgeom_b200 as V
     from helpers import shape_specs
     from vecgeom_b200 import workloads as W
-    spec = shape_specs()[kind]
+    spec = spec_of_kind(kind)
     n = 1 << 14
     wl = W.make_workload(spec, n, W.SEED_BASE + 23)
     g, pv = build_placed(spec, "generic")
@@ -226,7 +234,7 @@ def test_fp32_refine_equals_fp64(kind, placement):
     import vecgeom_b200 as V
     from helpers import shape_specs
     from vecgeom_b200 import workloads as W
-    spec = shape_specs()[kind]
+    spec = spec_of_kind(kind)
     n = 1 << 15
     wl = W.make_workload(spec, n, W.SEED_BASE + 31)
     # a far shell too: most of its rays miss, so the float screen settles them

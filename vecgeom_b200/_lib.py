@@ -69,6 +69,8 @@ SIGNATURES = {
     "vgb_unplaced_orb": (ctypes.c_int, [_vp, _dbl, _pi32]),
     "vgb_unplaced_parallelepiped": (ctypes.c_int, [_vp] + [_dbl] * 6 + [_pi32]),
     "vgb_unplaced_paraboloid": (ctypes.c_int, [_vp] + [_dbl] * 3 + [_pi32]),
+    "vgb_unplaced_trapezoid": (ctypes.c_int, [_vp] + [_dbl] * 11 + [_pi32]),
+    "vgb_unplaced_trapezoid_corners": (ctypes.c_int, [_vp, _vp, _pi32]),
     "vgb_unplaced_boolean": (ctypes.c_int, [_vp, _i32, _i32, _i32, _pi32]),
     "vgb_transformation": (ctypes.c_int, [_vp] + [_dbl] * 6 + [_pi32]),
     "vgb_transformation_matrix": (ctypes.c_int, [_vp, _dbl, _dbl, _dbl, _vp, _pi32]),

@@ -61,7 +61,8 @@ constexpr int kBoolMaxRounds = 4096;
   X(VGB_SHAPE_POLYHEDRON, vgb::PolyhedronOps, vgb::PolyhedronP)      \
   X(VGB_SHAPE_ORB, vgb::OrbOps, vgb::OrbP)                            \
   X(VGB_SHAPE_PARALLELEPIPED, vgb::ParaOps, vgb::ParaP)               \
-  X(VGB_SHAPE_PARABOLOID, vgb::ParaboloidOps, vgb::ParaboloidP)
+  X(VGB_SHAPE_PARABOLOID, vgb::ParaboloidOps, vgb::ParaboloidP)       \
+  X(VGB_SHAPE_TRAPEZOID, vgb::TrapezoidOps, vgb::TrapezoidP)
 
 template <class P> VGB_HD P comp_params(const double *rec) {
   return bind_params(*reinterpret_cast<const P *>(rec), rec);

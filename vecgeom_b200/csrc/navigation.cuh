@@ -147,7 +147,7 @@ template <class L> VGB_HD void nav_min_reduce(double &v, int &i) {
 // ---------------------------------------------------------------------------
 // shape dispatch over the shape types a geometry holds (kMask bit = type)
 // ---------------------------------------------------------------------------
-constexpr uint32_t kNavMaskAll = 0x1ffeu;  // types 1..12
+constexpr uint32_t kNavMaskAll = 0x3ffeu;  // types 1..13
 constexpr uint32_t kNavMaskBoxTubeTrd =
     (1u << VGB_SHAPE_BOX) | (1u << VGB_SHAPE_TUBE) | (1u << VGB_SHAPE_TRD);
 

@@ -14,6 +14,7 @@
 #include "orb.cuh"
 #include "parallelepiped.cuh"
 #include "paraboloid.cuh"
+#include "trapezoid.cuh"
 
 struct vgb_geometry;
 

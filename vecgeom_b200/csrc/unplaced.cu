@@ -247,6 +247,99 @@ ParaboloidP make_paraboloid(double rlo, double rhi, double dz) {
   return q;
 }
 
+// UnplacedTrapezoid::fromParametersToCorners (source/UnplacedTrapezoid.cpp:673-685)
+void trapezoid_corners(const TrapezoidP &t, double pt[8][3]) {
+  const double mz = -t.dz, pz = t.dz;
+  const double xs[8] = {mz * t.tthetaCphi - t.dy1 * t.tanAlpha1 - t.dx1,
+                        mz * t.tthetaCphi - t.dy1 * t.tanAlpha1 + t.dx1,
+                        mz * t.tthetaCphi + t.dy1 * t.tanAlpha1 - t.dx2,
+                        mz * t.tthetaCphi + t.dy1 * t.tanAlpha1 + t.dx2,
+                        pz * t.tthetaCphi - t.dy2 * t.tanAlpha2 - t.dx3,
+                        pz * t.tthetaCphi - t.dy2 * t.tanAlpha2 + t.dx3,
+                        pz * t.tthetaCphi + t.dy2 * t.tanAlpha2 - t.dx4,
+                        pz * t.tthetaCphi + t.dy2 * t.tanAlpha2 + t.dx4};
+  const double ys[4] = {mz * t.tthetaSphi - t.dy1, mz * t.tthetaSphi + t.dy1,
+                        pz * t.tthetaSphi - t.dy2, pz * t.tthetaSphi + t.dy2};
+  for (int k = 0; k < 8; ++k) {
+    pt[k][0] = xs[k];
+    pt[k][1] = ys[k / 2];
+    pt[k][2] = k < 4 ? mz : pz;
+  }
+}
+
+// UnplacedTrapezoid::MakePlane (source/UnplacedTrapezoid.cpp:272-330): the
+// plane through the quadrilateral p1..p4, its normal (p3 - p1) x (p4 - p2)
+// scaled to unit length; the reference's coplanarity check only prints.
+static void trapezoid_plane(TrapezoidP &t, int i, const double *p1, const double *p2,
+                            const double *p3, const double *p4) {
+  const double a = (p3[1] - p1[1]) * (p4[2] - p2[2]) - (p4[1] - p2[1]) * (p3[2] - p1[2]);
+  const double b = -(p3[0] - p1[0]) * (p4[2] - p2[2]) + (p4[0] - p2[0]) * (p3[2] - p1[2]);
+  const double c = (p3[0] - p1[0]) * (p4[1] - p2[1]) - (p4[0] - p2[0]) * (p3[1] - p1[1]);
+  const double norm = 1.0 / std::sqrt(a * a + b * b + c * c);
+  t.a[i] = a * norm;
+  t.b[i] = b * norm;
+  t.c[i] = c * norm;
+  t.d[i] = -(t.a[i] * p1[0] + t.b[i] * p1[1] + t.c[i] * p1[2]);
+}
+
+// UnplacedTrapezoid::MakePlanes(corners) (source/UnplacedTrapezoid.cpp:215-262):
+// -Y, +Y, -X, +X faces
+void trapezoid_planes(TrapezoidP &t, const double pt[8][3]) {
+  trapezoid_plane(t, 0, pt[0], pt[1], pt[5], pt[4]);
+  trapezoid_plane(t, 1, pt[2], pt[6], pt[7], pt[3]);
+  trapezoid_plane(t, 2, pt[0], pt[4], pt[6], pt[2]);
+  trapezoid_plane(t, 3, pt[1], pt[3], pt[7], pt[5]);
+}
+
+// UnplacedTrapezoid(pDz, pTheta, pPhi, pDy1, pDx1, pDx2, pTanAlpha1, pDy2,
+// pDx3, pDx4, pTanAlpha2), angles in radians (source/UnplacedTrapezoid.cpp:29-52)
+TrapezoidP make_trapezoid(double dz, double theta, double phi, double dy1, double dx1,
+                          double dx2, double tanAlpha1, double dy2, double dx3, double dx4,
+                          double tanAlpha2) {
+  TrapezoidP t;
+  std::memset(&t, 0, sizeof(t));
+  t.dz = dz;
+  t.theta = theta;
+  t.phi = phi;
+  t.dy1 = dy1;
+  t.dx1 = dx1;
+  t.dx2 = dx2;
+  t.tanAlpha1 = tanAlpha1;
+  t.dy2 = dy2;
+  t.dx3 = dx3;
+  t.dx4 = dx4;
+  t.tanAlpha2 = tanAlpha2;
+  t.tthetaSphi = std::tan(theta) * std::sin(phi);
+  t.tthetaCphi = std::tan(theta) * std::cos(phi);
+  double pt[8][3];
+  trapezoid_corners(t, pt);
+  trapezoid_planes(t, pt);
+  return t;
+}
+
+// UnplacedTrapezoid(TrapCorners_t) (source/UnplacedTrapezoid.cpp:96-105): the
+// planes from the corners as given, then fromCornersToParameters (:651-671)
+TrapezoidP make_trapezoid_corners(const double pt[8][3]) {
+  TrapezoidP t;
+  std::memset(&t, 0, sizeof(t));
+  trapezoid_planes(t, pt);
+  t.dz = pt[7][2];
+  const double dzRecip = 1.0 / t.dz;
+  t.dy1 = 0.50 * (pt[2][1] - pt[0][1]);
+  t.dx1 = 0.50 * (pt[1][0] - pt[0][0]);
+  t.dx2 = 0.50 * (pt[3][0] - pt[2][0]);
+  t.tanAlpha1 = 0.25 * (pt[2][0] + pt[3][0] - pt[1][0] - pt[0][0]) / t.dy1;
+  t.dy2 = 0.50 * (pt[6][1] - pt[4][1]);
+  t.dx3 = 0.50 * (pt[5][0] - pt[4][0]);
+  t.dx4 = 0.50 * (pt[7][0] - pt[6][0]);
+  t.tanAlpha2 = 0.25 * (pt[6][0] + pt[7][0] - pt[5][0] - pt[4][0]) / t.dy2;
+  t.tthetaCphi = (pt[4][0] + t.dy2 * t.tanAlpha2 + t.dx3) * dzRecip;
+  t.tthetaSphi = (pt[4][1] + t.dy2) * dzRecip;
+  t.theta = std::atan(std::sqrt(t.tthetaSphi * t.tthetaSphi + t.tthetaCphi * t.tthetaCphi));
+  t.phi = std::atan2(t.tthetaSphi, t.tthetaCphi);
+  return t;
+}
+
 // UnplacedTrd::calculateCached (volumes/UnplacedTrd.h:38-51)
 TrdP make_trd(double dx1, double dx2, double dy1, double dy2, double dz) {
   TrdP t;
@@ -603,6 +696,12 @@ bool shape_bbox(const vgb_geometry *g, int32_t u, double b[6]) {
       const ParaboloidP &p = *reinterpret_cast<const ParaboloidP *>(rec);
       return sym(p.dx, p.dx, p.dz);
     }
+    case VGB_SHAPE_TRAPEZOID: {  // the Extent encloses the solid exactly
+      double lo[3], hi[3];
+      reference_extent(VGB_SHAPE_TRAPEZOID, rec, lo, hi);
+      b[0] = lo[0]; b[1] = lo[1]; b[2] = lo[2]; b[3] = hi[0]; b[4] = hi[1]; b[5] = hi[2];
+      return true;
+    }
     case VGB_SHAPE_PARALLELEPIPED: {
       // the box's corners mapped back through the shear
       const ParaP &p = *reinterpret_cast<const ParaP *>(rec);
@@ -724,6 +823,28 @@ bool reference_extent(int type, const double *rec, double lo[3], double hi[3]) {
     case VGB_SHAPE_SPHERE: {  // source/UnplacedSphere.cpp:174-179
       const SphereP &p = *reinterpret_cast<const SphereP *>(rec);
       return set(-p.rmax, -p.rmax, -p.rmax, p.rmax, p.rmax, p.rmax);
+    }
+    case VGB_SHAPE_TRAPEZOID: {  // source/UnplacedTrapezoid.cpp:428-466
+      const TrapezoidP &p = *reinterpret_cast<const TrapezoidP *>(rec);
+      double pt[8][3];
+      trapezoid_corners(p, pt);
+      // per axis: std::max / std::min of corner pairs, then the pairs' pairs
+      for (int ax = 0; ax < 2; ++ax) {
+        double e01 = vmax(pt[0][ax], pt[1][ax]), e23 = vmax(pt[2][ax], pt[3][ax]);
+        double e45 = vmax(pt[4][ax], pt[5][ax]), e67 = vmax(pt[6][ax], pt[7][ax]);
+        double ea = e01 > e23 ? e01 : e23, eb = e45 > e67 ? e45 : e67;
+        hi[ax] = ea > eb ? ea : eb;
+        e01 = vmin(pt[0][ax], pt[1][ax]);
+        e23 = vmin(pt[2][ax], pt[3][ax]);
+        e45 = vmin(pt[4][ax], pt[5][ax]);
+        e67 = vmin(pt[6][ax], pt[7][ax]);
+        ea = e01 < e23 ? e01 : e23;
+        eb = e45 < e67 ? e45 : e67;
+        lo[ax] = ea < eb ? ea : eb;
+      }
+      lo[2] = -p.dz;
+      hi[2] = p.dz;
+      return true;
     }
     case VGB_SHAPE_PARABOLOID: {  // source/UnplacedParaboloid.cpp:169-176
       const ParaboloidP &p = *reinterpret_cast<const ParaboloidP *>(rec);
@@ -872,6 +993,39 @@ vgb_status vgb_unplaced_paraboloid(vgb_geometry *g, double rlo, double rhi, doub
     return set_error(VGB_EINVAL, "vgb_unplaced_paraboloid: need rlo, rhi >= 0, rlo != rhi, dz > 0");
   ParaboloidP q = make_paraboloid(rlo, rhi, dz);
   return add_unplaced(g, VGB_SHAPE_PARABOLOID, &q, sizeof(q), 0, id);
+}
+
+vgb_status vgb_unplaced_trapezoid(vgb_geometry *g, double dz, double theta, double phi,
+                                  double dy1, double dx1, double dx2, double tan_alpha1,
+                                  double dy2, double dx3, double dx4, double tan_alpha2,
+                                  int32_t *id) {
+  VGB_CHECK_OPEN(g);
+  // the reference prints "Invalid input length parameters" and goes on
+  // (source/UnplacedTrapezoid.cpp:37-46); here they are refused
+  if (!(dz > 0 && dy1 > 0 && dx1 > 0 && dx2 > 0 && dy2 > 0 && dx3 > 0 && dx4 > 0))
+    return set_error(VGB_EINVAL, "vgb_unplaced_trapezoid: half-lengths must be > 0");
+  TrapezoidP t = make_trapezoid(dz, theta, phi, dy1, dx1, dx2, tan_alpha1, dy2, dx3, dx4,
+                                tan_alpha2);
+  return add_unplaced(g, VGB_SHAPE_TRAPEZOID, &t, sizeof(t), 0, id);
+}
+
+vgb_status vgb_unplaced_trapezoid_corners(vgb_geometry *g, const double *corners,
+                                          int32_t *id) {
+  VGB_CHECK_OPEN(g);
+  if (!corners) return set_error(VGB_EINVAL, "vgb_unplaced_trapezoid_corners: null corners");
+  double pt[8][3];
+  std::memcpy(pt, corners, sizeof(pt));
+  // the corner layout the reference expects: z = -dz for 0..3, +dz for 4..7
+  const double dz = pt[7][2];
+  for (int k = 0; k < 8; ++k)
+    if (!(pt[k][2] == (k < 4 ? -dz : dz)))
+      return set_error(VGB_EINVAL,
+                       "vgb_unplaced_trapezoid_corners: corners 0-3 need z = -dz, 4-7 z = +dz");
+  if (!(dz > 0 && pt[2][1] > pt[0][1] && pt[1][0] > pt[0][0] && pt[3][0] > pt[2][0] &&
+        pt[6][1] > pt[4][1] && pt[5][0] > pt[4][0] && pt[7][0] > pt[6][0]))
+    return set_error(VGB_EINVAL, "vgb_unplaced_trapezoid_corners: degenerate corners");
+  TrapezoidP t = make_trapezoid_corners(pt);
+  return add_unplaced(g, VGB_SHAPE_TRAPEZOID, &t, sizeof(t), 0, id);
 }
 
 vgb_status vgb_unplaced_sphere(vgb_geometry *g, double rmin, double rmax, double sphi,

@@ -254,6 +254,24 @@ class Geometry:
     def UnplacedParaboloid(self, rlo, rhi, dz) -> int:
         return self._id(self.L.vgb_unplaced_paraboloid, rlo, rhi, dz)
 
+    def UnplacedTrapezoid(self, dz, theta, phi, dy1, dx1, dx2, tan_alpha1, dy2, dx3, dx4,
+                          tan_alpha2) -> int:
+        """UnplacedTrapezoid(pDz, pTheta, pPhi, pDy1, pDx1, pDx2, pTanAlpha1, pDy2,
+        pDx3, pDx4, pTanAlpha2), angles in radians
+        (volumes/UnplacedTrapezoid.h:93-95)."""
+        return self._id(self.L.vgb_unplaced_trapezoid, dz, theta, phi, dy1, dx1, dx2,
+                        tan_alpha1, dy2, dx3, dx4, tan_alpha2)
+
+    def UnplacedTrapezoidFromCorners(self, corners) -> int:
+        """UnplacedTrapezoid(TrapCorners_t) (volumes/UnplacedTrapezoid.h:103):
+        8 corners (x, y, z), 0-3 at z = -dz, 4-7 at z = +dz."""
+        c = np.ascontiguousarray(corners, np.float64).reshape(8, 3)
+        return self._id(self.L.vgb_unplaced_trapezoid_corners, c.ctypes.data)
+
+    def UnplacedTrapezoidBox(self, xbox, ybox, zbox) -> int:
+        """UnplacedTrapezoid(xbox, ybox, zbox) (volumes/UnplacedTrapezoid.h:115)."""
+        return self.UnplacedTrapezoid(zbox, 0., 0., ybox, xbox, xbox, 0., ybox, xbox, xbox, 0.)
+
     def UnplacedBooleanVolume(self, op: int, left: PlacedVolume, right: PlacedVolume) -> int:
         return self._id(self.L.vgb_unplaced_boolean, op, left.id, right.id)
 

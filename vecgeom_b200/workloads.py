@@ -32,7 +32,8 @@ def isotropic(rng: np.random.Generator, n: int):
 class ShapeSpec:
     """One unplaced shape: constructor arguments plus sampling helpers."""
     kind: str                       # box, tube, cone, sphere, torus, polycone, polyhedron, boolsub,
-                                    # trd, orb, parallelepiped, paraboloid
+                                    # trd, orb, parallelepiped, paraboloid, trapezoid,
+                                    # trapezoidcorners
     params: dict
     half: tuple                     # half extents of the axis-aligned bounding box
     center: tuple = (0., 0., 0.)
@@ -134,6 +135,55 @@ def paraboloid_spec(rlo, rhi, dz) -> ShapeSpec:
         return (np.abs(z) <= dz) & (z >= a * (x * x + y * y) + b)
     h = max(rlo, rhi)
     return ShapeSpec("paraboloid", dict(rlo=rlo, rhi=rhi, dz=dz), (h, h, dz), contains=contains)
+
+
+def _trapezoid_shape(kind, params, corners) -> ShapeSpec:
+    """ShapeSpec of a trapezoid given its 8 corners (0-3 at -dz, 4-7 at +dz):
+    the bounding box of the corners and the four side planes' test."""
+    pt = np.asarray(corners, np.float64).reshape(8, 3)
+    dz = pt[7, 2]
+    quads = ((0, 1, 5, 4), (2, 6, 7, 3), (0, 4, 6, 2), (1, 3, 7, 5))
+    planes = []
+    for i1, i2, i3, i4 in quads:
+        n = np.cross(pt[i3] - pt[i1], pt[i4] - pt[i2])
+        n = n / np.linalg.norm(n)
+        planes.append((n, -n.dot(pt[i1])))
+
+    def contains(x, y, z):
+        ok = np.abs(z) <= dz
+        for n, d in planes:
+            ok &= n[0] * x + n[1] * y + n[2] * z + d <= 0
+        return ok
+    lo, hi = pt.min(axis=0), pt.max(axis=0)
+    return ShapeSpec(kind, params, tuple((hi - lo) / 2), center=tuple((hi + lo) / 2),
+                     contains=contains)
+
+
+def trapezoid_corners(dz, theta, phi, dy1, dx1, dx2, tan_alpha1, dy2, dx3, dx4, tan_alpha2):
+    """The 8 corners of UnplacedTrapezoid's parameters
+    (source/UnplacedTrapezoid.cpp:673-685)."""
+    tc, ts = math.tan(theta) * math.cos(phi), math.tan(theta) * math.sin(phi)
+    out = []
+    for z, dy, dxa, dxb, ta in ((-dz, dy1, dx1, dx2, tan_alpha1), (dz, dy2, dx3, dx4, tan_alpha2)):
+        for sy, dx in ((-1, dxa), (1, dxb)):
+            for sx in (-1, 1):
+                out.append((z * tc + sy * dy * ta + sx * dx, z * ts + sy * dy, z))
+    return np.array(out)
+
+
+def trapezoid_spec(dz, theta, phi, dy1, dx1, dx2, tan_alpha1, dy2, dx3, dx4,
+                   tan_alpha2) -> ShapeSpec:
+    """General trapezoid (UnplacedTrapezoid's 11 parameters, angles in radians)."""
+    args = (dz, theta, phi, dy1, dx1, dx2, tan_alpha1, dy2, dx3, dx4, tan_alpha2)
+    names = ("dz", "theta", "phi", "dy1", "dx1", "dx2", "tan_alpha1", "dy2", "dx3", "dx4",
+             "tan_alpha2")
+    return _trapezoid_shape("trapezoid", dict(zip(names, args)), trapezoid_corners(*args))
+
+
+def trapezoid_corners_spec(corners) -> ShapeSpec:
+    """Trapezoid built from its 8 corners (UnplacedTrapezoid(TrapCorners_t))."""
+    c = np.asarray(corners, np.float64).reshape(8, 3)
+    return _trapezoid_shape("trapezoidcorners", dict(corners=c.ravel().tolist()), c)
 
 
 def trd_spec(dx1, dx2, dy1, dy2, dz) -> ShapeSpec:
@@ -411,6 +461,12 @@ def build_unplaced(geom, spec: ShapeSpec) -> int:
         return geom.UnplacedOrb(p["r"])
     if k == "paraboloid":
         return geom.UnplacedParaboloid(p["rlo"], p["rhi"], p["dz"])
+    if k == "trapezoid":
+        return geom.UnplacedTrapezoid(p["dz"], p["theta"], p["phi"], p["dy1"], p["dx1"], p["dx2"],
+                                      p["tan_alpha1"], p["dy2"], p["dx3"], p["dx4"],
+                                      p["tan_alpha2"])
+    if k == "trapezoidcorners":
+        return geom.UnplacedTrapezoidFromCorners(p["corners"])
     if k == "parallelepiped":
         return geom.UnplacedParallelepiped(p["x"], p["y"], p["z"], p["alpha"], p["theta"],
                                            p["phi"])
@@ -543,6 +599,25 @@ def zoo_specs(exclude=()) -> list:
     `exclude`."""
     specs = ([config1_box()] + list(config2_shapes().values()) + list(config3_shapes().values())
              + [trd_spec(20., 10., 25., 15., 30.)])
+    return [s for s in specs if s.kind not in exclude]
+
+
+def zoo2_specs(exclude=()) -> list:
+    """The second mixed navigation geometry's shapes: orb, parallelepiped,
+    paraboloid, two trapezoids (one from corners), a box-tube union and a
+    box-tube intersection, less the kinds in `exclude` (every one reaches less
+    than 135 mm from its centre)."""
+    specs = [orb_spec(25.), parallelepiped_spec(20., 30., 40., 30., 20., 40.),
+             paraboloid_spec(10., 30., 40.),
+             trapezoid_spec(40., 0.3, 0.7, 20., 10., 15., 0.2, 30., 20., 27.5, 0.2),
+             trapezoid_corners_spec([(-10., -20., -40.), (10., -20., -40.), (-10., 20., -40.),
+                                     (10., 20., -40.), (-30., -40., 40.), (30., -40., 40.),
+                                     (-30., 40., 40.), (30., 40., 40.)]),
+             boolean_spec("boolunion", (20., 20., 20.), 12., 35.,
+                          right_place=(8., 0., 0., 0., 0., 0.)),
+             boolean_spec("boolinter", (25., 20., 15.), 18., 40.,
+                          left_place=(2., -1., 3., 0., 0., 15.),
+                          right_place=(0., 2., 0., 0., 90., 30.))]
     return [s for s in specs if s.kind not in exclude]
 
 
