@@ -185,6 +185,29 @@ vgb_status vgb_geometry_max_depth(const vgb_geometry *g, int32_t *depth);
 vgb_status vgb_geometry_device_bytes(const vgb_geometry *g, int64_t *bytes);
 
 /* ---------------------------------------------------------------------------
+ * Ingestion and export formats.
+ *
+ * Flat image: the recorded object graph (shape records with their constructor
+ * arguments, transformations, logical volumes and labels, placements, world)
+ * in one checksummed little-endian blob.  The reference has no such image (it
+ * rebuilds its object graph from ROOT, Geant4 or generated C++ source,
+ * source/RootGeoManager.cpp:48-169, source/CppExporter.cpp); it is the
+ * ingestion path of this library.  Serialising writes *len bytes into buf when
+ * cap suffices (buf NULL: only *len); VGB_ENOSPC when cap is too small.
+ * Deserialising creates a new, open geometry with the same ids; close it as
+ * usual.  A malformed or corrupted image is VGB_EINVAL. */
+vgb_status vgb_geometry_serialize(const vgb_geometry *g, void *buf, size_t cap, size_t *len);
+vgb_status vgb_geometry_deserialize(const void *buf, size_t len, vgb_geometry **g);
+vgb_status vgb_geometry_save(const vgb_geometry *g, const char *path);
+vgb_status vgb_geometry_load(const char *path, vgb_geometry **g);
+/* GeomCppExporter::DumpGeometry (management/CppExporter.h, source/CppExporter.cpp):
+ * C++ source of `VPlacedVolume const * generateDetector()` that rebuilds the
+ * geometry with VecGeom's API; numbers with 17 significant digits; a comment
+ * lists this geometry's placed ids in the order the function creates the
+ * placements.  Buffer convention as vgb_geometry_serialize (no terminating NUL). */
+vgb_status vgb_geometry_export_cpp(const vgb_geometry *g, char *buf, size_t cap, size_t *len);
+
+/* ---------------------------------------------------------------------------
  * Batched shape operations (the VPlacedVolume SOA3D virtuals).
  *
  * One call runs one operation over n points for one placed volume.

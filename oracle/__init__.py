@@ -34,6 +34,23 @@ def build(with_ref: bool = True) -> None:
                    stdout=subprocess.DEVNULL)
 
 
+def _make_print(target: str) -> str:
+    return subprocess.run(["make", "-s", "-C", HERE, target], check=True, capture_output=True,
+                          text=True).stdout.strip()
+
+
+def reference_tree():
+    """The reference source tree oracle/Makefile builds from, or None when it is
+    absent (its base/Global.h missing)."""
+    ref = _make_print("print-ref")
+    return ref if os.path.exists(os.path.join(ref, "base", "Global.h")) else None
+
+
+def reference_cxxflags() -> list:
+    """The flags oracle/Makefile compiles the reference's sources with."""
+    return _make_print("print-ref-cxxflags").split()
+
+
 def _p(a):
     return None if a is None else a.ctypes.data_as(_vp)
 

@@ -81,6 +81,13 @@ SIGNATURES = {
     "vgb_geometry_close": (ctypes.c_int, [_vp]),
     "vgb_geometry_max_depth": (ctypes.c_int, [_vp, _pi32]),
     "vgb_geometry_device_bytes": (ctypes.c_int, [_vp, _pi64]),
+    "vgb_geometry_serialize": (ctypes.c_int, [_vp, _vp, ctypes.c_size_t,
+                                              ctypes.POINTER(ctypes.c_size_t)]),
+    "vgb_geometry_deserialize": (ctypes.c_int, [_vp, ctypes.c_size_t, ctypes.POINTER(_vp)]),
+    "vgb_geometry_save": (ctypes.c_int, [_vp, _cp]),
+    "vgb_geometry_load": (ctypes.c_int, [_cp, ctypes.POINTER(_vp)]),
+    "vgb_geometry_export_cpp": (ctypes.c_int, [_vp, _vp, ctypes.c_size_t,
+                                               ctypes.POINTER(ctypes.c_size_t)]),
     "vgb_batch": (ctypes.c_int, [_vp, _i32, _i32, _i64] + [_vp] * 9 + [_i32, _i32, _vp]),
     "vgb_batch_fused": (ctypes.c_int, [_vp, _i32, _u32, _i64] + [_vp] * 8 + [_u32, _i32, _vp]),
     "vgb_Contains": (ctypes.c_int, [_vp, _i32, _i64, _vp, _vp, _vp, _vp, _vp]),

@@ -106,6 +106,8 @@ vgb_status vgb::add_unplaced(vgb_geometry *g, int type, const void *rec, size_t 
   g->params.resize(g->params.size() + nd + (nd % 2), 0.);
   std::memcpy(g->params.data() + u.param_off, rec, bytes);
   g->unplaced.push_back(u);
+  g->ctor_form.push_back(kCtorDefault);
+  g->ctor_args.emplace_back();
   if (id) *id = (int32_t)g->unplaced.size() - 1;
   return VGB_OK;
 }

@@ -79,8 +79,15 @@ struct DeviceImage {
 
 }  // namespace vgb
 
+namespace vgb {
+// Constructor forms of a shape (the trapezoid has two)
+enum : int32_t { kCtorDefault = 0, kCtorCorners = 1 };
+}  // namespace vgb
+
 struct vgb_geometry {
   std::vector<vgb::UnplacedRec> unplaced;
+  std::vector<int32_t> ctor_form;               // per unplaced: kCtorDefault / kCtorCorners
+  std::vector<std::vector<double>> ctor_args;   // per unplaced: its constructor's arguments
   std::vector<double> params;
   std::vector<vgb::RawXform> raw_xforms;
   std::vector<vgb::DXform> xforms;  // per (placed volume), effective for its shape

@@ -911,6 +911,20 @@ bool reference_extent(int type, const double *rec, double lo[3], double hi[3]) {
 
 }  // namespace vgb
 
+// add_unplaced plus the constructor's own arguments, which the flat image and
+// the C++ export carry
+static vgb_status add_shape(vgb_geometry *g, int type, const void *rec, size_t bytes,
+                            int32_t extra, int32_t *id, std::vector<double> args,
+                            int32_t form = kCtorDefault) {
+  int32_t uid = -1;
+  vgb_status s = add_unplaced(g, type, rec, bytes, extra, &uid);
+  if (s != VGB_OK) return s;
+  g->ctor_form[uid] = form;
+  g->ctor_args[uid] = std::move(args);
+  if (id) *id = uid;
+  return VGB_OK;
+}
+
 extern "C" {
 
 vgb_status vgb_unplaced_polyhedron(vgb_geometry *g, double phi_start_deg, double phi_delta_deg,
@@ -927,7 +941,12 @@ vgb_status vgb_unplaced_polyhedron(vgb_geometry *g, double phi_start_deg, double
       return set_error(VGB_EINVAL, "vgb_unplaced_polyhedron: z planes must not decrease");
   std::vector<double> blob =
       make_polyhedron(phi_start_deg, phi_delta_deg, sides, nz, z, rmin, rmax);
-  return add_unplaced(g, VGB_SHAPE_POLYHEDRON, blob.data(), blob.size() * sizeof(double), 0, id);
+  std::vector<double> args = {phi_start_deg, phi_delta_deg, (double)sides, (double)nz};
+  args.insert(args.end(), z, z + nz);
+  args.insert(args.end(), rmin, rmin + nz);
+  args.insert(args.end(), rmax, rmax + nz);
+  return add_shape(g, VGB_SHAPE_POLYHEDRON, blob.data(), blob.size() * sizeof(double), 0, id,
+                   std::move(args));
 }
 
 vgb_status vgb_unplaced_polycone(vgb_geometry *g, double sphi, double dphi, int32_t nz,
@@ -945,7 +964,12 @@ vgb_status vgb_unplaced_polycone(vgb_geometry *g, double sphi, double dphi, int3
   std::vector<double> blob = make_polycone(sphi, dphi, nz, rmin, rmax, z);
   if (reinterpret_cast<const PolyconeP *>(blob.data())->nsec < 1)
     return set_error(VGB_EINVAL, "vgb_unplaced_polycone: no section (all z planes equal)");
-  return add_unplaced(g, VGB_SHAPE_POLYCONE, blob.data(), blob.size() * sizeof(double), 0, id);
+  std::vector<double> args = {sphi, dphi, (double)nz};
+  args.insert(args.end(), rmin, rmin + nz);
+  args.insert(args.end(), rmax, rmax + nz);
+  args.insert(args.end(), z, z + nz);
+  return add_shape(g, VGB_SHAPE_POLYCONE, blob.data(), blob.size() * sizeof(double), 0, id,
+                   std::move(args));
 }
 
 vgb_status vgb_unplaced_torus(vgb_geometry *g, double rmin, double rmax, double rtor, double sphi,
@@ -954,7 +978,7 @@ vgb_status vgb_unplaced_torus(vgb_geometry *g, double rmin, double rmax, double 
   if (!(rmin >= 0 && rmax > rmin && rtor > rmax && dphi > 0))
     return set_error(VGB_EINVAL, "vgb_unplaced_torus: need 0 <= rmin < rmax < rtor, dphi > 0");
   TorusP t = make_torus(rmin, rmax, rtor, sphi, dphi);
-  return add_unplaced(g, VGB_SHAPE_TORUS, &t, sizeof(t), 0, id);
+  return add_shape(g, VGB_SHAPE_TORUS, &t, sizeof(t), 0, id, {rmin, rmax, rtor, sphi, dphi});
 }
 
 vgb_status vgb_unplaced_trd(vgb_geometry *g, double dx1, double dx2, double dy1, double dy2,
@@ -964,14 +988,14 @@ vgb_status vgb_unplaced_trd(vgb_geometry *g, double dx1, double dx2, double dy1,
         (dy1 > 0 || dy2 > 0)))
     return set_error(VGB_EINVAL, "vgb_unplaced_trd: invalid half-lengths");
   TrdP t = make_trd(dx1, dx2, dy1, dy2, dz);
-  return add_unplaced(g, VGB_SHAPE_TRD, &t, sizeof(t), 0, id);
+  return add_shape(g, VGB_SHAPE_TRD, &t, sizeof(t), 0, id, {dx1, dx2, dy1, dy2, dz});
 }
 
 vgb_status vgb_unplaced_orb(vgb_geometry *g, double r, int32_t *id) {
   VGB_CHECK_OPEN(g);
   if (!(r > 0)) return set_error(VGB_EINVAL, "vgb_unplaced_orb: radius must be > 0");
   OrbP o = make_orb(r);
-  return add_unplaced(g, VGB_SHAPE_ORB, &o, sizeof(o), 0, id);
+  return add_shape(g, VGB_SHAPE_ORB, &o, sizeof(o), 0, id, {r});
 }
 
 vgb_status vgb_unplaced_parallelepiped(vgb_geometry *g, double x, double y, double z,
@@ -981,7 +1005,8 @@ vgb_status vgb_unplaced_parallelepiped(vgb_geometry *g, double x, double y, doub
   if (!(x > 0 && y > 0 && z > 0))
     return set_error(VGB_EINVAL, "vgb_unplaced_parallelepiped: half-lengths must be > 0");
   ParaP a = make_parallelepiped(x, y, z, alpha_deg, theta_deg, phi_deg);
-  return add_unplaced(g, VGB_SHAPE_PARALLELEPIPED, &a, sizeof(a), 0, id);
+  return add_shape(g, VGB_SHAPE_PARALLELEPIPED, &a, sizeof(a), 0, id,
+                   {x, y, z, alpha_deg, theta_deg, phi_deg});
 }
 
 vgb_status vgb_unplaced_paraboloid(vgb_geometry *g, double rlo, double rhi, double dz,
@@ -992,7 +1017,7 @@ vgb_status vgb_unplaced_paraboloid(vgb_geometry *g, double rlo, double rhi, doub
   if (!(rlo >= 0 && rhi >= 0 && dz > 0 && rhi != rlo))
     return set_error(VGB_EINVAL, "vgb_unplaced_paraboloid: need rlo, rhi >= 0, rlo != rhi, dz > 0");
   ParaboloidP q = make_paraboloid(rlo, rhi, dz);
-  return add_unplaced(g, VGB_SHAPE_PARABOLOID, &q, sizeof(q), 0, id);
+  return add_shape(g, VGB_SHAPE_PARABOLOID, &q, sizeof(q), 0, id, {rlo, rhi, dz});
 }
 
 vgb_status vgb_unplaced_trapezoid(vgb_geometry *g, double dz, double theta, double phi,
@@ -1006,7 +1031,8 @@ vgb_status vgb_unplaced_trapezoid(vgb_geometry *g, double dz, double theta, doub
     return set_error(VGB_EINVAL, "vgb_unplaced_trapezoid: half-lengths must be > 0");
   TrapezoidP t = make_trapezoid(dz, theta, phi, dy1, dx1, dx2, tan_alpha1, dy2, dx3, dx4,
                                 tan_alpha2);
-  return add_unplaced(g, VGB_SHAPE_TRAPEZOID, &t, sizeof(t), 0, id);
+  return add_shape(g, VGB_SHAPE_TRAPEZOID, &t, sizeof(t), 0, id,
+                   {dz, theta, phi, dy1, dx1, dx2, tan_alpha1, dy2, dx3, dx4, tan_alpha2});
 }
 
 vgb_status vgb_unplaced_trapezoid_corners(vgb_geometry *g, const double *corners,
@@ -1025,7 +1051,8 @@ vgb_status vgb_unplaced_trapezoid_corners(vgb_geometry *g, const double *corners
         pt[6][1] > pt[4][1] && pt[5][0] > pt[4][0] && pt[7][0] > pt[6][0]))
     return set_error(VGB_EINVAL, "vgb_unplaced_trapezoid_corners: degenerate corners");
   TrapezoidP t = make_trapezoid_corners(pt);
-  return add_unplaced(g, VGB_SHAPE_TRAPEZOID, &t, sizeof(t), 0, id);
+  return add_shape(g, VGB_SHAPE_TRAPEZOID, &t, sizeof(t), 0, id,
+                   std::vector<double>(corners, corners + 24), kCtorCorners);
 }
 
 vgb_status vgb_unplaced_sphere(vgb_geometry *g, double rmin, double rmax, double sphi,
@@ -1035,7 +1062,8 @@ vgb_status vgb_unplaced_sphere(vgb_geometry *g, double rmin, double rmax, double
         stheta >= 0 && stheta <= kPi))
     return set_error(VGB_EINVAL, "vgb_unplaced_sphere: invalid radii or angles");
   SphereP s = make_sphere(rmin, rmax, sphi, dphi, stheta, dtheta);
-  return add_unplaced(g, VGB_SHAPE_SPHERE, &s, sizeof(s), 0, id);
+  return add_shape(g, VGB_SHAPE_SPHERE, &s, sizeof(s), 0, id,
+                   {rmin, rmax, sphi, dphi, stheta, dtheta});
 }
 
 vgb_status vgb_unplaced_cone(vgb_geometry *g, double rmin1, double rmax1, double rmin2,
@@ -1044,7 +1072,8 @@ vgb_status vgb_unplaced_cone(vgb_geometry *g, double rmin1, double rmax1, double
   if (!(dz > 0 && rmin1 >= 0 && rmin2 >= 0 && rmax1 >= rmin1 && rmax2 >= rmin2 && dphi > 0))
     return set_error(VGB_EINVAL, "vgb_unplaced_cone: invalid radii, dz or dphi");
   ConeP c = make_cone(rmin1, rmax1, rmin2, rmax2, dz, sphi, dphi);
-  return add_unplaced(g, VGB_SHAPE_CONE, &c, sizeof(c), 0, id);
+  return add_shape(g, VGB_SHAPE_CONE, &c, sizeof(c), 0, id,
+                   {rmin1, rmax1, rmin2, rmax2, dz, sphi, dphi});
 }
 
 vgb_status vgb_unplaced_box(vgb_geometry *g, double dx, double dy, double dz, int32_t *id) {
@@ -1055,7 +1084,7 @@ vgb_status vgb_unplaced_box(vgb_geometry *g, double dx, double dy, double dz, in
   b.d[0] = dx;
   b.d[1] = dy;
   b.d[2] = dz;
-  return add_unplaced(g, VGB_SHAPE_BOX, &b, sizeof(b), 0, id);
+  return add_shape(g, VGB_SHAPE_BOX, &b, sizeof(b), 0, id, {dx, dy, dz});
 }
 
 vgb_status vgb_unplaced_tube(vgb_geometry *g, double rmin, double rmax, double dz, double sphi,
@@ -1064,7 +1093,7 @@ vgb_status vgb_unplaced_tube(vgb_geometry *g, double rmin, double rmax, double d
   if (!(rmin >= 0 && rmax > rmin && dz > 0 && dphi > 0))
     return set_error(VGB_EINVAL, "vgb_unplaced_tube: need 0 <= rmin < rmax, dz > 0, dphi > 0");
   TubeP t = make_tube(rmin, rmax, dz, sphi, dphi);
-  return add_unplaced(g, VGB_SHAPE_TUBE, &t, sizeof(t), 0, id);
+  return add_shape(g, VGB_SHAPE_TUBE, &t, sizeof(t), 0, id, {rmin, rmax, dz, sphi, dphi});
 }
 
 // ---------------------------------------------------------------------------
@@ -1095,7 +1124,8 @@ vgb_status vgb_unplaced_boolean(vgb_geometry *g, int32_t op, int32_t left_placed
   b.right.type = rt;
   b.right_generic = effective_xform(g->raw_xforms[pr.raw_xform], true);
   int32_t uid = -1;
-  vgb_status s = add_unplaced(g, VGB_SHAPE_BOOLEAN, &b, sizeof(b), left_placed, &uid);
+  vgb_status s = add_shape(g, VGB_SHAPE_BOOLEAN, &b, sizeof(b), left_placed, &uid,
+                           {(double)op, (double)left_placed, (double)right_placed});
   if (s != VGB_OK) return s;
   const int32_t off = g->unplaced[uid].param_off;
   BooleanP *rec = reinterpret_cast<BooleanP *>(g->params.data() + off);

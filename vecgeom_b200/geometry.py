@@ -18,6 +18,7 @@ Errors raise VgbError instead of asserting.
 from __future__ import annotations
 
 import ctypes
+import os
 from dataclasses import dataclass
 
 import numpy as np
@@ -305,6 +306,50 @@ class Geometry:
         out = ctypes.c_int64()
         check(self.L.vgb_geometry_device_bytes(self.handle, ctypes.byref(out)))
         return out.value
+
+    # -- ingestion and export formats ---------------------------------------
+    def _sized(self, fn) -> bytes:
+        n = ctypes.c_size_t()
+        check(fn(self.handle, None, 0, ctypes.byref(n)))
+        buf = ctypes.create_string_buffer(n.value)
+        check(fn(self.handle, buf, n.value, ctypes.byref(n)))
+        return buf.raw[:n.value]
+
+    def Serialize(self) -> bytes:
+        """The flat image of the geometry (vgb_geometry_serialize)."""
+        return self._sized(self.L.vgb_geometry_serialize)
+
+    def Save(self, path: str) -> None:
+        check(self.L.vgb_geometry_save(self.handle, os.fsencode(path)))
+
+    def ExportCpp(self) -> str:
+        """C++ source rebuilding the geometry with VecGeom's API
+        (GeomCppExporter::DumpGeometry, source/CppExporter.cpp)."""
+        return self._sized(self.L.vgb_geometry_export_cpp).decode()
+
+    @classmethod
+    def _adopt(cls, library, handle) -> "Geometry":
+        g = cls.__new__(cls)
+        g.L = library if library is not None else L.lib()
+        g.handle = handle
+        g.closed = False
+        g.world = None
+        return g
+
+    @classmethod
+    def FromImage(cls, data: bytes, library=None) -> "Geometry":
+        """A new open geometry from a flat image; ids as in the image."""
+        lib = library if library is not None else L.lib()
+        h = ctypes.c_void_p()
+        check(lib.vgb_geometry_deserialize(data, len(data), ctypes.byref(h)))
+        return cls._adopt(lib, h)
+
+    @classmethod
+    def Load(cls, path: str, library=None) -> "Geometry":
+        lib = library if library is not None else L.lib()
+        h = ctypes.c_void_p()
+        check(lib.vgb_geometry_load(os.fsencode(path), ctypes.byref(h)))
+        return cls._adopt(lib, h)
 
 
 # ---------------------------------------------------------------------------
