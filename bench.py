@@ -15,7 +15,10 @@ point batch through libvgb.  Workloads (seeded synthetic inputs):
           ops (DistanceToOut/SafetyToOut on the inside subset).
 value = point-ops / device time (inputs resident in HBM, L2 flushed before
 every op, CUDA events around each launch); e2e = the same ops through the
-public API with pinned host buffers (copies inside the timed region).
+public API with pinned host buffers (copies inside the timed region): per
+shape one vgb_batch_fused call for the ops on all points and one for the ops
+on the Contains() subset, so each point set crosses PCIe once; e2e_per_op =
+the same with one vgb_batch call per op.
 Rank 0 prints one JSON line.
 """
 from __future__ import annotations
@@ -576,6 +579,8 @@ def main():
         return torch.from_numpy(np.ascontiguousarray(a)).cuda()
 
     tasks = []   # (shape, opname, n, callable on device, callable on host)
+    fused_calls = []  # end-to-end: one fused host-buffer call per point set
+    fused_h2d = fused_d2h = 0
     checks = []  # (shape, opname, output, FP64 output, FP64 call) for the error report
     h2d_bytes = d2h_bytes = 0
     for si, (name, spec) in enumerate(shapes.items()):
@@ -631,6 +636,19 @@ def main():
                 h2d_bytes += m * 24
             d2h_bytes += m * out_d.element_size()
             tasks.append((name, opname, m, run_d, run_h))
+        # the fused end-to-end form: all points (Inside, Contains, SafetyToIn,
+        # DistanceToIn) and the Contains() subset (SafetyToOut, DistanceToOut)
+        code = {"contains": 0, "inside": 1, "distance_to_in": 2, "distance_to_out": 3,
+                "safety_to_in": 4, "safety_to_out": 5}
+        for local, (hp, hd, hs, m) in ((False, (HP, HD, HS, n)), (True, (HPS, HDS, HSS, ns))):
+            sel_ops = [o for o in OPS if (o in LOCAL_OPS) == local]
+            outs = {code[o]: torch.empty(m, dtype={"contains": torch.uint8, "inside": torch.int32}
+                                         .get(o, torch.float64)).pin_memory() for o in sel_ops}
+            mask = sum(1 << code[o] for o in sel_ops)
+            fused_calls.append(lambda pv=pv, mask=mask, hp=hp, hd=hd, hs=hs, outs=outs:
+                               pv.fused(mask, hp, outs, hd, hs))
+            fused_h2d += m * 56
+            fused_d2h += sum(v.element_size() * m for v in outs.values())
 
     # L2 flush: a read sweep over 256 MB (> 126 MB L2); reading leaves clean lines,
     # so the next kernel pays no write-back for the flush itself
@@ -698,24 +716,33 @@ def main():
             "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"}
 
     # end-to-end through the public API with pinned host buffers
-    e2e = None
+    e2e = e2e_per_op = None
     if not args.no_e2e:
-        for _ in range(2):
-            for t in tasks:
-                t[4]()
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        e2e_steps = max(1, min(args.steps, 3))
-        for _ in range(e2e_steps):
-            for t in tasks:
-                t[4]()
-        e2e_s = (time.perf_counter() - t0) / e2e_steps
-        if world > 1:
-            tt = torch.tensor([e2e_s], device="cuda")
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            e2e_s = float(tt.item())
+        def timed_wall(calls):
+            for _ in range(2):
+                for c in calls:
+                    c()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            reps = max(1, min(args.steps, 3))
+            for _ in range(reps):
+                for c in calls:
+                    c()
+            sec = (time.perf_counter() - t0) / reps
+            if world > 1:
+                tt = torch.tensor([sec], device="cuda")
+                dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+                sec = float(tt.item())
+            return sec
+        e2e_s = timed_wall(fused_calls)
         e2e = {"value": round(world * pts_per_step / e2e_s / 1e6, 2), "unit": "Mpoints/s",
-               "h2d_bytes_per_step": int(h2d_bytes), "d2h_bytes_per_step": int(d2h_bytes)}
+               "h2d_bytes_per_step": int(fused_h2d), "d2h_bytes_per_step": int(fused_d2h),
+               "api": "vgb_batch_fused, host buffers, 2 calls per shape"}
+        e2e_s = timed_wall([t[4] for t in tasks])
+        e2e_per_op = {"value": round(world * pts_per_step / e2e_s / 1e6, 2),
+                      "unit": "Mpoints/s", "h2d_bytes_per_step": int(h2d_bytes),
+                      "d2h_bytes_per_step": int(d2h_bytes),
+                      "api": "vgb_batch, host buffers, 1 call per op"}
 
     per_op = {f"{t[0]}:{t[1]}": round(t[2] / (per_task_ms[i] / args.steps * 1e-3) / 1e6, 1)
               for i, t in enumerate(tasks)}
@@ -745,7 +772,7 @@ def main():
             "data": "synthetic (seeded)",
             "config": dict(workload_desc(args.workload, n, args.precision),
                            l2="flushed (256 MB read sweep) before every op, outside the events"),
-            "per_op_mpoints_s": per_op, "roofline": roof, "e2e": e2e,
+            "per_op_mpoints_s": per_op, "roofline": roof, "e2e": e2e, "e2e_per_op": e2e_per_op,
             "error_vs_fp64": err,
             "gpu_launches": launches, "clocks": clk}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -259,3 +259,47 @@ def test_fp32_refine_equals_fp64(kind, placement):
         torch.cuda.synchronize()
         same = (a == b) | (torch.isnan(a) & torch.isnan(b)) if dt == torch.float64 else a == b
         assert bool(same.all()), f"{kind} {meth}: {int((~same).sum())} differ"
+
+
+FUSED_OPS = {"contains": 0, "inside": 1, "distance_to_in": 2, "distance_to_out": 3,
+             "safety_to_in": 4, "safety_to_out": 5}
+
+
+def fused_against_per_op(spec, n, seed, on_device):
+    """vgb_batch_fused over all six ops equals six vgb_batch calls, bit for bit."""
+    import torch
+    import vecgeom_b200 as V
+    from vecgeom_b200 import workloads as W
+    wl = W.make_workload(spec, n, seed)
+    g, pv = build_placed(spec, "generic")
+    pts, dirs = (wl.x, wl.y, wl.z), (wl.dx, wl.dy, wl.dz)
+    want = run_all_ops(pv, pts, dirs, pts, dirs, wl.step)
+    conv = dev if on_device else (lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory())
+    dt = {"contains": torch.uint8, "inside": torch.int32}
+    outs = {k: torch.zeros(n, dtype=dt.get(k, torch.float64),
+                           device="cuda" if on_device else "cpu") for k in FUSED_OPS}
+    if not on_device:
+        outs = {k: v.pin_memory() for k, v in outs.items()}
+    pv.fused(0x3f, V.SOA3D(*(conv(a) for a in pts)), {FUSED_OPS[k]: v for k, v in outs.items()},
+             V.SOA3D(*(conv(a) for a in dirs)), conv(wl.step))
+    torch.cuda.synchronize()
+    got = {k: v.cpu().numpy() for k, v in outs.items()}
+    for k in FUSED_OPS:
+        a, b = got[k], want[k]
+        same = (a == b) | (np.isnan(a) & np.isnan(b)) if a.dtype.kind == "f" else a == b
+        assert same.all(), f"{spec.kind} fused {k}: {np.flatnonzero(~same)[:5]}"
+
+
+@pytest.mark.parametrize("kind", sorted(VGB_SHAPES))
+@pytest.mark.parametrize("on_device", [True, False], ids=["device", "host"])
+def test_fused_equals_per_op(kind, on_device):
+    from vecgeom_b200 import workloads as W
+    fused_against_per_op(spec_of_kind(kind), 1 << 14, W.SEED_BASE + 41, on_device)
+
+
+@pytest.mark.parametrize("on_device", [True, False], ids=["device", "host"])
+def test_fused_host_staging_across_chunks(on_device):
+    """More points than one staging chunk (1 M), the last chunk ragged."""
+    from vecgeom_b200 import workloads as W
+    fused_against_per_op(spec_of_kind("sphere"), (1 << 20) * 2 + 4099, W.SEED_BASE + 43,
+                         on_device)

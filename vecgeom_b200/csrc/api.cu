@@ -206,9 +206,70 @@ vgb_status vgb_batch_fused(const vgb_geometry *gc, int32_t placed, uint32_t ops,
   io.n = n;
   io.ops = ops;
   io.flags = flags;
-  if (classify(x) != kPtrDevice)
-    return set_error(VGB_EINVAL, "vgb_batch_fused: needs device pointers");
-  return launch_fused_f64(gc, placed, io, static_cast<cudaStream_t>(stream));
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const PtrKind kx = classify(x);
+  bool all_host = kx == kPtrHost, all_dev = kx == kPtrDevice;
+  for (int k = 0; k < 6; ++k) {
+    if (!io.out[k]) continue;
+    const PtrKind ko = classify(io.out[k]);
+    all_host = all_host && ko == kPtrHost;
+    all_dev = all_dev && ko == kPtrDevice;
+  }
+  if (all_dev) return launch_fused_f64(gc, placed, io, s);
+  if (!all_host)
+    return set_error(VGB_EINVAL, "vgb_batch_fused: inputs and outputs must all be device or all host");
+
+  // host buffers: the points (and directions, steps) cross once per chunk for
+  // all the ops, on the two internal streams as in vgb_batch
+  vgb_geometry *g = const_cast<vgb_geometry *>(gc);
+  const int64_t chunk = n < (1 << 20) ? n : (1 << 20);
+  auto span = [&](size_t elem) { return ((chunk * elem + 255) / 256) * 256; };
+  size_t half = 3 * span(8) + (nd ? 4 * span(8) : 0);
+  for (int k = 0; k < 6; ++k)
+    if (io.out[k]) half += span(out_size(k));
+  std::lock_guard<std::mutex> lock(g->staging_mu);
+  if ((st = ensure_staging(g, 2 * half)) != VGB_OK) return st;
+  cudaStream_t *sts = g->staging_streams;
+  cudaError_t e = cudaEventRecord(g->staging_start, s);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(sts[0], g->staging_start, 0);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(sts[1], g->staging_start, 0);
+  if (e != cudaSuccess) return cuda_error(e, "vgb_batch_fused: stream ordering");
+  char *base = static_cast<char *>(g->staging);
+  const double *hin[7] = {x, y, z, dx, dy, dz, step_max};
+  for (int64_t b = 0, c = 0; b < n; b += chunk, ++c) {
+    const int64_t m = (n - b < chunk) ? (n - b) : chunk;
+    cudaStream_t cs = sts[c & 1];
+    char *p = base + (c & 1) * half;
+    double *din[7] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    for (int i = 0; i < (nd ? 7 : 3); ++i) {
+      din[i] = reinterpret_cast<double *>(p);
+      p += span(8);
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync(din[i], hin[i] + b, m * sizeof(double), cudaMemcpyHostToDevice, cs);
+    }
+    if (e != cudaSuccess) return cuda_error(e, "vgb_batch_fused: host-to-device copy");
+    FusedIO cio = io;
+    cio.x = din[0]; cio.y = din[1]; cio.z = din[2];
+    cio.dx = din[3]; cio.dy = din[4]; cio.dz = din[5]; cio.step = din[6];
+    for (int k = 0; k < 6; ++k) {
+      if (!io.out[k]) continue;
+      cio.out[k] = p;
+      p += span(out_size(k));
+    }
+    cio.n = m;
+    if ((st = launch_fused_f64(gc, placed, cio, cs)) != VGB_OK) return st;
+    for (int k = 0; k < 6 && e == cudaSuccess; ++k) {
+      if (!io.out[k]) continue;
+      const size_t osz = out_size(k);
+      e = cudaMemcpyAsync(static_cast<char *>(io.out[k]) + b * osz, cio.out[k], m * osz,
+                          cudaMemcpyDeviceToHost, cs);
+    }
+    if (e != cudaSuccess) return cuda_error(e, "vgb_batch_fused: device-to-host copy");
+  }
+  e = cudaStreamSynchronize(sts[0]);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(sts[1]);
+  if (e != cudaSuccess) return cuda_error(e, "vgb_batch_fused: synchronize");
+  return VGB_OK;
 }
 
 vgb_status vgb_Contains(const vgb_geometry *g, int32_t placed, int64_t n, const double *x,
