@@ -119,14 +119,58 @@ class ClockSampler:
         self._thread = None
         self.err = None
 
+    def _handle(self, N):
+        """NVML handle of this process's GPU: by index, else by the UUID CUDA
+        reports (NVML's numbering can differ from CUDA's in a container)."""
+        try:
+            return N.nvmlDeviceGetHandleByIndex(self.index)
+        except Exception:  # noqa: BLE001
+            import torch
+            uuid = str(torch.cuda.get_device_properties(self.index).uuid)
+            return N.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+
+    def _smi_loop(self, err):
+        """Fallback: nvidia-smi's query loop (reads only)."""
+        import torch
+        uuid = str(torch.cuda.get_device_properties(self.index).uuid)
+        uuid = uuid if uuid.startswith("GPU-") else "GPU-" + uuid
+        cmd = ["nvidia-smi", "-i", uuid, "--query-gpu=clocks.sm,clocks.max.sm,"
+               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+               "--format=csv,noheader,nounits", "-lms", "50"]
+        try:
+            proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError as e:
+            self.err = f"{err}; nvidia-smi unavailable: {e}"
+            return
+
+        def loop():
+            names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+            for line in proc.stdout:
+                if self._stop.is_set():
+                    break
+                f = [v.strip() for v in line.split(",")]
+                try:
+                    self.samples.append(float(f[0]))
+                    self.max_mhz = float(f[1])
+                except (ValueError, IndexError):
+                    continue
+                for name, v in zip(names, f[2:]):
+                    if v.lower() == "active":
+                        self.reasons.add(name)
+            proc.terminate()
+        self._proc = proc
+        self._thread = threading.Thread(target=loop, daemon=True)
+        self._thread.start()
+
     def start(self):
         try:
             import pynvml as N
             N.nvmlInit()
-            h = N.nvmlDeviceGetHandleByIndex(self.index)
+            h = self._handle(N)
             self.max_mhz = float(N.nvmlDeviceGetMaxClockInfo(h, N.NVML_CLOCK_SM))
         except Exception as e:  # noqa: BLE001
-            self.err = f"nvml unavailable: {e}"
+            self._smi_loop(f"nvml unavailable: {e}")
             return
 
         def loop():
@@ -146,6 +190,13 @@ class ClockSampler:
 
     def stop(self) -> dict:
         self._stop.set()
+        proc = getattr(self, "_proc", None)
+        if proc is not None:
+            proc.terminate()
+            try:
+                proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                proc.kill()
         if self._thread is not None:
             self._thread.join(timeout=2)
         if not self.samples:
@@ -640,8 +691,9 @@ def main():
         # DistanceToIn) and the Contains() subset (SafetyToOut, DistanceToOut)
         code = {"contains": 0, "inside": 1, "distance_to_in": 2, "distance_to_out": 3,
                 "safety_to_in": 4, "safety_to_out": 5}
-        for local, (hp, hd, hs, m) in ((False, (HP, HD, HS, n)), (True, (HPS, HDS, HSS, ns))):
-            sel_ops = [o for o in OPS if (o in LOCAL_OPS) == local]
+        for on_subset, (hp, hd, hs, m) in ((False, (HP, HD, HS, n)),
+                                           (True, (HPS, HDS, HSS, ns))):
+            sel_ops = [o for o in OPS if (o in LOCAL_OPS) == on_subset]
             outs = {code[o]: torch.empty(m, dtype={"contains": torch.uint8, "inside": torch.int32}
                                          .get(o, torch.float64)).pin_memory() for o in sel_ops}
             mask = sum(1 << code[o] for o in sel_ops)

@@ -8,6 +8,8 @@
 // which make a device virtual call per point, with shape and op resolved at
 // compile time.
 #pragma once
+#include <type_traits>
+
 #include "shapes.cuh"
 
 namespace vgb {
@@ -49,13 +51,23 @@ constexpr int kStageMaxDoubles = 6144;  // 48 KB of dynamic shared memory
 extern __shared__ double vgb_stage[];
 
 // Distance kernels carry the most live state; they are compiled for four
-// resident 256-thread blocks per SM (64 registers); the others keep the
-// compiler's own choice (0: no minimum).
-template <int OP> struct MinBlocks {
+// resident 256-thread blocks per SM (64 registers), or the shape's own
+// `kDistanceBlocks` (five for tube and cone: 51 registers, more warps to hide
+// the FP64 latency; measured 5 % faster DistanceToIn, while the sphere and the
+// composite shapes spill at five); the others keep the compiler's own choice
+// (0: no minimum).
+template <class Ops, class = void> struct DistanceBlocks {
+  static constexpr int value = 4;
+};
+template <class Ops>
+struct DistanceBlocks<Ops, std::void_t<decltype(Ops::kDistanceBlocks)>> {
+  static constexpr int value = Ops::kDistanceBlocks;
+};
+template <class Ops, int OP> struct MinBlocks {
   static constexpr int value =
       (OP == VGB_OP_DISTANCE_TO_IN || OP == VGB_OP_DISTANCE_TO_OUT ||
        OP == VGB_OP_DISTANCE_TO_IN_MINIMIZE || OP == VGB_OP_DISTANCE_TO_OUT_NODE ||
-       OP == VGB_OP_PLACED_DISTANCE_TO_OUT) ? 4 : 0;
+       OP == VGB_OP_PLACED_DISTANCE_TO_OUT) ? DistanceBlocks<Ops>::value : 0;
 };
 
 template <class Ops, class P, int OP>
@@ -122,7 +134,7 @@ __device__ __forceinline__ void batch_loop(const P &prm, const DXform &X, const 
 }
 
 template <class Ops, class P, int OP>
-__global__ void __launch_bounds__(kBatchBlock, MinBlocks<OP>::value)
+__global__ void __launch_bounds__(kBatchBlock, MinBlocks<Ops, OP>::value)
     k_batch(const P prm, const DXform X, const BatchIO io) {
   if constexpr (Stageable<P>::value) {
     if (io.stage > 0) {

@@ -28,6 +28,7 @@ struct ConeP {
 };
 
 template <class R> struct ConeOps {
+  static constexpr int kDistanceBlocks = 5;  // resident blocks of the distance kernels
   using W = WedgeOps<R>;
   static constexpr double kHalfCarTol = kTolerance * 0.5;
   static constexpr double kHalfRadTol = kRadTolerance * 0.5;

@@ -22,6 +22,7 @@ struct TubeP {
 };
 
 template <class R> struct TubeOps {
+  static constexpr int kDistanceBlocks = 5;  // resident blocks of the distance kernels
   using W = WedgeOps<R>;
 
   // TubeUtilities::PointInCyclicalSector<onSurface=false> (:55-92)
