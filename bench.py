@@ -109,7 +109,7 @@ class ClockSampler:
                "sw_power_cap": "nvmlClocksEventReasonSwPowerCap",
                "hw_power_brake": "nvmlClocksEventReasonHwPowerBrakeSlowdown"}
 
-    def __init__(self, index: int, period_s: float = 0.005):
+    def __init__(self, index: int, period_s: float = 0.001):
         self.index = index
         self.period = period_s
         self.samples = []
