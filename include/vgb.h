@@ -326,8 +326,10 @@ vgb_status vgb_basket_graph_launch(vgb_basket_plan *plan, void *stream);
  * process exits), so it takes at most VGB_NOALLOC_MAX_BASKETS baskets and
  * returns VGB_ENOSPC beyond that.  It has no counterpart in the reference.
  *
- *  - baskets is a host array; it is read (copied to the device) before the call
- *    returns.  Launch shape: 256 threads per CTA, 1024 points per tile.
+ *  - baskets is a host array, pageable or pinned; the call copies it into a
+ *    host array of its own before the device copy starts, so the caller may
+ *    refill it as soon as the call returns.  Launch shape: 256 threads per CTA,
+ *    1024 points per tile.
  *  - The first call on each device looks up the array's device address; make
  *    that first call from a thread whose current device is the geometry's.
  *  - Every call reuses the same array and leaves its tables in it; nothing in

@@ -90,6 +90,56 @@ def test_noalloc_matches_the_plan_on_two_calls_in_a_row():
 
 
 @pytest.mark.gpu
+def test_noalloc_at_its_limit_with_empty_baskets():
+    """Exactly VGB_NOALLOC_MAX_BASKETS small baskets, every seventh one empty:
+    the table kernel then scans 8 baskets per thread and fills the last prefix
+    entry.  Compared with the plan on two calls in a row, the second from a
+    pinned host array that is overwritten as soon as the call returns."""
+    import torch
+    import vecgeom_b200 as V
+    from vecgeom_b200 import _lib
+    nb = _lib.NOALLOC_MAX_BASKETS
+    bs = W.config4_baskets(nb, seed=W.SEED_BASE + 65)
+    for b in bs:
+        b.n = min(b.n, 24)
+    g = V.Geometry()
+    placed, offsets, pts, dirs, step = W.build_baskets(g, bs)
+    g.CloseGeometry()
+    arrays = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in (*pts, *dirs, step)]
+    n = len(arrays[0])
+    table = [(pv, o, 0 if k % 7 == 3 else b.n)
+             for k, (pv, o, b) in enumerate(zip(placed, offsets, bs))]
+    want = _outs(n)
+    V.BasketPlan(g, table, DTI | STI).run(V.SOA3D(*arrays[:3]), V.SOA3D(*arrays[3:6]),
+                                          arrays[6], want)
+    got1 = _outs(n)
+    assert _noalloc(g, table, DTI | STI, arrays, got1) == 0
+    # second call from pinned host memory, scribbled over right after the call
+    L = V.lib()
+    pinned = torch.empty(nb * ctypes.sizeof(CBasket), dtype=torch.uint8).pin_memory()
+    arr = (CBasket * nb).from_address(pinned.data_ptr())
+    for k, (pv, off, cnt) in enumerate(table):
+        arr[k].placed, arr[k].offset, arr[k].count = pv.id, off, cnt
+    o = (ctypes.c_void_p * 6)()
+    got2 = _outs(n)
+    for op, t in got2.items():
+        o[op] = t.data_ptr()
+    assert L.vgb_basket_run_noalloc(g.handle, arr, nb, DTI | STI,
+                                    *(a.data_ptr() for a in arrays), o, 0, None) == 0
+    for k in range(nb):
+        arr[k].count = 0
+    torch.cuda.synchronize()
+    empty = torch.zeros(n, dtype=torch.bool, device="cuda")
+    for k, (pv, off, cnt) in enumerate(table):
+        if cnt == 0:
+            empty[off:off + bs[k].n] = True
+    for op in want:
+        assert _same(got1[op], want[op]), f"first call, op {op}"
+        assert _same(got2[op], want[op]), f"second call (pinned array), op {op}"
+        assert bool((got1[op][empty] == -5.).all()), "an empty basket was written"
+
+
+@pytest.mark.gpu
 def test_noalloc_rejects_more_baskets_than_its_table():
     import vecgeom_b200 as V
     from vecgeom_b200 import _lib

@@ -420,6 +420,11 @@ static __device__ __align__(256) unsigned char g_noalloc_tables[kNoallocBytes];
 constexpr int kMaxDevices = 64;
 std::mutex g_noalloc_mu;
 void *g_noalloc_addr[kMaxDevices] = {};
+// Host copy of the caller's basket records.  The library allocated it, so it is
+// plain pageable memory: cudaMemcpyAsync from it returns only once the driver has
+// staged the bytes, and the caller's own array (pinned or not) is never read after
+// the call returns.  Filled and copied under g_noalloc_mu.
+vgb_basket g_noalloc_host[kNoallocMax];
 
 // Device address of the array on `dev` (the current device); looked up once.
 vgb_status noalloc_tables(int dev, unsigned char **p) {
@@ -528,7 +533,11 @@ extern "C" vgb_status vgb_basket_run_noalloc(const vgb_geometry *g, const vgb_ba
   vgb_basket *raw = reinterpret_cast<vgb_basket *>(tables + kNoallocRawOff);
   BasketRec *rec = reinterpret_cast<BasketRec *>(tables + kNoallocRecOff);
   int64_t *prefix = reinterpret_cast<int64_t *>(tables + kNoallocPrefixOff);
-  e = cudaMemcpyAsync(raw, baskets, sizeof(vgb_basket) * nb, cudaMemcpyHostToDevice, s);
+  {
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    std::memcpy(g_noalloc_host, baskets, sizeof(vgb_basket) * nb);
+    e = cudaMemcpyAsync(raw, g_noalloc_host, sizeof(vgb_basket) * nb, cudaMemcpyHostToDevice, s);
+  }
   if (e != cudaSuccess) return cuda_error(e, "vgb_basket_run_noalloc: basket copy");
   k_noalloc_tables<<<1, 1024, 0, s>>>(raw, nb, g->dev.placed, kNoallocTile, rec, prefix);
   FusedIO io;
