@@ -73,11 +73,7 @@ NCU_TRAFFIC_PER_POINT = {
 
 def workload_shapes(name: str):
     from vecgeom_b200 import workloads as W
-    if name == "box":
-        return {"box": W.config1_box()}, 1 << 20, "uniform"
-    if name == "heavy":
-        return W.config3_shapes(), 1 << 22, "mixed"
-    return W.config2_shapes(), 1 << 22, "mixed"
+    return W.bench_config(name)
 
 
 def workload_desc(name, n, precision):
@@ -635,7 +631,7 @@ def main():
     checks = []  # (shape, opname, output, FP64 output, FP64 call) for the error report
     h2d_bytes = d2h_bytes = 0
     for si, (name, spec) in enumerate(shapes.items()):
-        wl = W.make_workload(spec, n, W.SEED_BASE + 1000 * rank + si, mix=mix)
+        wl = W.make_workload(spec, n, W.bench_seed(si, rank), mix=mix)
         pv = placed[name]
         P = V.SOA3D(dev(wl.x), dev(wl.y), dev(wl.z))
         D = V.SOA3D(dev(wl.dx), dev(wl.dy), dev(wl.dz))

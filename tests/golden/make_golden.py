@@ -5,7 +5,7 @@ the reference sources by ``make -C oracle ref``) on seeded inputs and stores
 inputs + outputs as .npz fixtures.  The fixtures travel with the repository,
 so the parity tests need neither the reference tree nor its build.
 
-    python tests/golden/make_golden.py [shape ...]
+    python tests/golden/make_golden.py [--placement NAME] [shape ...]
 """
 from __future__ import annotations
 
@@ -82,6 +82,11 @@ def make_case(ref, name: str, spec, placement: str, seed: int) -> dict:
 
 
 def main(argv) -> None:
+    only = None
+    if "--placement" in argv:
+        k = argv.index("--placement")
+        only = argv[k + 1]
+        argv = argv[:k] + argv[k + 2:]
     ref = oracle.RefLib()
     shapes = shape_specs()
     names = argv or list(shapes)
@@ -92,6 +97,8 @@ def main(argv) -> None:
         # other fixtures unchanged
         base = W.SEED_BASE + 10 * (zlib.crc32(name.encode()) % 100000)
         for j, placement in enumerate(PLACEMENTS):
+            if only is not None and placement != only:
+                continue
             case = make_case(ref, name, shapes[name], placement, base + j)
             path = os.path.join(HERE, f"{name}_{placement}.npz")
             np.savez_compressed(path, **case)

@@ -32,6 +32,10 @@ PLACEMENTS = {
     "translated": (5., -3., 7., 0., 0., 0.),
     "rotz90": (1., 2., 3., 90., 0., 0.),     # drops the 6e-17 entries (code 0x10a-like)
     "generic": (-4., 6., 2.5, 30., 45., 60.),
+    # nonzero entries r1, r3, r5, r6, r8 only: rotation code 0x16A, whose
+    # specialised transform carries the reference's typo (third row
+    # m2*R5 + m2*R8, base/Transformation3D.h:388-392)
+    "quirk16a": (2., -1., 3., 0., 30., 90.),
 }
 
 

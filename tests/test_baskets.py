@@ -1,12 +1,19 @@
 """Baskets: many shape instances of mixed types in one persistent launch.
 
-The basket kernel runs the same per-point functions as vgb_batch_fused, so its
-results must equal, bit for bit, one fused call per basket; the tuned launch
-shape and the CUDA-graph replay must not change them.
+The mixed-basket workload (lognormal basket sizes, the eight benchmark kinds
+with lengths jittered +-20%, random Euler placements and translations) is
+checked against the reference itself: every basket's shape is built in the
+reference (oracle/_ref) with its own Transformation3D(tx, ty, tz, phi, theta,
+psi) (source/Transformation3D.cpp:36-55) and runs the basket's points there.
+The tuned launch shape and the CUDA-graph replay must not change the results.
 """
+import os
+
 import numpy as np
 import pytest
 
+import oracle
+from helpers import assert_distances, assert_exact, assert_torus_distances, ref_unplaced
 from vecgeom_b200 import workloads as W
 
 DTI, STI = 1 << 2, 1 << 4  # op masks: DistanceToIn, SafetyToIn
@@ -45,19 +52,6 @@ def _outs(n, ops):
             for op in range(6) if (ops >> op) & 1}
 
 
-def _per_basket(placed, offsets, bs, P, D, step, ops):
-    import vecgeom_b200 as V
-    n = P.size()
-    ref = _outs(n, ops)
-    for pv, off, b in zip(placed, offsets, bs):
-        if b.n == 0:
-            continue
-        sl = slice(off, off + b.n)
-        pv.fused(ops, V.SOA3D(P.x[sl], P.y[sl], P.z[sl]), {k: v[sl] for k, v in ref.items()},
-                 dirs=V.SOA3D(D.x[sl], D.y[sl], D.z[sl]), step_max=step[sl])
-    return ref
-
-
 def _same(a, b):
     import torch
     if a.dtype == torch.float64:
@@ -65,20 +59,73 @@ def _same(a, b):
     return bool((a == b).all())
 
 
+def _reference_baskets(bs, offsets, pts, dirs, step, ops):
+    """Every basket through the reference: its jittered shape at its own Euler
+    placement; sphere DistanceToIn through USolids' USphere (the reference's
+    own is a stub)."""
+    ref = oracle.RefLib()
+    threads = os.cpu_count() or 1
+    n = len(pts[0])
+    want = {op: oracle.out_array(op, n) for op in range(6) if (ops >> op) & 1}
+    for off, b in zip(offsets, bs):
+        if b.n == 0:
+            continue
+        sl = slice(off, off + b.n)
+        p = tuple(np.ascontiguousarray(a[sl]) for a in pts)
+        d = tuple(np.ascontiguousarray(a[sl]) for a in dirs)
+        s = np.ascontiguousarray(step[sl])
+        rpv = ref.placed(ref_unplaced(ref, b.spec), *b.place)
+        for op in want:
+            if op == oracle.DISTANCE_TO_IN and b.spec.kind == "sphere":
+                want[op][sl] = ref.usphere_distance_to_in(b.spec.params, ref.last_transform, p, d,
+                                                          nthreads=threads)
+            elif op in (oracle.DISTANCE_TO_IN, oracle.DISTANCE_TO_OUT):
+                want[op][sl] = ref.batch(rpv, op, p, d, s, nthreads=threads)
+            else:
+                want[op][sl] = ref.batch(rpv, op, p, nthreads=threads)
+    return want
+
+
 @pytest.mark.gpu
-@pytest.mark.parametrize("ops", [DTI | STI, ALL], ids=["dti_sti", "all_ops"])
-def test_baskets_match_per_basket_calls(ops):
+@pytest.mark.skipif(not oracle.RefLib.available(), reason="oracle/_ref not built")
+@pytest.mark.parametrize("ops,nb", [(DTI | STI, 320), (ALL, 96)], ids=["dti_sti", "all_ops"])
+def test_baskets_match_the_reference(ops, nb):
+    """nb baskets of the mixed workload (one of them empty), each with its own
+    random placement and jittered parameters, against the reference."""
     import torch
     import vecgeom_b200 as V
-    g, bs, placed, offsets, P, D, step = _setup(96, W.SEED_BASE + 41)
+    bs = W.config4_baskets(nb, seed=W.SEED_BASE + 41)
+    for b in bs:
+        b.n = min(b.n, 4096)
+    bs[3].n = 0
+    g = V.Geometry()
+    placed, offsets, pts, dirs, step = W.build_baskets(g, bs)
+    g.CloseGeometry()
+    dev = lambda a: torch.from_numpy(a).cuda()  # noqa: E731
+    P = V.SOA3D(*(dev(a) for a in pts))
+    D = V.SOA3D(*(dev(a) for a in dirs))
     plan = V.BasketPlan(g, [(pv, o, b.n) for pv, o, b in zip(placed, offsets, bs)], ops)
     got = _outs(P.size(), ops)
-    plan.run(P, D, step, got)
+    plan.run(P, D, dev(step), got)
     torch.cuda.synchronize()
-    want = _per_basket(placed, offsets, bs, P, D, step, ops)
-    torch.cuda.synchronize()
-    for op in got:
-        assert _same(got[op], want[op]), f"op {op} differs"
+    got = {op: v.cpu().numpy() for op, v in got.items()}
+    want = _reference_baskets(bs, offsets, pts, dirs, step, ops)
+    kinds = set()
+    for off, b in zip(offsets, bs):
+        if b.n == 0:
+            continue
+        kinds.add(b.spec.kind)
+        sl = slice(off, off + b.n)
+        what = f"basket at {off} ({b.spec.kind}, {b.n} points, placement {b.place})"
+        for op in got:
+            g_, w_ = got[op][sl], want[op][sl]
+            if op in (oracle.CONTAINS, oracle.INSIDE):
+                assert_exact(g_, w_, f"{what} op {op}")
+            elif b.spec.kind == "torus" and op in (oracle.DISTANCE_TO_IN, oracle.DISTANCE_TO_OUT):
+                assert_torus_distances(g_, w_, b.spec.params, what=f"{what} op {op}")
+            else:
+                assert_distances(g_, w_, f"{what} op {op}")
+    assert kinds == set(W.BASKET_KINDS)
 
 
 @pytest.mark.gpu

@@ -77,3 +77,32 @@ def test_host_build_matches_reference(hc, path):
     assert_distances(host_run(hc, g, pv, 5, pl), d["safety_to_out"], "SafetyToOut")
     assert_distances(host_run(hc, g, pv, 2, pm, dm, step), d["distance_to_in"], "DistanceToIn")
     assert_distances(host_run(hc, g, pv, 3, pl, dl, step), d["distance_to_out"], "DistanceToOut")
+
+
+def test_host_build_matches_reference_on_mixed_baskets(hc):
+    """256 baskets of the mixed workload (jittered shapes of the eight kinds at
+    random Euler placements and translations), every op, host build against the
+    reference; the GPU runs the same comparison through the basket kernel."""
+    import oracle
+    from helpers import assert_distances, assert_exact
+    from test_baskets import _reference_baskets
+    if not oracle.RefLib.available():
+        pytest.skip("oracle/_ref not built")
+    bs = W.config4_baskets(256, seed=W.SEED_BASE + 49)
+    for b in bs:
+        b.n = min(b.n, 512)
+    g = Geometry(library=hc)
+    placed, offsets, pts, dirs, step = W.build_baskets(g, bs)
+    want = _reference_baskets(bs, offsets, pts, dirs, step, 0x3f)
+    for pv, off, b in zip(placed, offsets, bs):
+        sl = slice(off, off + b.n)
+        p = tuple(a[sl] for a in pts)
+        d = tuple(a[sl] for a in dirs)
+        what = f"basket at {off} ({b.spec.kind}, placement {b.place})"
+        for op in range(6):
+            got = host_run(hc, g, pv, op, p, d if op in (2, 3) else None,
+                           np.ascontiguousarray(step[sl]) if op in (2, 3) else None)
+            if op < 2:
+                assert_exact(got, want[op][sl], f"{what} op {op}")
+            else:
+                assert_distances(got, want[op][sl], f"{what} op {op}")

@@ -1,14 +1,22 @@
 """Navigation server (continuous batching) on the layered detector.
 
 Each request's per-track results (step count, final point, FNV-1a hash of its
-(next placed id, step, safety) records) must equal what vgb_nav_trace produces for the
-same tracks, whether the request is served alone or while other requests of
-uneven sizes arrive and finish around it.
+(next placed id, step, safety) records) must equal the reference's own
+SimpleNavigator trace of the same tracks (FindNextBoundaryAndStep + GetSafety,
+navigation/SimpleNavigator.h:340-596, run by oracle/_ref in a fresh process),
+whether the request is served alone or while other requests of uneven sizes
+arrive and finish around it.
 """
+import os
+import sys
+
 import numpy as np
 import pytest
 
+import oracle
 from vecgeom_b200 import workloads as W
+
+HERE = os.path.dirname(os.path.abspath(__file__))
 
 MAX_STEPS = 48
 
@@ -48,9 +56,24 @@ def requests(sizes, seed):
     return out
 
 
-def trace_truth(g, pts, dirs):
-    from test_navigation import gpu_trace
-    ids, steps, saf, nst = gpu_trace(g, pts, dirs, MAX_STEPS)
+def reference_truth(reqs):
+    """Per request: the reference's trace results of its tracks (one traced
+    batch of all requests' tracks, split back per request)."""
+    sys.path.insert(0, os.path.join(HERE, "golden"))
+    from make_nav_golden import reference_trace_isolated
+    pts = tuple(np.concatenate([r[0][j] for r in reqs]) for j in range(3))
+    dirs = tuple(np.concatenate([r[1][j] for r in reqs]) for j in range(3))
+    ids, steps, saf, nst = reference_trace_isolated(pts, dirs, MAX_STEPS, os.cpu_count() or 1)
+    out, b = [], 0
+    for r in reqs:
+        m = len(r[0][0])
+        sl = slice(b * MAX_STEPS, (b + m) * MAX_STEPS)
+        out.append(truth_of(r[0], r[1], ids[sl], steps[sl], saf[sl], nst[b:b + m]))
+        b += m
+    return out
+
+
+def truth_of(pts, dirs, ids, steps, saf, nst):
     n = len(pts[0])
     ids = ids.reshape(n, MAX_STEPS)
     steps = steps.reshape(n, MAX_STEPS)
@@ -93,13 +116,14 @@ def assert_same(res, want, what):
 
 
 @pytest.mark.gpu
-def test_served_alone_and_in_the_mix_match_the_trace():
+@pytest.mark.skipif(not oracle.RefLib.available(), reason="oracle/_ref not built")
+def test_served_alone_and_in_the_mix_match_the_reference():
     import vecgeom_b200 as V
-    g = V.Geometry()
-    W.build_detector(W.VgbBuilder(g))
     sizes = [300, 17, 1000, 1, 513, 2048, 64, 777]
     reqs = requests(sizes, W.SEED_BASE + 91)
-    truth = [trace_truth(g, *r) for r in reqs]
+    truth = reference_truth(reqs)
+    g = V.Geometry()
+    W.build_detector(W.VgbBuilder(g))
     # small slot table so admission has to wait for retirements
     for precision in (0, 1):
         srv = V.NavServer(g, max_tracks=2560, steps_per_launch=5, max_steps=MAX_STEPS,

@@ -439,6 +439,26 @@ def config3_shapes(seed: int = SEED_BASE + 3) -> dict:
     }
 
 
+def bench_config(name: str):
+    """(shapes, points per shape, point mix) of a benchmark workload: "box"
+    (the box, 2^20 points uniform in 1.5x its box), "shapes" (tube, cone,
+    sphere, 2^22 mixed points each) or "heavy" (torus, polycone, polyhedron,
+    box minus tube, 2^22 mixed points each)."""
+    if name == "box":
+        return {"box": config1_box()}, 1 << 20, "uniform"
+    if name == "heavy":
+        return config3_shapes(), 1 << 22, "mixed"
+    if name == "shapes":
+        return config2_shapes(), 1 << 22, "mixed"
+    raise ValueError(name)
+
+
+def bench_seed(shape_index: int, rank: int = 0) -> int:
+    """Seed of the points of the shape_index-th shape of a benchmark workload
+    on one rank (every rank draws its own batch)."""
+    return SEED_BASE + 1000 * rank + shape_index
+
+
 def build_unplaced(geom, spec: ShapeSpec) -> int:
     """Create spec's unplaced shape in a vecgeom_b200.Geometry; returns its id."""
     p = spec.params
