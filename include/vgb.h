@@ -97,6 +97,15 @@ const char *vgb_version(void);
 int64_t vgb_launch_count(void);
 void vgb_launch_count_reset(void);
 
+/* Measurement support, no counterpart in the reference: the FP64 (fp32 = 0) or
+ * FP32 (fp32 = 1) FMA throughput of the current GPU.  One launch of independent
+ * FMA chains filling every SM, `iters` FMAs per chain, timed with CUDA events
+ * on `stream` (synchronises it).  Returns the flops executed (an FMA counts 2)
+ * and the launch time; flops / ms is the peak the compute-bound kernels are
+ * reported against. */
+vgb_status vgb_measure_fma_peak(int32_t fp32, int32_t iters, void *stream, double *flops,
+                                float *ms);
+
 /* ---------------------------------------------------------------------------
  * Geometry construction and upload.
  * Replaces the host object graph (Unplaced*, LogicalVolume, Transformation3D,

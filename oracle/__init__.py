@@ -21,6 +21,9 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libvgref.so")
+# the same reference build with its torus's atan2/sincos/cbrt correctly rounded
+# (ref_crlibm.cpp); every other object keeps the C library's functions
+REF_CR_SO = os.path.join(HERE, "_ref", "libvgref_crlibm.so")
 
 # or_op / or_shape (vgb_oracle.h)
 CONTAINS, INSIDE, DISTANCE_TO_IN, DISTANCE_TO_OUT, SAFETY_TO_IN, SAFETY_TO_OUT = range(6)
@@ -114,14 +117,16 @@ class Oracle:
 
 
 class RefLib:
-    """The reference VecGeom Scalar backend (oracle/_ref/libvgref.so)."""
+    """The reference VecGeom Scalar backend (oracle/_ref/libvgref.so); with
+    crlibm=True the build whose torus uses correctly rounded atan2/sin/cos/cbrt
+    (oracle/_ref/libvgref_crlibm.so)."""
 
     @staticmethod
-    def available() -> bool:
-        return os.path.exists(REF_SO)
+    def available(crlibm: bool = False) -> bool:
+        return os.path.exists(REF_CR_SO if crlibm else REF_SO)
 
-    def __init__(self):
-        L = ctypes.CDLL(REF_SO)
+    def __init__(self, crlibm: bool = False):
+        L = ctypes.CDLL(REF_CR_SO if crlibm else REF_SO)
         for name, argn in (("vgref_box", 3), ("vgref_tube", 5), ("vgref_cone", 7),
                            ("vgref_sphere", 6), ("vgref_torus", 5), ("vgref_trd", 5)):
             f = getattr(L, name)

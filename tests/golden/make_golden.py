@@ -36,6 +36,15 @@ def spec_json(spec) -> str:
     return json.dumps({"kind": spec.kind, "params": p})
 
 
+_CR = []
+
+
+def _crlibm_ref():
+    if not _CR:
+        _CR.append(oracle.RefLib(crlibm=True))
+    return _CR[0]
+
+
 def make_case(ref, name: str, spec, placement: str, seed: int) -> dict:
     wl = W.make_workload(spec, N, seed)
     # near-surface etc. are drawn in the shape's frame; move them to the mother
@@ -72,6 +81,17 @@ def make_case(ref, name: str, spec, placement: str, seed: int) -> dict:
         use_dir = op in (oracle.DISTANCE_TO_IN, oracle.DISTANCE_TO_OUT)
         out[opname] = ref.batch(pv, op, pts, dirs if use_dir else None,
                                 wl.step if use_dir else None)
+    if spec.kind == "torus" and oracle.RefLib.available(crlibm=True):
+        # the reference's torus with correctly rounded atan2/sin/cos/cbrt
+        # (oracle/ref_crlibm.cpp): its distances move with the C library's last
+        # bits, and these are the values of a correctly rounding library
+        cr = _crlibm_ref()
+        tc = cr.L.vgref_transform_euler(tx, ty, tz, phi, theta, psi)
+        pvc = cr.L.vgref_place(cr.L.vgref_logical(name.encode(), ref_unplaced(cr, spec)), tc)
+        out["distance_to_in_crlibm"] = cr.batch(pvc, oracle.DISTANCE_TO_IN, pts_m, dirs_m,
+                                                wl.step)
+        out["distance_to_out_crlibm"] = cr.batch(pvc, oracle.DISTANCE_TO_OUT, pts_l, dirs_l,
+                                                 wl.step)
     if spec.kind == "sphere":
         # the reference's sphere DistanceToIn is a stub returning kInfinity
         # (volumes/kernel/SphereImplementation.h:84-93); pin it to USolids'

@@ -185,8 +185,9 @@ def reference_basket_isolated(pts, dirs, pstep, priors=BASKET_PRIORS, geometry="
     return isolated(_basket, pts, dirs, pstep, priors, geometry)
 
 
-def _traced(pts, dirs, max_steps, nthreads, geometry, navigator):
-    return reference_trace(oracle.RefLib(), pts, dirs, max_steps, nthreads, geometry, navigator)
+def _traced(pts, dirs, max_steps, nthreads, geometry, navigator, crlibm=False):
+    return reference_trace(oracle.RefLib(crlibm=crlibm), pts, dirs, max_steps, nthreads, geometry,
+                           navigator)
 
 
 def _boxes(geometry):
@@ -202,8 +203,10 @@ def isolated(fn, *args):
 
 
 def reference_trace_isolated(pts, dirs, max_steps=MAX_STEPS, nthreads=1, geometry="detector",
-                             navigator="simple"):
-    return isolated(_traced, pts, dirs, max_steps, nthreads, geometry, navigator)
+                             navigator="simple", crlibm=False):
+    """The trace in a fresh process; crlibm=True traces with the reference build
+    whose torus takes correctly rounded atan2/sin/cos/cbrt."""
+    return isolated(_traced, pts, dirs, max_steps, nthreads, geometry, navigator, crlibm)
 
 
 def reference_boxes_isolated(geometry: str) -> np.ndarray:

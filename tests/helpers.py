@@ -6,16 +6,16 @@ Parity bar (the FP64 form against the reference Scalar backend):
   * distances and safeties: |a-b| <= 1e-9 mm or |a-b| <= 1e-12 |b|; both
     infinite with the same sign, or both NaN, also match.
 
-Torus distances on the GPU are the one exception.  The reference solves the
-torus quartic with complex cube roots built from atan2/cos/sin/cbrt
-(volumes/kernel/TorusImplementation.h:24-160) and polishes only some roots; its
-results move with the last bit of the C library's transcendentals, which differ
-from CUDA's by up to an ulp.  The host build of the same code (glibc) matches
-the reference at the strict bar; on the GPU the torus distances are held to
-  * |a-b| <= 1e-5 mm or 1e-6 |b| (the solver's own accuracy), and
-  * at most 1% of rays outside that (a root accepted by one libm and rejected by
-    the other), each of whose GPU hit points must lie on the torus surface
-    within 1e-6 mm.
+Torus distances are held to the same bar against the reference built with
+correctly rounded atan2/sin/cos/cbrt (oracle/_ref/libvgref_crlibm.so).  The
+reference solves the torus quartic with complex cube roots built from those C
+library functions (volumes/kernel/TorusImplementation.h:283-316) and its
+unpolished roots move with their last bits: on a few rays per hundred its own
+DistanceToIn changes by up to ~3e-7 mm between glibc (whose cbrt is not
+correctly rounded) and a correctly rounding library.  libvgb evaluates those
+functions correctly rounded on the host and the GPU (crmath.cuh), so it matches
+the correctly rounded build; against the glibc build it differs exactly on the
+rays where the two reference builds differ from each other.
 """
 from __future__ import annotations
 
@@ -59,56 +59,36 @@ def assert_distances(a, b, what: str = "") -> None:
                              f"got {np.asarray(a)[i].tolist()} want {np.asarray(b)[i].tolist()}")
 
 
-TORUS_ABS_TOL = 1e-5
-TORUS_REL_TOL = 1e-6
-TORUS_FLIP_FRACTION = 0.01
-TORUS_SURFACE_TOL = 1e-6
-
-
-def torus_surface_residual(params, x, y, z):
-    """Distance-like residual of local points to the nearest torus surface:
-    the rmax / rmin tubes and, for a phi sector, the two cut planes."""
-    r = np.hypot(x, y)
-    rho = np.hypot(r - params["rtor"], z)
-    res = np.abs(rho - params["rmax"])
-    if params["rmin"] > 0:
-        res = np.minimum(res, np.abs(rho - params["rmin"]))
-    if params["dphi"] < 2 * math.pi:
-        for ang in (params["sphi"], params["sphi"] + params["dphi"]):
-            # distance to the half-plane at angle ang, for points within the tube
-            dplane = np.abs(-math.sin(ang) * x + math.cos(ang) * y)
-            along = math.cos(ang) * x + math.sin(ang) * y
-            res = np.where((along > 0) & (rho <= params["rmax"] + TORUS_SURFACE_TOL),
-                           np.minimum(res, dplane), res)
-    return res
-
-
-def assert_torus_distances(got, want, params, p_local=None, v_local=None,
-                           what: str = "") -> dict:
-    """The GPU torus bar (module docstring).  p_local / v_local, when given, are
-    the point and the unit direction the shape arithmetic sees; the hit points
-    of rays outside the tolerance are then checked on the surface.  Returns the
-    error statistics."""
-    got = np.asarray(got, np.float64)
-    want = np.asarray(want, np.float64)
-    fin = np.isfinite(got) & np.isfinite(want)
-    with np.errstate(invalid="ignore"):
-        d = np.abs(got - want)
-        close = fin & ((d <= TORUS_ABS_TOL) | (d <= TORUS_REL_TOL * np.abs(want)))
-    ok = close | distances_match(got, want)
-    flips = np.flatnonzero(~ok)
-    stats = {"n": len(ok), "strict_mismatch": int((~distances_match(got, want)).sum()),
-             "flips": len(flips), "max_err_close": float(d[close].max()) if close.any() else 0.}
-    assert len(flips) <= max(2, TORUS_FLIP_FRACTION * len(ok)), f"{what}: {stats}"
-    hit = flips[np.isfinite(got[flips])]
-    if len(hit) and p_local is not None:
-        px, py, pz = (np.asarray(a, np.float64)[hit] for a in p_local)
-        vx, vy, vz = (np.asarray(a, np.float64)[hit] for a in v_local)
-        t = got[hit]
-        res = torus_surface_residual(params, px + t * vx, py + t * vy, pz + t * vz)
-        assert (res <= TORUS_SURFACE_TOL).all(), \
-            f"{what}: GPU hit points off the surface: {res.tolist()} at {hit.tolist()}"
+def assert_torus_distances(got, want_crlibm, want_glibc=None, what: str = "") -> dict:
+    """The torus bar (module docstring): the parity bar against the reference
+    built with correctly rounded functions; returns the number of rays on which
+    the two reference builds themselves differ beyond the bar (where the glibc
+    build's value depends on its library's rounding)."""
+    assert_distances(got, want_crlibm, f"{what} (vs the reference with correctly rounded libm)")
+    stats = {"n": len(np.asarray(got))}
+    if want_glibc is not None:
+        stats["libm_dependent"] = int((~distances_match(want_glibc, want_crlibm)).sum())
+        stats["differ_from_glibc_build"] = int((~distances_match(got, want_glibc)).sum())
     return stats
+
+
+def reference_defined(spec, z_local) -> np.ndarray:
+    """Points on which the reference's result is defined.  Its polyhedron
+    Contains/Inside index the z-segment array with the number of z-planes below
+    the point (volumes/kernel/PolyhedronImplementation.h:350-370, :763, :809),
+    but its bounding tube reaches kTolerance beyond the end planes
+    (source/UnplacedPolyhedron.cpp:120-130): a point within that band above the
+    last plane reads one segment past the array, one at or just below the first
+    plane (Inside) reads segment -1.  That is undefined behaviour (it crashed the
+    reference on 2^22 near-surface points); libvgb clamps to the end segment.
+    Such points are left out of comparisons with the reference."""
+    z = np.asarray(z_local, np.float64)
+    ok = np.ones(len(z), bool)
+    if spec.kind == "polyhedron":
+        zp = np.asarray(spec.params["z"], np.float64)
+        band = 4e-9
+        ok &= ~((np.abs(z - zp[0]) <= band) | (np.abs(z - zp[-1]) <= band))
+    return ok
 
 
 def assert_exact(a, b, what: str = "") -> None:

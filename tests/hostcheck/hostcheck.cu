@@ -229,3 +229,19 @@ extern "C" int hc_nav_basket(vgb_geometry *g, int64_t n, const double *x, const 
   }
   return 0;
 }
+
+// The correctly rounded functions of crmath.cuh, element-wise over arrays
+// (fn: 0 atan2(a, b), 1 sin(a), 2 cos(a), 3 cbrt(a)).
+#include "../../vecgeom_b200/csrc/crmath.cuh"
+extern "C" int hc_crmath(int32_t fn, int64_t n, const double *a, const double *b, double *out) {
+  for (int64_t i = 0; i < n; ++i) {
+    switch (fn) {
+    case 0: out[i] = cr_atan2(a[i], b[i]); break;
+    case 1: out[i] = cr_sin(a[i]); break;
+    case 2: out[i] = cr_cos(a[i]); break;
+    case 3: out[i] = cr_cbrt(a[i]); break;
+    default: return -1;
+    }
+  }
+  return 0;
+}

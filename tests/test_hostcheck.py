@@ -75,8 +75,13 @@ def test_host_build_matches_reference(hc, path):
     assert_exact(host_run(hc, g, pv, 1, pm), d["inside"], "Inside")
     assert_distances(host_run(hc, g, pv, 4, pm), d["safety_to_in"], "SafetyToIn")
     assert_distances(host_run(hc, g, pv, 5, pl), d["safety_to_out"], "SafetyToOut")
-    assert_distances(host_run(hc, g, pv, 2, pm, dm, step), d["distance_to_in"], "DistanceToIn")
-    assert_distances(host_run(hc, g, pv, 3, pl, dl, step), d["distance_to_out"], "DistanceToOut")
+    # the torus takes correctly rounded atan2/sin/cos/cbrt: its distances are
+    # pinned to the reference built with those (the *_crlibm outputs)
+    sfx = "_crlibm" if spec.kind == "torus" else ""
+    assert_distances(host_run(hc, g, pv, 2, pm, dm, step), d["distance_to_in" + sfx],
+                     "DistanceToIn")
+    assert_distances(host_run(hc, g, pv, 3, pl, dl, step), d["distance_to_out" + sfx],
+                     "DistanceToOut")
 
 
 def test_host_build_matches_reference_on_mixed_baskets(hc):
@@ -93,16 +98,18 @@ def test_host_build_matches_reference_on_mixed_baskets(hc):
         b.n = min(b.n, 512)
     g = Geometry(library=hc)
     placed, offsets, pts, dirs, step = W.build_baskets(g, bs)
-    want = _reference_baskets(bs, offsets, pts, dirs, step, 0x3f)
+    want, keep = _reference_baskets(bs, offsets, pts, dirs, step, 0x3f)
     for pv, off, b in zip(placed, offsets, bs):
         sl = slice(off, off + b.n)
+        k = keep[sl]
         p = tuple(a[sl] for a in pts)
         d = tuple(a[sl] for a in dirs)
         what = f"basket at {off} ({b.spec.kind}, placement {b.place})"
         for op in range(6):
             got = host_run(hc, g, pv, op, p, d if op in (2, 3) else None,
                            np.ascontiguousarray(step[sl]) if op in (2, 3) else None)
+            w = want[("crlibm", op)] if b.spec.kind == "torus" and op in (2, 3) else want[op]
             if op < 2:
-                assert_exact(got, want[op][sl], f"{what} op {op}")
+                assert_exact(got[k], w[sl][k], f"{what} op {op}")
             else:
-                assert_distances(got, want[op][sl], f"{what} op {op}")
+                assert_distances(got[k], w[sl][k], f"{what} op {op}")

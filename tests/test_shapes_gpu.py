@@ -90,16 +90,13 @@ def run_all_ops(pv, pm, dm, pl, dl, step, on_device=True):
 
 
 def check_against(res, want, what, spec=None, local=None):
-    """local = (points, directions) of DistanceToOut, for the torus bar."""
     assert_exact(res["contains"], want["contains"], f"{what} Contains")
     assert_exact(res["inside"], want["inside"], f"{what} Inside")
     for k in ("safety_to_in", "safety_to_out"):
         assert_distances(res[k], want[k], f"{what} {k}")
     if spec is not None and spec.kind == "torus":
-        assert_torus_distances(res["distance_to_in"], want["distance_to_in"], spec.params,
-                               what=f"{what} distance_to_in")
-        assert_torus_distances(res["distance_to_out"], want["distance_to_out"], spec.params,
-                               *local, what=f"{what} distance_to_out")
+        for k in ("distance_to_in", "distance_to_out"):
+            assert_torus_distances(res[k], want[k + "_crlibm"], want[k], f"{what} {k}")
         return
     for k in ("distance_to_in", "distance_to_out"):
         assert_distances(res[k], want[k], f"{what} {k}")
@@ -157,6 +154,11 @@ def reference_outputs(spec, placement, pts, dirs, step):
         want["distance_to_in"] = ref.usphere_distance_to_in(spec.params, ref.last_transform, pts,
                                                             dirs)
     want["distance_to_out"] = call(oracle.DISTANCE_TO_OUT, pts, dirs, step)
+    if spec.kind == "torus" and oracle.RefLib.available(crlibm=True):
+        cr = oracle.RefLib(crlibm=True)
+        pvc = cr.placed(ref_unplaced(cr, spec), *PLACEMENTS[placement])
+        want["distance_to_in_crlibm"] = cr.batch(pvc, oracle.DISTANCE_TO_IN, pts, dirs, step)
+        want["distance_to_out_crlibm"] = cr.batch(pvc, oracle.DISTANCE_TO_OUT, pts, dirs, step)
     return want
 
 

@@ -10,7 +10,12 @@
 //    (Transform instead of TransformDirection, :906); the batch kernel applies
 //    that through kDirectionAsPoint;
 //  * the Newton polish runs only when the last root tested was valid (:851).
+// The complex cube root takes atan2, sin, cos and cbrt correctly rounded
+// (crmath.cuh), on the host and on the GPU alike: the reference calls the C
+// library's functions there, and the last bits of those move its roots, so
+// only correctly rounded values make the result independent of the library.
 #pragma once
+#include "crmath.cuh"
 #include "tube.cuh"
 
 namespace vgb {
@@ -53,20 +58,21 @@ template <class R> VGB_HD Cx<R> csqrt_real(R x) {
   const R l = sqrt(fabs(x));
   return {realcoef * l, imcoef * l};
 }
+// cbrt(Complex) (:283-316)
 template <class R> VGB_HD Cx<R> ccbrt(Cx<R> x) {
   R rr, s, c;
   if (x.i != (R)0.0) {
     rr = sqrt(x.r * x.r + x.i * x.i);
-    const R angle = atan2(x.i, x.r);
+    const R angle = cr_atan2(x.i, x.r);
     const R newangle = angle / (R)3.;
-    s = sin(newangle);
-    c = cos(newangle);
+    s = cr_sin(newangle);
+    c = cr_cos(newangle);
   } else {
     rr = x.r;
     s = 0.;
     c = 1.;
   }
-  const R rc = cbrt(rr);
+  const R rc = cr_cbrt(rr);
   return {rc * c, rc * s};
 }
 

@@ -14,6 +14,7 @@ only to draw inputs; results are always computed by libvgb.
 from __future__ import annotations
 
 import math
+import os
 from dataclasses import dataclass, field
 from typing import Callable
 
@@ -402,6 +403,29 @@ def make_workload(spec: ShapeSpec, n: int, seed: int, mix: str = "mixed",
         x, y, z = uniform_points(spec, n, seed)
     dx, dy, dz = isotropic(np.random.default_rng(seed + 7919), n)
     return ShapeWorkload(spec, x, y, z, dx, dy, dz, np.full(n, step_max))
+
+
+def _bench_workload_arrays(job):
+    config, shape, n, seed, mix = job
+    wl = make_workload(bench_config(config)[0][shape], n, seed, mix=mix)
+    return wl.x, wl.y, wl.z, wl.dx, wl.dy, wl.dz, wl.step
+
+
+def bench_workloads(jobs: list, processes: int | None = None) -> list:
+    """The workloads of (benchmark config, shape name, n, seed, mix) jobs,
+    drawn in spawned worker processes (numpy sampling of a 2^22-point mix takes
+    seconds per shape).  Spawned, never forked, so it is safe after CUDA has
+    started in the caller; the arrays equal those of sequential make_workload
+    calls."""
+    import multiprocessing as mp
+    from concurrent.futures import ProcessPoolExecutor
+    if len(jobs) <= 1:
+        arrays = [_bench_workload_arrays(j) for j in jobs]
+    else:
+        workers = min(len(jobs), processes or (os.cpu_count() or 1))
+        with ProcessPoolExecutor(max_workers=workers, mp_context=mp.get_context("spawn")) as ex:
+            arrays = list(ex.map(_bench_workload_arrays, jobs))
+    return [ShapeWorkload(bench_config(j[0])[0][j[1]], *a) for j, a in zip(jobs, arrays)]
 
 
 # ---------------------------------------------------------------------------
