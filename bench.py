@@ -59,6 +59,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--shapes", default="", help="comma list restricting the workload's shapes")
+    ap.add_argument("--only", action="store_true",
+                    help="only the named workload (the default run adds the other "
+                         "configurations and the other precision as extra keys)")
     return ap.parse_args()
 
 
@@ -76,7 +79,16 @@ def workload_shapes(name: str):
     return W.bench_config(name)
 
 
+L2_POLICY = "flushed (256 MB read sweep) before every op, outside the events"
+
+
 def workload_desc(name, n, precision):
+    d = _workload_desc(name, n, precision)
+    d["l2"] = L2_POLICY
+    return d
+
+
+def _workload_desc(name, n, precision):
     if name == "heavy":
         return {"workload": "torus/polycone/polyhedron/box-minus-tube, 2^22 mixed points each",
                 "shapes": ["torus(0,5,50)", "polycone(10 planes, phi 0-300deg)",
@@ -206,27 +218,28 @@ class ClockSampler:
 # CPU baseline: the reference Scalar backend (oracle/_ref) or the C oracle
 # ---------------------------------------------------------------------------
 
-def cpu_rate(shapes: dict, n_total: int, seed: int, budget_s: float = 12.0) -> dict:
+def cpu_rate(workloads: dict, budget_s: float = 12.0, sample: int = 1 << 18) -> dict:
     """Point-ops/s of the reference on this host's cores, all threads, on a
-    bounded sample (the first points of the same workload)."""
+    bounded sample: the first `sample` points of each shape's arrays of the very
+    workload the GPU arm times (same seeds, same mix).  Each op repeats for
+    about budget_s / (shapes x ops) seconds."""
     import oracle
     from oracle import oracle_unplaced, ref_unplaced
-    from vecgeom_b200 import workloads as W
     threads = os.cpu_count() or 1
     use_ref = oracle.RefLib.available()
     kind = "reference" if use_ref else "port"
-    sample = min(n_total, 1 << 18)
-    per = budget_s / (len(shapes) * len(OPS))
+    per = budget_s / (len(workloads) * len(OPS))
     tot_pts, tot_t = 0, 0.0
     if use_ref:
         ref = oracle.RefLib()
     else:
         orc = oracle.Oracle()
         threads = 1
-    for si, (name, spec) in enumerate(shapes.items()):
-        wl = W.make_workload(spec, sample, seed + si, mix="uniform" if name == "box" else "mixed")
-        pts = (wl.x, wl.y, wl.z)
-        dirs = (wl.dx, wl.dy, wl.dz)
+    for name, wl in workloads.items():
+        spec = wl.spec
+        m0 = min(sample, wl.n)
+        pts = tuple(np.ascontiguousarray(a[:m0]) for a in (wl.x, wl.y, wl.z))
+        dirs = tuple(np.ascontiguousarray(a[:m0]) for a in (wl.dx, wl.dy, wl.dz))
         if use_ref:
             pv = ref.placed(ref_unplaced(ref, spec))
             tr = ref.last_transform
@@ -258,31 +271,45 @@ def cpu_rate(shapes: dict, n_total: int, seed: int, budget_s: float = 12.0) -> d
                     break
             tot_pts += reps * m
             tot_t += el
+    m0 = min(sample, min(wl.n for wl in workloads.values()))
     return {"value": tot_pts / tot_t / 1e6, "unit": "Mpoints/s", "cores": threads, "kind": kind,
-            "sample": f"{sample} points per shape (first points of the same seeded workload), "
-                      f"each op repeated for ~{per:.2f} s, {threads} threads"}
+            "sample": f"the first {m0} points of each shape's arrays of the timed workload (same "
+                      f"seeds and mix), the same ops (DistanceToOut/SafetyToOut on the Contains() "
+                      f"subset); each op repeated for ~{per:.2f} s, {threads} threads"}
+
+
+def generate(workload: str, n: int = 0, rank: int = 0) -> dict:
+    """The seeded arrays of a shape workload, shape name -> ShapeWorkload,
+    drawn in spawned worker processes."""
+    from vecgeom_b200 import workloads as W
+    shapes, n0, mix = W.bench_config(workload)
+    n = n or n0
+    jobs = [(workload, name, n, W.bench_seed(si, rank), mix) for si, name in enumerate(shapes)]
+    return dict(zip(shapes, W.bench_workloads(jobs)))
 
 
 def run_reference_arm(args):
+    """The reference's own CPU implementation of the path (oracle/_ref, the
+    reference compiled from its sources) on this host's cores, on the GPU arm's
+    workload, metric and config.  A step is a bounded sample of the workload."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    from vecgeom_b200 import workloads as W
-    shapes, n, _ = workload_shapes(args.workload)
-    if args.n:
-        n = args.n
+    wls = generate(args.workload, args.n)
+    n = next(iter(wls.values())).n
+    step_budget = max(2.0, 60.0 / max(1, args.steps))
     for _ in range(args.warmup):
-        pass
+        cpu_rate(wls, budget_s=0.5, sample=1 << 14)
     times = []
     cb = None
     for _ in range(max(1, args.steps)):
-        cb = cpu_rate(shapes, n, W.SEED_BASE + 2, budget_s=max(2.0, 60.0 / max(1, args.steps)))
+        cb = cpu_rate(wls, budget_s=step_budget)
         times.append(cb["value"])
     v = float(np.median(times))
     line = {"impl": "reference", "metric": "Mpoints/s per shape op (fp64)", "value": v,
             "unit": "Mpoints/s", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
             "config": workload_desc(args.workload, n, "fp64"),
             "cpu_baseline": {"value": v, "unit": "Mpoints/s", "cores": cb["cores"],
                              "kind": cb["kind"], "sample": cb["sample"]},
@@ -406,7 +433,7 @@ def run_baskets(args):
             "e2e": {"value": round(2 * n / e2e_s / 1e6, 2), "unit": "Mpoints/s",
                     "h2d_bytes_per_step": 56 * n, "d2h_bytes_per_step": 16 * n},
             "gpu_launches": launches, "clocks": clocks}
-    print(json.dumps(line), flush=True)
+    return line
 
 
 # ---------------------------------------------------------------------------
@@ -571,48 +598,93 @@ def run_nav(args):
                     "h2d_bytes_per_step": int(48 * sizes.sum() / nreq),
                     "d2h_bytes_per_step": int(36 * sizes.sum() / nreq)},
             "gpu_launches": launches, "clocks": clocks}
-    print(json.dumps(line), flush=True)
+    return line
 
 
 # ---------------------------------------------------------------------------
-# the GPU arm
+# peaks and rooflines
 # ---------------------------------------------------------------------------
 
-def main():
-    args = parse()
-    if args.impl == "reference":
-        run_reference_arm(args)
-        return
-    if args.workload == "baskets":
-        run_baskets(args)
-        return
-    if args.workload == "nav":
-        run_nav(args)
-        return
+def load_peaks() -> dict:
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        return {}
+
+
+def load_op_costs() -> dict:
+    """Algorithmic flops per point of every (workload, shape, op), from
+    bench/op_costs.json (bench/make_op_costs.py)."""
+    try:
+        return json.load(open(os.path.join(ROOT, "bench", "op_costs.json")))["workloads"]
+    except (OSError, ValueError, KeyError):
+        return {}
+
+
+def measure_fma_peaks(stream) -> dict:
+    """FP64 and FP32 FMA throughput of this GPU (vgb_measure_fma_peak: one
+    launch of independent FMA chains on every SM, CUDA events; best of 5 after
+    2 warm-up launches), in GFLOP/s with an FMA counted as 2 flops."""
+    import ctypes
+    import vecgeom_b200 as V
+    L = V.lib()
+    out = {}
+    for name, fp32, iters in (("fp64", 0, 2048), ("fp32", 1, 4096)):
+        best = 0.0
+        for k in range(7):
+            fl, ms = ctypes.c_double(), ctypes.c_float()
+            V.check(L.vgb_measure_fma_peak(fp32, iters, ctypes.c_void_p(stream.cuda_stream),
+                                           ctypes.byref(fl), ctypes.byref(ms)))
+            if k >= 2:
+                best = max(best, fl.value / (ms.value * 1e-3) / 1e9)
+        out[f"{name}_gflops"] = round(best, 1)
+    out["method"] = ("vgb_measure_fma_peak: 8 independent FMA chains per thread, every SM "
+                     "filled, CUDA events; best of 5")
+    return out
+
+
+def op_roofline(opname: str, points: int, seconds: float, flops_per_point, hbm_gbs: float,
+                fp64_gflops) -> dict:
+    """Where one op sits: its algorithmic bytes (and flops, when counted) per
+    point over its event-timed duration, against measured HBM bandwidth and
+    FP64 FMA throughput; the bound is the resource its arithmetic intensity
+    (flops per byte) saturates first."""
+    gbs = BYTES[opname] * points / seconds / 1e9
+    r = {"gbs": round(gbs, 1), "frac_hbm": round(gbs / hbm_gbs, 4), "bound": "hbm"}
+    if flops_per_point is not None and fp64_gflops:
+        gfl = flops_per_point * points / seconds / 1e9
+        ai = flops_per_point / BYTES[opname]
+        r.update({"gflops": round(gfl, 1), "frac_fp64": round(gfl / fp64_gflops, 4),
+                  "flops_per_byte": round(ai, 3)})
+        if ai > fp64_gflops / hbm_gbs:
+            r["bound"] = "fp64"
+    return r
+
+
+# ---------------------------------------------------------------------------
+# shape workloads on the GPU
+# ---------------------------------------------------------------------------
+
+def run_shapes(args, workload: str, wls: dict, precision: str, peaks: dict, fma: dict,
+               with_e2e: bool = True, with_cpu: bool = True, world: int = 1, rank: int = 0,
+               dist=None) -> dict:
+    """One step = every (shape, op) of the workload once over its whole batch
+    (inputs resident in HBM, L2 flushed before every op, CUDA events around
+    each launch).  Returns the JSON line."""
     import torch
-    import torch.distributed as dist
 
     import vecgeom_b200 as V
     from vecgeom_b200 import workloads as W
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    if world > 1:
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
     L = V.lib()
-    prec = V.PREC_FP64 if args.precision == "fp64" else V.PREC_FP32_REFINE
-
-    shapes, n, mix = workload_shapes(args.workload)
+    prec = V.PREC_FP64 if precision == "fp64" else V.PREC_FP32_REFINE
+    shapes = {k: w.spec for k, w in wls.items()}
     if args.shapes:
         keep = set(args.shapes.split(","))
         shapes = {k: v for k, v in shapes.items() if k in keep}
-    if args.n:
-        n = args.n
+    n = next(iter(wls.values())).n
     stream = torch.cuda.current_stream()
+    local = torch.cuda.current_device()
 
     # --- geometry + inputs resident in HBM --------------------------------
     g = V.Geometry()
@@ -631,7 +703,7 @@ def main():
     checks = []  # (shape, opname, output, FP64 output, FP64 call) for the error report
     h2d_bytes = d2h_bytes = 0
     for si, (name, spec) in enumerate(shapes.items()):
-        wl = W.make_workload(spec, n, W.bench_seed(si, rank), mix=mix)
+        wl = wls[name]
         pv = placed[name]
         P = V.SOA3D(dev(wl.x), dev(wl.y), dev(wl.z))
         D = V.SOA3D(dev(wl.dx), dev(wl.dy), dev(wl.dz))
@@ -646,20 +718,19 @@ def main():
         ns = int(sel.sum().item())
         # pinned host copies for the end-to-end leg
         pin = lambda t: t.cpu().pin_memory()  # noqa: E731
-        HP = V.SOA3D(pin(P.x), pin(P.y), pin(P.z))
-        HD = V.SOA3D(pin(D.x), pin(D.y), pin(D.z))
-        HS = pin(S)
-        HPS = V.SOA3D(pin(PS.x), pin(PS.y), pin(PS.z))
-        HDS = V.SOA3D(pin(DS.x), pin(DS.y), pin(DS.z))
-        HSS = pin(SS)
+        if with_e2e:
+            HP = V.SOA3D(pin(P.x), pin(P.y), pin(P.z))
+            HD = V.SOA3D(pin(D.x), pin(D.y), pin(D.z))
+            HS = pin(S)
+            HPS = V.SOA3D(pin(PS.x), pin(PS.y), pin(PS.z))
+            HDS = V.SOA3D(pin(DS.x), pin(DS.y), pin(DS.z))
+            HSS = pin(SS)
         for opname in OPS:
             local_op = opname in LOCAL_OPS
             m = ns if local_op else n
             dt = {"contains": torch.uint8, "inside": torch.int32}.get(opname, torch.float64)
             out_d = torch.empty(m, dtype=dt, device="cuda")
-            out_h = torch.empty(m, dtype=dt).pin_memory()
             pts_d, dirs_d, st_d = (PS, DS, SS) if local_op else (P, D, S)
-            pts_h, dirs_h, st_h = (HPS, HDS, HSS) if local_op else (HP, HD, HS)
             meth = {"contains": "Contains", "inside": "Inside", "safety_to_in": "SafetyToIn",
                     "safety_to_out": "SafetyToOut", "distance_to_in": "DistanceToIn",
                     "distance_to_out": "DistanceToOut"}[opname]
@@ -668,35 +739,42 @@ def main():
             if opname.startswith("distance"):
                 run64 = (lambda fn=fn, a=pts_d, b=dirs_d, s=st_d, o=out64:
                          fn(a, b, s, o, precision=V.PREC_FP64))
-            else:
-                run64 = lambda fn=fn, a=pts_d, o=out64: fn(a, o, precision=V.PREC_FP64)  # noqa
-            checks.append((name, opname, out_d, out64, run64))
-            if opname.startswith("distance"):
                 run_d = (lambda fn=fn, a=pts_d, b=dirs_d, s=st_d, o=out_d:
                          fn(a, b, s, o, precision=prec))
-                run_h = (lambda fn=fn, a=pts_h, b=dirs_h, s=st_h, o=out_h:
-                         fn(a, b, s, o, precision=prec))
-                h2d_bytes += m * 56
             else:
+                run64 = lambda fn=fn, a=pts_d, o=out64: fn(a, o, precision=V.PREC_FP64)  # noqa
                 run_d = lambda fn=fn, a=pts_d, o=out_d: fn(a, o, precision=prec)  # noqa: E731
-                run_h = lambda fn=fn, a=pts_h, o=out_h: fn(a, o, precision=prec)  # noqa: E731
-                h2d_bytes += m * 24
-            d2h_bytes += m * out_d.element_size()
+            checks.append((name, opname, out_d, out64, run64))
+            run_h = None
+            if with_e2e:
+                out_h = torch.empty(m, dtype=dt).pin_memory()
+                pts_h, dirs_h, st_h = (HPS, HDS, HSS) if local_op else (HP, HD, HS)
+                if opname.startswith("distance"):
+                    run_h = (lambda fn=fn, a=pts_h, b=dirs_h, s=st_h, o=out_h:
+                             fn(a, b, s, o, precision=prec))
+                    h2d_bytes += m * 56
+                else:
+                    run_h = lambda fn=fn, a=pts_h, o=out_h: fn(a, o, precision=prec)  # noqa
+                    h2d_bytes += m * 24
+                d2h_bytes += m * out_d.element_size()
             tasks.append((name, opname, m, run_d, run_h))
-        # the fused end-to-end form: all points (Inside, Contains, SafetyToIn,
-        # DistanceToIn) and the Contains() subset (SafetyToOut, DistanceToOut)
-        code = {"contains": 0, "inside": 1, "distance_to_in": 2, "distance_to_out": 3,
-                "safety_to_in": 4, "safety_to_out": 5}
-        for on_subset, (hp, hd, hs, m) in ((False, (HP, HD, HS, n)),
-                                           (True, (HPS, HDS, HSS, ns))):
-            sel_ops = [o for o in OPS if (o in LOCAL_OPS) == on_subset]
-            outs = {code[o]: torch.empty(m, dtype={"contains": torch.uint8, "inside": torch.int32}
-                                         .get(o, torch.float64)).pin_memory() for o in sel_ops}
-            mask = sum(1 << code[o] for o in sel_ops)
-            fused_calls.append(lambda pv=pv, mask=mask, hp=hp, hd=hd, hs=hs, outs=outs:
-                               pv.fused(mask, hp, outs, hd, hs))
-            fused_h2d += m * 56
-            fused_d2h += sum(v.element_size() * m for v in outs.values())
+        if with_e2e:
+            # the fused end-to-end form: all points (Inside, Contains, SafetyToIn,
+            # DistanceToIn) and the Contains() subset (SafetyToOut, DistanceToOut)
+            code = {"contains": 0, "inside": 1, "distance_to_in": 2, "distance_to_out": 3,
+                    "safety_to_in": 4, "safety_to_out": 5}
+            for on_subset, (hp, hd, hs, m) in ((False, (HP, HD, HS, n)),
+                                               (True, (HPS, HDS, HSS, ns))):
+                sel_ops = [o for o in OPS if (o in LOCAL_OPS) == on_subset]
+                outs = {code[o]: torch.empty(m, dtype={"contains": torch.uint8,
+                                                       "inside": torch.int32}
+                                             .get(o, torch.float64)).pin_memory()
+                        for o in sel_ops}
+                mask = sum(1 << code[o] for o in sel_ops)
+                fused_calls.append(lambda pv=pv, mask=mask, hp=hp, hd=hd, hs=hs, outs=outs:
+                                   pv.fused(mask, hp, outs, hd, hs, precision=prec))
+                fused_h2d += m * 56
+                fused_d2h += sum(v.element_size() * m for v in outs.values())
 
     # L2 flush: a read sweep over 256 MB (> 126 MB L2); reading leaves clean lines,
     # so the next kernel pays no write-back for the flush itself
@@ -714,7 +792,8 @@ def main():
             if timed:
                 ev[k][1].record(stream)
 
-    for _ in range(max(3, args.warmup)):
+    warm = max(3, args.warmup)
+    for _ in range(warm):
         one_step(False)
     torch.cuda.synchronize()
 
@@ -743,29 +822,41 @@ def main():
     pts_per_step = sum(t[2] for t in tasks)
     value = world * pts_per_step / (step_ms * 1e-3) / 1e6
 
-    # roofline of the dominant kernel (largest share of the step)
+    # rooflines: every op, and the dominant one (largest share of the step)
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    fp64_peak = fma.get("fp64_gflops")
+    costs = load_op_costs().get(workload, {})
+    per_op, per_op_roof = {}, {}
+    for i, (name, opname, m, _, _) in enumerate(tasks):
+        sec = per_task_ms[i] / args.steps * 1e-3
+        per_op[f"{name}:{opname}"] = round(m / sec / 1e6, 1)
+        c = costs.get(name, {})
+        fl = c.get(opname, {}).get("flops_per_point") if isinstance(c, dict) else None
+        per_op_roof[f"{name}:{opname}"] = op_roofline(opname, m, sec, fl, hbm_peak, fp64_peak)
     k = int(np.argmax(per_task_ms))
     name, opname, m, _, _ = tasks[k]
-    avg_s = per_task_ms[k] / args.steps * 1e-3
-    peaks = {}
-    try:
-        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
-    except (OSError, ValueError):
-        pass
-    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
-    achieved = BYTES[opname] * m / avg_s / 1e9
+    dom = per_op_roof[f"{name}:{opname}"]
     traffic = None
-    tp = NCU_TRAFFIC_PER_POINT.get((name, opname, args.precision))
+    tp = NCU_TRAFFIC_PER_POINT.get((name, opname, precision))
     if tp is not None:
         traffic = int(round(tp * m))
-    roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
-            "frac": round(achieved / hbm_peak, 4), "traffic": traffic,
-            "kernel": f"{name} {opname}", "bytes_per_point": BYTES[opname],
-            "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"}
+    if dom["bound"] == "fp64":
+        roof = {"bound": "fp64", "achieved": dom["gflops"], "peak": fp64_peak, "unit": "GFLOP/s",
+                "frac": dom["frac_fp64"]}
+    else:
+        roof = {"bound": "hbm", "achieved": dom["gbs"], "peak": hbm_peak, "unit": "GB/s",
+                "frac": dom["frac_hbm"]}
+    roof.update({"traffic": traffic, "kernel": f"{name} {opname}",
+                 "bytes_per_point": BYTES[opname],
+                 "flops_per_point": (costs.get(name, {}) or {}).get(opname, {}).get(
+                     "flops_per_point") if isinstance(costs.get(name), dict) else None,
+                 "frac_hbm": dom["frac_hbm"], "frac_fp64": dom.get("frac_fp64"),
+                 "peak_source": ("hbm: measured (MEASURED_PEAKS.json)" if "hbm_gbs" in peaks
+                                 else "hbm: fallback") + "; fp64: measured (vgb_measure_fma_peak)"})
 
     # end-to-end through the public API with pinned host buffers
     e2e = e2e_per_op = None
-    if not args.no_e2e:
+    if with_e2e:
         def timed_wall(calls):
             for _ in range(2):
                 for c in calls:
@@ -792,11 +883,9 @@ def main():
                       "d2h_bytes_per_step": int(d2h_bytes),
                       "api": "vgb_batch, host buffers, 1 call per op"}
 
-    per_op = {f"{t[0]}:{t[1]}": round(t[2] / (per_task_ms[i] / args.steps * 1e-3) / 1e6, 1)
-              for i, t in enumerate(tasks)}
     # FP32+refine: error of every op against the FP64 form on the same points
     err = None
-    if args.precision != "fp64":
+    if precision != "fp64":
         err = {}
         for t, (name, opname, o, o64, run64) in zip(tasks, checks):
             t[3]()
@@ -811,20 +900,80 @@ def main():
                 "p99_mm": float(torch.quantile(dif[:1 << 24].float(), .99).item())
                 if dif.numel() else 0.,
                 "class_mismatches": int(bad.sum().item())}
-    line = {"metric": "Mpoints/s per shape op" + (" (fp64)" if args.precision == "fp64"
+    line = {"metric": "Mpoints/s per shape op" + (" (fp64)" if precision == "fp64"
                                                   else " (fp32+refine)"),
             "value": round(value, 2), "unit": "Mpoints/s", "n_gpus": world,
-            "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": round(step_ms, 4),
+            "steps": args.steps, "warmup": warm, "ms_per_step": round(step_ms, 4),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64" if args.precision == "fp64" else "f32+f64",
+            "dtype": "f64" if precision == "fp64" else "f32+f64",
             "data": "synthetic (seeded)",
-            "config": dict(workload_desc(args.workload, n, args.precision),
-                           l2="flushed (256 MB read sweep) before every op, outside the events"),
-            "per_op_mpoints_s": per_op, "roofline": roof, "e2e": e2e, "e2e_per_op": e2e_per_op,
-            "error_vs_fp64": err,
+            "config": workload_desc(workload, n, precision),
+            "per_op_mpoints_s": per_op, "roofline": roof, "roofline_per_op": per_op_roof,
+            "e2e": e2e, "e2e_per_op": e2e_per_op, "error_vs_fp64": err,
             "gpu_launches": launches, "clocks": clk}
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_rate(shapes, n, W.SEED_BASE + 2)
+    if with_cpu and rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_rate({k: wls[k] for k in shapes})
+    return line
+
+
+def summary(line: dict) -> dict:
+    """The keys of a sub-benchmark line kept under the default line's configs."""
+    keep = ("metric", "value", "unit", "ms_per_step", "config", "per_op_mpoints_s", "roofline",
+            "roofline_per_op", "e2e", "error_vs_fp64", "gpu_launches", "clocks", "cpu_baseline")
+    return {k: line[k] for k in keep if k in line}
+
+
+# ---------------------------------------------------------------------------
+# the GPU arm
+# ---------------------------------------------------------------------------
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference_arm(args)
+        return
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    extra = (args.workload == "shapes" and world == 1 and not args.only)
+    # seeded inputs are drawn before CUDA starts, in spawned worker processes
+    wls = {}
+    if args.workload in ("shapes", "heavy", "box"):
+        wls[args.workload] = generate(args.workload, args.n, rank)
+    if extra:
+        wls["box"] = generate("box")
+        wls["heavy"] = generate("heavy")
+    import torch
+    import torch.distributed as dist
+
+    torch.cuda.set_device(local)
+    if args.workload == "baskets":
+        print(json.dumps(run_baskets(args)), flush=True)
+        return
+    if args.workload == "nav":
+        print(json.dumps(run_nav(args)), flush=True)
+        return
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    peaks = load_peaks()
+    fma = measure_fma_peaks(torch.cuda.current_stream())
+    line = run_shapes(args, args.workload, wls[args.workload], args.precision, peaks, fma,
+                      world=world, rank=rank, dist=dist if world > 1 else None)
+    line["fma_peaks"] = fma
+    if extra:
+        other = "fp32r" if args.precision == "fp64" else "fp64"
+        line["other_precision"] = summary(run_shapes(args, "shapes", wls["shapes"], other, peaks,
+                                                     fma, with_e2e=True, with_cpu=False))
+        line["configs"] = {
+            "box": summary(run_shapes(args, "box", wls["box"], "fp64", peaks, fma,
+                                      with_e2e=False)),
+            "heavy": summary(run_shapes(args, "heavy", wls["heavy"], "fp64", peaks, fma,
+                                        with_e2e=False)),
+            "baskets": run_baskets(args),
+            "nav": run_nav(args),
+        }
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

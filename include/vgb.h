@@ -105,6 +105,11 @@ void vgb_launch_count_reset(void);
  * reported against. */
 vgb_status vgb_measure_fma_peak(int32_t fp32, int32_t iters, void *stream, double *flops,
                                 float *ms);
+/* Measurement support, no counterpart in the reference: how many points the
+ * FP32+refine kernels settled with their float selection (certified) and how
+ * many they sent to the FP64 path, summed since the last reset (reset != 0
+ * zeroes the counts after reading; synchronises the device). */
+vgb_status vgb_refine_counts(int64_t *certified, int64_t *fallback, int32_t reset);
 
 /* ---------------------------------------------------------------------------
  * Geometry construction and upload.

@@ -58,6 +58,7 @@ SIGNATURES = {
     "vgb_launch_count_reset": (None, []),
     "vgb_measure_fma_peak": (ctypes.c_int, [_i32, _i32, _vp, ctypes.POINTER(_dbl),
                                             ctypes.POINTER(ctypes.c_float)]),
+    "vgb_refine_counts": (ctypes.c_int, [_pi64, _pi64, _i32]),
     "vgb_geometry_create": (ctypes.c_int, [ctypes.POINTER(_vp)]),
     "vgb_geometry_destroy": (ctypes.c_int, [_vp]),
     "vgb_unplaced_box": (ctypes.c_int, [_vp, _dbl, _dbl, _dbl, _pi32]),

@@ -6,6 +6,7 @@
 #include "batch.cuh"
 #include "dispatch.h"
 #include "geometry.h"
+#include "refine.cuh"
 
 namespace vgb {
 
@@ -19,7 +20,19 @@ static int grid_for(int64_t n) {
 template <class Ops, class P>
 static vgb_status launch_ops(const P &prm, const DXform &X, int op, BatchIO io, cudaStream_t s,
                              int32_t rec_len = 0, int precision = VGB_PREC_FP64) {
-  (void)precision;  // both forms run the FP64 kernels for single-volume batches
+  // FP32+refine: DistanceToIn of the shapes with a float selector (refine.cuh);
+  // every other (shape, op) computes in FP64 in both forms
+  if constexpr (!std::is_void<typename RefineDti<Ops>::type>::value) {
+    if (precision == VGB_PREC_FP32_REFINE && op == VGB_OP_DISTANCE_TO_IN) {
+      const int64_t tiles = (io.n + kRefineTile - 1) / kRefineTile;
+      const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(tiles, 148 * 8));
+      k_refine_dti<typename RefineDti<Ops>::type, Ops, P><<<grid, kRefineBlock, 0, s>>>(prm, X, io);
+      count_launch();
+      cudaError_t e = cudaGetLastError();
+      if (e != cudaSuccess) return cuda_error(e, "vgb_batch: kernel launch");
+      return VGB_OK;
+    }
+  }
   const int grid = grid_for(io.n);
   io.stage = (Stageable<P>::value && rec_len > 0 && rec_len <= kStageMaxDoubles) ? rec_len : 0;
   const size_t smem = (size_t)io.stage * sizeof(double);
@@ -121,3 +134,17 @@ vgb_status launch_fused_f64(const vgb_geometry *g, int32_t placed, const FusedIO
 }
 
 }  // namespace vgb
+
+extern "C" vgb_status vgb_refine_counts(int64_t *certified, int64_t *fallback, int32_t reset) {
+  vgb::RefineCounts c = {0, 0};
+  cudaError_t e = cudaMemcpyFromSymbol(&c, vgb::g_refine_counts, sizeof(c));
+  if (e != cudaSuccess) return vgb::cuda_error(e, "vgb_refine_counts");
+  if (certified) *certified = (int64_t)c.certified;
+  if (fallback) *fallback = (int64_t)c.fallback;
+  if (reset) {
+    const vgb::RefineCounts z = {0, 0};
+    e = cudaMemcpyToSymbol(vgb::g_refine_counts, &z, sizeof(z));
+    if (e != cudaSuccess) return vgb::cuda_error(e, "vgb_refine_counts");
+  }
+  return VGB_OK;
+}
