@@ -245,3 +245,26 @@ extern "C" int hc_crmath(int32_t fn, int64_t n, const double *a, const double *b
   }
   return 0;
 }
+
+// The FP32+refine DistanceToIn of a sphere placed volume on the host: the float
+// selection and the FP64 value of the winning root where it certifies, the FP64
+// DistanceToIn elsewhere (the GPU kernel runs the same functions).  winners[i]
+// is the selection's result (0: uncertain).
+#include "../../vecgeom_b200/csrc/refine.cuh"
+extern "C" int hc_refine_dti(const vgb_geometry *g, int32_t placed, int64_t n, const double *x,
+                             const double *y, const double *z, const double *dx,
+                             const double *dy, const double *dz, const double *st, double *out,
+                             int32_t *winners) {
+  const PlacedRec &pr = g->placed[placed];
+  const DXform &X = g->xforms[pr.xform];
+  if (g->unplaced[pr.unplaced].type != VGB_SHAPE_SPHERE) return -2;
+  const SphereP &s = *static_cast<const SphereP *>(shape_params(g, pr.unplaced));
+  for (int64_t i = 0; i < n; ++i) {
+    const V3<double> p = xf_point(X, V3<double>{x[i], y[i], z[i]});
+    const V3<double> v = dti_dir<SphereOps<double>>(X, V3<double>{dx[i], dy[i], dz[i]});
+    const int w = SphereRefine::select(s, p, v);
+    winners[i] = w;
+    out[i] = w ? SphereRefine::eval(s, p, v, w) : SphereOps<double>::distance_to_in(s, p, v, st[i]);
+  }
+  return 0;
+}

@@ -115,3 +115,48 @@ def test_bench_batch_matches_reference_at_full_size(config, shape):
     else:
         for k in ("distance_to_in", "distance_to_out"):
             assert_distances(got[k], want[k], f"{what} {k}")
+
+
+def test_fp32_refine_at_full_size_equals_fp64():
+    """The FP32+refine form on the benchmark's tube/cone/sphere batches (2^22
+    mixed points each): every op bit-identical to the FP64 form, and the
+    sphere's float selection really settles most of its DistanceToIn points
+    (vgb_refine_counts)."""
+    import ctypes
+    import torch
+    import vecgeom_b200 as V
+    from vecgeom_b200 import workloads as W
+    shapes, n, mix = W.bench_config("shapes")
+    L = V.lib()
+    for si, (name, spec) in enumerate(shapes.items()):
+        wl = W.make_workload(spec, n, W.bench_seed(si), mix=mix)
+        g = V.Geometry()
+        pv = g.LogicalVolume(name, W.build_unplaced(g, spec)).Place(g.Transformation3D())
+        g.CloseGeometry()
+        dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()  # noqa: E731
+        P = V.SOA3D(dev(wl.x), dev(wl.y), dev(wl.z))
+        D = V.SOA3D(dev(wl.dx), dev(wl.dy), dev(wl.dz))
+        S = dev(wl.step)
+        c = torch.empty(n, dtype=torch.uint8, device="cuda")
+        pv.Contains(P, c)
+        sel = c.bool()
+        PS = V.SOA3D(P.x[sel].contiguous(), P.y[sel].contiguous(), P.z[sel].contiguous())
+        DS = V.SOA3D(D.x[sel].contiguous(), D.y[sel].contiguous(), D.z[sel].contiguous())
+        SS = S[sel].contiguous()
+        V.check(L.vgb_refine_counts(None, None, 1))
+        for meth, args, pts in (("Contains", (), P), ("Inside", (), P), ("SafetyToIn", (), P),
+                                ("DistanceToIn", (D, S), P), ("SafetyToOut", (), PS),
+                                ("DistanceToOut", (DS, SS), PS)):
+            m = pts.size()
+            dt = {"Contains": torch.uint8, "Inside": torch.int32}.get(meth, torch.float64)
+            a = torch.full((m,), 7, dtype=dt, device="cuda")
+            b = torch.full((m,), 9, dtype=dt, device="cuda")
+            getattr(pv, meth)(pts, *args, a, precision=V.PREC_FP64)
+            getattr(pv, meth)(pts, *args, b, precision=V.PREC_FP32_REFINE)
+            torch.cuda.synchronize()
+            same = (a == b) | (torch.isnan(a) & torch.isnan(b)) if dt == torch.float64 else a == b
+            assert bool(same.all()), f"{name} {meth}: {int((~same).sum())} differ"
+        cert, fb = ctypes.c_int64(), ctypes.c_int64()
+        V.check(L.vgb_refine_counts(ctypes.byref(cert), ctypes.byref(fb), 1))
+        if name == "sphere":
+            assert cert.value + fb.value == n and cert.value > 0.6 * n, (cert.value, fb.value)

@@ -113,3 +113,32 @@ def test_host_build_matches_reference_on_mixed_baskets(hc):
                 assert_exact(got[k], w[sl][k], f"{what} op {op}")
             else:
                 assert_distances(got[k], w[sl][k], f"{what} op {op}")
+
+
+def test_host_fp32_refine_sphere_distance_to_in_equals_fp64(hc):
+    """The FP32+refine DistanceToIn of the sphere (refine.cuh: float selection
+    with certified decisions, FP64 value of the winning root, FP64 kernel for
+    uncertain points) equals the FP64 form bit for bit; on the benchmark's
+    tube/cone/sphere mix the float selection settles most points."""
+    from helpers import shape_specs
+    vp = ctypes.c_void_p
+    hc.hc_refine_dti.restype = ctypes.c_int
+    hc.hc_refine_dti.argtypes = [vp, ctypes.c_int32, ctypes.c_int64] + [vp] * 9
+    cases = [("bench", W.config2_shapes()["sphere"], "identity", 1 << 18)]
+    cases += [(k, s, pl, 1 << 15) for k, s in shape_specs().items() if s.kind == "sphere"
+              for pl in ("identity", "generic")]
+    for name, spec, pl, n in cases:
+        g = Geometry(library=hc)
+        pv = g.LogicalVolume("s", W.build_unplaced(g, spec)).Place(
+            g.Transformation3D(*PLACEMENTS[pl]))
+        wl = W.make_workload(spec, n, W.SEED_BASE + 2)
+        a = [np.ascontiguousarray(v) for v in (wl.x, wl.y, wl.z, wl.dx, wl.dy, wl.dz, wl.step)]
+        want = host_run(hc, g, pv, 2, a[:3], a[3:6], a[6])
+        got = np.zeros(n)
+        win = np.zeros(n, np.int32)
+        assert hc.hc_refine_dti(g.handle, pv.id, n, *(v.ctypes.data for v in a), got.ctypes.data,
+                                win.ctypes.data) == 0
+        same = (got == want) | (np.isnan(got) & np.isnan(want))
+        assert same.all(), f"{name} {pl}: {np.flatnonzero(~same)[:5]}"
+        if name == "bench":
+            assert (win > 0).mean() > 0.6, (win > 0).mean()

@@ -32,16 +32,16 @@ constexpr float kSafe = 8.f;
 // is e marks the point uncertain unless |a - b| > e (NaN operands included).
 struct Cert {
   bool ok = true;
-  VGB_D bool gt(float a, float b, float e) {
+  VGB_HD bool gt(float a, float b, float e) {
     ok &= fabsf(a - b) > e;
     return a > b;
   }
-  VGB_D bool ge(float a, float b, float e) {
+  VGB_HD bool ge(float a, float b, float e) {
     ok &= fabsf(a - b) > e;
     return a >= b;
   }
-  VGB_D bool lt(float a, float b, float e) { return gt(b, a, e); }
-  VGB_D bool le(float a, float b, float e) { return ge(b, a, e); }
+  VGB_HD bool lt(float a, float b, float e) { return gt(b, a, e); }
+  VGB_HD bool le(float a, float b, float e) { return ge(b, a, e); }
 };
 
 // A float value with a bound on its absolute error.
@@ -70,7 +70,7 @@ struct SphereRefine {
   // theta of (rho, z) against cut k: -1 below, +1 above; certified margin on
   // f = z sin c - rho cos c = r sin(c - theta), whose float error is bounded
   // from the errors of rho and z.
-  static VGB_D int cut_side_f(const ThetaCut &k, FE rho, FE z, Cert &ct) {
+  static VGB_HD int cut_side_f(const ThetaCut &k, FE rho, FE z, Cert &ct) {
     if (k.mode == 1) return 1;
     if (k.mode == 2) return -1;
     const float sn = (float)k.sn, cs = (float)k.cs;
@@ -80,7 +80,7 @@ struct SphereRefine {
     ct.ok &= fabsf(f) > e;
     return f > 0.f ? -1 : 1;
   }
-  static VGB_D bool theta_in(const SphereP &s, FE rho, FE z, Cert &ct) {
+  static VGB_HD bool theta_in(const SphereP &s, FE rho, FE z, Cert &ct) {
     // th >= tolS && th <= tolE
     return cut_side_f(s.cut[kCutTolS], rho, z, ct) > 0 && cut_side_f(s.cut[kCutTolE], rho, z, ct) < 0;
   }
@@ -93,7 +93,7 @@ struct SphereRefine {
     bool real;
     double minus, plus;
   };
-  static VGB_D Cone64 cone64(double tan2, double dist2, double pDotV2d, const V3<double> &p,
+  static VGB_HD Cone64 cone64(double tan2, double dist2, double pDotV2d, const V3<double> &p,
                              const V3<double> &v) {
     Cone64 o = {false, 0., 0.};
     const double t1 = 1. - v.z * v.z * (1. + tan2);
@@ -113,7 +113,7 @@ struct SphereRefine {
   }
 
   // The winner of DistanceToIn for this point, or kSdUncertain.
-  static VGB_D int select(const SphereP &s, const V3<double> &p64, const V3<double> &v64) {
+  static VGB_HD int select(const SphereP &s, const V3<double> &p64, const V3<double> &v64) {
     if (!s.fullPhi) return kSdUncertain;
     Cert ct;
     const float px = (float)p64.x, py = (float)p64.y, pz = (float)p64.z;
@@ -182,7 +182,7 @@ struct SphereRefine {
     if (!ct.ok) return kSdUncertain;
 
     int win = kSdInf;
-    FE snxt = {__int_as_float(0x7f800000), 0.f};
+    FE snxt = {HUGE_VALF, 0.f};
     // inner sphere (:790-930)
     if (s.rmin != 0) {
       const float ci = rad2 - fRmin * fRmin;
@@ -303,7 +303,7 @@ struct SphereRefine {
   }
 
   // The FP64 value of a winner, in dti_core's operation order.
-  static VGB_D double eval(const SphereP &s, const V3<double> &p, const V3<double> &v, int win) {
+  static VGB_HD double eval(const SphereP &s, const V3<double> &p, const V3<double> &v, int win) {
     using R = double;
     const R rho2 = p.x * p.x + p.y * p.y;
     const R rad2 = rho2 + p.z * p.z;
