@@ -54,6 +54,25 @@ def reference_cxxflags() -> list:
     return _make_print("print-ref-cxxflags").split()
 
 
+def reference_defined(spec, z_local) -> np.ndarray:
+    """Points on which the reference's result is defined.  Its polyhedron
+    Contains/Inside index the z-segment array with the number of z-planes below
+    the point (volumes/kernel/PolyhedronImplementation.h:350-370, :763, :809),
+    but its bounding tube reaches kTolerance beyond the end planes
+    (source/UnplacedPolyhedron.cpp:120-130): a point within that band above the
+    last plane reads one segment past the array, one at or just below the first
+    plane (Inside) reads segment -1.  That is undefined behaviour (it crashed the
+    reference on 2^22 near-surface points); libvgb clamps to the end segment.
+    Comparisons with the reference, and timings of it, leave such points out."""
+    z = np.asarray(z_local, np.float64)
+    ok = np.ones(len(z), bool)
+    if spec.kind == "polyhedron":
+        zp = np.asarray(spec.params["z"], np.float64)
+        band = 4e-9
+        ok &= ~((np.abs(z - zp[0]) <= band) | (np.abs(z - zp[-1]) <= band))
+    return ok
+
+
 def _p(a):
     return None if a is None else a.ctypes.data_as(_vp)
 

@@ -72,25 +72,6 @@ def assert_torus_distances(got, want_crlibm, want_glibc=None, what: str = "") ->
     return stats
 
 
-def reference_defined(spec, z_local) -> np.ndarray:
-    """Points on which the reference's result is defined.  Its polyhedron
-    Contains/Inside index the z-segment array with the number of z-planes below
-    the point (volumes/kernel/PolyhedronImplementation.h:350-370, :763, :809),
-    but its bounding tube reaches kTolerance beyond the end planes
-    (source/UnplacedPolyhedron.cpp:120-130): a point within that band above the
-    last plane reads one segment past the array, one at or just below the first
-    plane (Inside) reads segment -1.  That is undefined behaviour (it crashed the
-    reference on 2^22 near-surface points); libvgb clamps to the end segment.
-    Such points are left out of comparisons with the reference."""
-    z = np.asarray(z_local, np.float64)
-    ok = np.ones(len(z), bool)
-    if spec.kind == "polyhedron":
-        zp = np.asarray(spec.params["z"], np.float64)
-        band = 4e-9
-        ok &= ~((np.abs(z - zp[0]) <= band) | (np.abs(z - zp[-1]) <= band))
-    return ok
-
-
 def assert_exact(a, b, what: str = "") -> None:
     a = np.asarray(a)
     b = np.asarray(b)
@@ -104,7 +85,8 @@ def assert_exact(a, b, what: str = "") -> None:
 # ---------------------------------------------------------------------------
 # building one ShapeSpec in each implementation
 # ---------------------------------------------------------------------------
-from oracle import oracle_generic_xform, oracle_unplaced, ref_unplaced  # noqa: E402,F401
+from oracle import (oracle_generic_xform, oracle_unplaced, ref_unplaced,  # noqa: E402,F401
+                    reference_defined)
 from vecgeom_b200.workloads import build_unplaced as vgb_unplaced  # noqa: E402,F401
 
 

@@ -19,13 +19,20 @@ namespace vgb {
 
 // One quadrilateral: its plane (unit normal, distance to the origin), the four
 // side planes bounding it and its four corners (volumes/Quadrilaterals.h:28-35).
+// 33 doubles: the padding double makes consecutive quadrilaterals start 66
+// 4-byte words apart, i.e. two shared-memory banks apart, so the lanes of a warp
+// reading the quadrilaterals of different phi sides (the safety and distance
+// walks do) hit different banks instead of all one (a 256-byte stride is a
+// multiple of the 128-byte bank cycle).
 struct PhQuad {
   double n[3];
   double d;
   double sn[4][3];
   double sd[4];
   double c[4][3];
+  double pad;
 };
+static_assert(sizeof(PhQuad) == 33 * sizeof(double), "PhQuad stride");
 
 // A z-segment: index ranges into the quadrilateral table.
 struct PhSeg {
