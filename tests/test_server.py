@@ -152,3 +152,27 @@ def test_server_capacity_and_errors():
     assert rid in done or srv.result(rid)["nsteps"].size == 0
     with pytest.raises(V.VgbError):
         srv.result(12345)
+
+
+@pytest.mark.gpu
+def test_small_request_passes_a_large_one_that_does_not_fit():
+    """Admission is not strictly first come first served: with 10 chunks of
+    slots, a 2048-track request (8 chunks) running and a second one queued that
+    does not fit, a 64-track request that arrives after it is admitted into the
+    two free chunks and finishes first."""
+    import vecgeom_b200 as V
+    g = V.Geometry()
+    W.build_detector(W.VgbBuilder(g))
+    srv = V.NavServer(g, max_tracks=2560, steps_per_launch=2, max_steps=MAX_STEPS)
+    a = srv.submit(*W.isotropic_tracks(2048, W.SEED_BASE + 95))
+    srv.step()
+    b = srv.submit(*W.isotropic_tracks(2048, W.SEED_BASE + 96))
+    c = srv.submit(*W.isotropic_tracks(64, W.SEED_BASE + 97))
+    order = []
+    for _ in range(10000):
+        done, live, queued = srv.step()
+        order += list(done)
+        if len(order) == 3:
+            break
+    assert set(order) == {a, b, c}
+    assert order.index(c) < order.index(b), order

@@ -3,10 +3,13 @@
 // Device memory holds a fixed table of track slots, carved into chunks of
 // kChunk tracks.  A request owns whole chunks; the last one is padded with
 // finished tracks.  Every iteration (vgb_server_step):
-//   1. admit: queued requests, in arrival order, take free chunks; the points
-//      of all of them go to the device in one copy from a pinned staging
-//      buffer, and one launch scatters them into their slots, locates them
-//      (LocatePoint from the world) and clears their counters;
+//   1. admit: queued requests, in arrival order, take free chunks; a request
+//      that does not fit is passed over by later ones that do (a large request
+//      does not hold up the small ones behind it), until it has been passed
+//      over kMaxBypass times, after which nothing more is admitted ahead of it;
+//      the points of all admitted requests go to the device in one copy from a
+//      pinned staging buffer, and one launch scatters them into their slots,
+//      locates them (LocatePoint from the world) and clears their counters;
 //   2. step: one launch over the chunks of all admitted requests advances every
 //      live track by up to steps_per_launch steps, each GetSafety and
 //      FindNextBoundaryAndStep (one warp per track, the navigator of
@@ -189,6 +192,7 @@ int srv_grid(int64_t ntracks) {
 struct Request {
   int64_t id = -1;
   int64_t n = 0;
+  int32_t bypassed = 0;    // admissions of later requests while this one waited
   std::vector<double> in;  // x, y, z, dx, dy, dz (6 n)
   std::vector<int32_t> chunks;
   std::vector<TrackResult> out;
@@ -268,21 +272,35 @@ template <uint32_t kMask> void launch_step(vgb_server *s, int64_t nt) {
         s->d_live, s->g->dev.nav_flags);
 }
 
-// Admits queued requests while free chunks last (arrival order: a request that
-// does not fit blocks the ones behind it), all in one copy and one launch.
+// A waiting request is passed over by at most this many later admissions; then
+// the later requests wait behind it until the slots it needs are free.
+constexpr int32_t kMaxBypass = 16;
+
+// Admits queued requests while free chunks last, all in one copy and one
+// launch: in arrival order, each request that fits; one that does not stays
+// queued and later ones may pass it, up to kMaxBypass times.
 vgb_status admit(vgb_server *s) {
   std::vector<Request *> batch;
   int64_t nc = 0;
+  std::vector<Request *> waiting;  // passed over in this admission, in order
   while (!s->queue.empty()) {
     Request *r = s->queue.front();
     const int64_t need = (r->n + kChunk - 1) / kChunk;
-    if (need > (int64_t)s->free_chunks.size()) break;
+    if (need > (int64_t)s->free_chunks.size()) {
+      if (r->bypassed >= kMaxBypass) break;  // it goes next: nothing passes it
+      s->queue.pop_front();
+      waiting.push_back(r);
+      continue;
+    }
     s->queue.pop_front();
+    for (Request *w : waiting) ++w->bypassed;
     r->chunks.assign(s->free_chunks.end() - need, s->free_chunks.end());
     s->free_chunks.resize(s->free_chunks.size() - need);
     batch.push_back(r);
     nc += need;
   }
+  // the passed-over requests go back to the front, in their arrival order
+  for (auto it = waiting.rbegin(); it != waiting.rend(); ++it) s->queue.push_front(*it);
   if (batch.empty()) return VGB_OK;
   const int64_t nt = nc * kChunk;
   int64_t c = 0;
