@@ -970,12 +970,14 @@ def main():
     peaks = load_peaks()
     fma = measure_fma_peaks(torch.cuda.current_stream())
     line = run_shapes(args, args.workload, wls[args.workload], args.precision, peaks, fma,
-                      world=world, rank=rank, dist=dist if world > 1 else None)
+                      with_e2e=not args.no_e2e, world=world, rank=rank,
+                      dist=dist if world > 1 else None)
     line["fma_peaks"] = fma
     if extra:
         other = "fp32r" if args.precision == "fp64" else "fp64"
         line["other_precision"] = summary(run_shapes(args, "shapes", wls["shapes"], other, peaks,
-                                                     fma, with_e2e=True, with_cpu=False))
+                                                     fma, with_e2e=not args.no_e2e,
+                                                     with_cpu=False))
         line["configs"] = {
             "box": summary(run_shapes(args, "box", wls["box"], "fp64", peaks, fma,
                                       with_e2e=False)),

@@ -297,9 +297,11 @@ typedef struct vgb_basket_plan vgb_basket_plan;
 
 /* Builds the tile table of nb baskets (host array) for the op mask `ops` (bits
  * 1 << vgb_op over CONTAINS, INSIDE, DISTANCE_TO_IN, DISTANCE_TO_OUT,
- * SAFETY_TO_IN, SAFETY_TO_OUT).  block = threads per CTA (128, 256 or 512) and
+ * SAFETY_TO_IN, SAFETY_TO_OUT).  block = threads per CTA (256 or 512) and
  * tile = points per tile (a multiple of block); 0 picks the defaults (256,
- * 1024) until vgb_basket_tune chooses. */
+ * 1024) until vgb_basket_tune chooses.  A launch runs one kernel per shape kind
+ * present (booleans per component pair), as concurrent branches of the
+ * caller's stream. */
 vgb_status vgb_basket_plan_create(const vgb_geometry *g, const vgb_basket *baskets, int32_t nb,
                                   uint32_t ops, int32_t block, int32_t tile,
                                   vgb_basket_plan **plan);

@@ -1,13 +1,18 @@
 // baskets.cu -- many baskets (placed volume + its points) in one persistent launch,
 // the autotuner that picks its launch shape, and its CUDA-graph replay.
 //
-// A plan splits every basket into tiles of `tile` points; tile t belongs to the
-// basket found by a binary search over the per-basket tile prefix.  A CTA takes
-// tiles t = blockIdx.x, blockIdx.x + gridDim.x, ... (the grid is sized to the
-// resident CTAs of 148 SMs), stages the tile's shape record and transform in
-// shared memory (one broadcast read per tile instead of a parameter bank) and
-// runs the fused per-point ops of batch.cuh over the tile's points.  Each tile
-// holds one shape, so the shape switch is uniform across the CTA.
+// A plan keeps its baskets sorted by shape kind and splits every basket into
+// tiles of `tile` points; tile t belongs to the basket found by a binary search
+// over the per-basket tile prefix.  Each kind present has its own kernel
+// (k_baskets_kind: that shape's per-point code only, registers sized for it),
+// and the kinds' kernels run as concurrent branches forked from the caller's
+// stream, so a captured graph holds them as parallel nodes of one launch.  A
+// CTA takes its kind's tiles t0 + blockIdx.x, + gridDim.x, ... (the grid is
+// sized to the kernel's resident CTAs on every SM), stages the tile's shape
+// record and transform in shared memory (one broadcast read per tile instead of
+// a parameter bank) and runs the fused per-point ops of batch.cuh over the
+// tile's points.  The allocation-free entry point (below) runs all kinds in one
+// kernel with a switch over the shapes (k_baskets).
 #include <algorithm>
 #include <cstring>
 #include <mutex>
@@ -99,16 +104,40 @@ __global__ void __launch_bounds__(kBlock, 1)
   }
 }
 
-template <uint32_t kOps> int occupancy_grid(int block) {
+// One shape kind: the tiles [t0, t1) of the baskets [b0, b1) (the plan keeps
+// its baskets sorted by kind), with the kind's own per-point code, so the
+// kernel carries no switch over every shape and its registers fit its shape.
+template <class Ops, class P, int kBlock, uint32_t kOps>
+__global__ void __launch_bounds__(kBlock)
+    k_baskets_kind(const BasketGeom G, const BasketRec *__restrict__ baskets,
+                   const int64_t *__restrict__ prefix, int32_t b0, int32_t b1, int64_t t0,
+                   int64_t t1, int32_t tile, const FusedIO io) {
+  __shared__ __align__(16) double srec[kRecDoubles];
+  __shared__ DXform sx;
+  for (int64_t t = t0 + blockIdx.x; t < t1; t += gridDim.x) {
+    int lo = b0, hi = b1;
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (prefix[mid] <= t) lo = mid; else hi = mid;
+    }
+    const BasketRec b = baskets[lo];
+    const int64_t first = b.offset + (t - prefix[lo]) * tile;
+    const int64_t last = b.offset + b.count;
+    const int64_t end = first + tile < last ? first + tile : last;
+    const UnplacedRec u = G.unplaced[b.unplaced];
+    run_tile<Ops, P, kBlock, kOps>(G.params + u.param_off, G.xforms + b.xform, first, end, io,
+                                   srec, &sx);
+  }
+}
+
+// resident CTAs of the all-shape kernel on every SM (the allocation-free entry
+// point launches it with 256-thread CTAs)
+template <uint32_t kOps> int occupancy_grid() {
   int dev = 0, sms = 148, per_sm = 1;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaError_t e = cudaSuccess;
-  switch (block) {
-    case 128: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_baskets<128, kOps>, 128, 0); break;
-    case 256: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_baskets<256, kOps>, 256, 0); break;
-    default: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_baskets<512, kOps>, 512, 0); break;
-  }
+  const cudaError_t e =
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_baskets<256, kOps>, 256, 0);
   if (e != cudaSuccess || per_sm < 1) {
     cudaGetLastError();
     per_sm = 1;
@@ -117,7 +146,7 @@ template <uint32_t kOps> int occupancy_grid(int block) {
 }
 
 bool valid_shape(int block, int tile) {
-  return (block == 128 || block == 256 || block == 512) && tile >= block && tile % block == 0 &&
+  return (block == 256 || block == 512) && tile >= block && tile % block == 0 &&
          tile <= (1 << 16);
 }
 
@@ -138,6 +167,18 @@ struct vgb_basket_plan {
   int32_t tile = 1024;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t graph_exec = nullptr;
+  // the shape kinds present: type, basket range [b0, b1) and tile range
+  // [t0, t1) of the kind in the kind-sorted basket order
+  struct Kind {
+    int32_t type, sub, b0, b1;  // sub: the component pair of a boolean kind
+    int64_t t0, t1;
+  };
+  std::vector<Kind> kinds;
+  // one stream and join event per kind after the first, and the fork event:
+  // the kinds' kernels run as concurrent branches (nodes of one captured graph)
+  std::vector<cudaStream_t> kstreams;
+  std::vector<cudaEvent_t> kjoin;
+  cudaEvent_t kfork = nullptr;
 };
 
 namespace vgb {
@@ -155,6 +196,10 @@ vgb_status set_tile(vgb_basket_plan *p, int32_t tile, cudaStream_t s) {
   if (e != cudaSuccess) return cuda_error(e, "basket plan: tile prefix upload");
   p->ntiles = prefix[p->nb];
   p->tile = tile;
+  for (auto &k : p->kinds) {
+    k.t0 = prefix[k.b0];
+    k.t1 = prefix[k.b1];
+  }
   return VGB_OK;
 }
 
@@ -173,25 +218,72 @@ FusedIO make_io(const vgb_basket_plan *p, const double *x, const double *y, cons
   return io;
 }
 
-template <uint32_t kOps>
-void launch_k(const vgb_basket_plan *p, const FusedIO &io, cudaStream_t s) {
+template <uint32_t kOps, int kBlock, class Ops, class P>
+void launch_kind_t(const vgb_basket_plan *p, const vgb_basket_plan::Kind &k, const FusedIO &io,
+                   cudaStream_t s) {
   const BasketGeom G = {p->g->dev.params, p->g->dev.unplaced, p->g->dev.xforms};
-  const int64_t cap = occupancy_grid<kOps>(p->block);
-  const int grid = (int)std::min<int64_t>(p->ntiles, cap);
-  switch (p->block) {
-    case 128: k_baskets<128, kOps><<<grid, 128, 0, s>>>(G, p->d_baskets, p->d_prefix, p->nb, p->ntiles, p->tile, io); break;
-    case 256: k_baskets<256, kOps><<<grid, 256, 0, s>>>(G, p->d_baskets, p->d_prefix, p->nb, p->ntiles, p->tile, io); break;
-    default: k_baskets<512, kOps><<<grid, 512, 0, s>>>(G, p->d_baskets, p->d_prefix, p->nb, p->ntiles, p->tile, io); break;
+  int dev = 0, sms = 148, per_sm = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_baskets_kind<Ops, P, kBlock, kOps>,
+                                                    kBlock, 0) != cudaSuccess || per_sm < 1) {
+    cudaGetLastError();
+    per_sm = 1;
   }
+  const int grid = (int)std::min<int64_t>(k.t1 - k.t0, (int64_t)sms * per_sm);
+  if (grid > 0)
+    k_baskets_kind<Ops, P, kBlock, kOps><<<grid, kBlock, 0, s>>>(
+        G, p->d_baskets, p->d_prefix, k.b0, k.b1, k.t0, k.t1, p->tile, io);
+}
+
+// A kind is a shape type; booleans are further told apart by their component
+// types, so the common pairs run their compile-time specialisations.
+constexpr int32_t kKindPairBox = 1, kKindPairBoxTube = 2;
+
+template <uint32_t kOps, int kBlock>
+void launch_kind(const vgb_basket_plan *p, const vgb_basket_plan::Kind &k, const FusedIO &io,
+                 cudaStream_t s) {
+  if (k.type == VGB_SHAPE_BOOLEAN) {
+    if (k.sub == kKindPairBoxTube)
+      launch_kind_t<kOps, kBlock, BoolBoxTube<double>, BooleanP>(p, k, io, s);
+    else if (k.sub == kKindPairBox)
+      launch_kind_t<kOps, kBlock, BoolBoxBox<double>, BooleanP>(p, k, io, s);
+    else
+      launch_kind_t<kOps, kBlock, BoolOps<double>, BooleanP>(p, k, io, s);
+    return;
+  }
+  switch (k.type) {
+#define VGB_KIND_CASE(T, OPS, P) \
+  case T: launch_kind_t<kOps, kBlock, OPS<double>, P>(p, k, io, s); break;
+    VGB_FOR_EACH_SHAPE(VGB_KIND_CASE)
+#undef VGB_KIND_CASE
+    default: break;
+  }
+}
+
+template <uint32_t kOps>
+void launch_kinds(const vgb_basket_plan *p, const FusedIO &io, cudaStream_t s) {
+  const int nk = (int)p->kinds.size();
+  if (nk > 1) cudaEventRecord(p->kfork, s);
+  for (int i = 0; i < nk; ++i) {
+    cudaStream_t ks = i == 0 ? s : p->kstreams[i - 1];
+    if (i > 0) cudaStreamWaitEvent(ks, p->kfork, 0);
+    if (p->block == 256)
+      launch_kind<kOps, 256>(p, p->kinds[i], io, ks);
+    else
+      launch_kind<kOps, 512>(p, p->kinds[i], io, ks);
+    if (i > 0) cudaEventRecord(p->kjoin[i - 1], ks);
+  }
+  for (int i = 1; i < nk; ++i) cudaStreamWaitEvent(s, p->kjoin[i - 1], 0);
 }
 
 vgb_status launch(const vgb_basket_plan *p, const FusedIO &io, cudaStream_t s) {
   if (p->ntiles == 0) return VGB_OK;
   if ((p->ops & ~kOpsDtiSti) == 0)
-    launch_k<kOpsDtiSti>(p, io, s);
+    launch_kinds<kOpsDtiSti>(p, io, s);
   else
-    launch_k<kOpsAll>(p, io, s);
-  count_launch();
+    launch_kinds<kOpsAll>(p, io, s);
+  count_launch((int)p->kinds.size());
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_error(e, "vgb_basket_run: kernel launch");
   return VGB_OK;
@@ -254,6 +346,47 @@ vgb_status vgb_basket_plan_create(const vgb_geometry *g, const vgb_basket *baske
     p->host[b] = BasketRec{pr.unplaced, pr.xform, k.offset, k.count};
     p->points = std::max<int64_t>(p->points, k.offset + k.count);
   }
+  // baskets in shape-kind order (each writes only its own points, so the order
+  // changes no result), one range per kind
+  auto sub_of = [&](const BasketRec &r) {
+    if (g->unplaced[r.unplaced].type != VGB_SHAPE_BOOLEAN) return 0;
+    const BooleanP &bp = *static_cast<const BooleanP *>(shape_params(g, r.unplaced));
+    if (bp.left.type == VGB_SHAPE_BOX && bp.right.type == VGB_SHAPE_TUBE) return kKindPairBoxTube;
+    if (bp.left.type == VGB_SHAPE_BOX && bp.right.type == VGB_SHAPE_BOX) return kKindPairBox;
+    return 0;
+  };
+  auto key_of = [&](const BasketRec &r) {
+    return g->unplaced[r.unplaced].type * 16 + sub_of(r);
+  };
+  std::stable_sort(p->host.begin(), p->host.end(), [&](const BasketRec &a, const BasketRec &b) {
+    return key_of(a) < key_of(b);
+  });
+  for (int b = 0; b < nb;) {
+    const int key = key_of(p->host[b]);
+    int e = b;
+    while (e < nb && key_of(p->host[e]) == key) ++e;
+    p->kinds.push_back({key / 16, key % 16, b, e, 0, 0});
+    b = e;
+  }
+  for (size_t k = 1; k < p->kinds.size(); ++k) {
+    cudaStream_t ks = nullptr;
+    cudaEvent_t ev = nullptr;
+    cudaError_t e = cudaStreamCreateWithFlags(&ks, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+    if (ks) p->kstreams.push_back(ks);
+    if (ev) p->kjoin.push_back(ev);
+    if (e != cudaSuccess) {
+      vgb_basket_plan_destroy(p);
+      return cuda_error(e, "vgb_basket_plan_create: kind streams");
+    }
+  }
+  if (p->kinds.size() > 1) {
+    cudaError_t e = cudaEventCreateWithFlags(&p->kfork, cudaEventDisableTiming);
+    if (e != cudaSuccess) {
+      vgb_basket_plan_destroy(p);
+      return cuda_error(e, "vgb_basket_plan_create: fork event");
+    }
+  }
   cudaError_t e = cudaMalloc((void **)&p->d_baskets, std::max(1, nb) * sizeof(BasketRec));
   if (e == cudaSuccess) e = cudaMalloc((void **)&p->d_prefix, (nb + 1) * sizeof(int64_t));
   if (e == cudaSuccess && nb > 0)
@@ -277,6 +410,9 @@ vgb_status vgb_basket_plan_destroy(vgb_basket_plan *p) {
   if (p->graph) cudaGraphDestroy(p->graph);
   cudaFree(p->d_baskets);
   cudaFree(p->d_prefix);
+  for (cudaStream_t ks : p->kstreams) cudaStreamDestroy(ks);
+  for (cudaEvent_t ev : p->kjoin) cudaEventDestroy(ev);
+  if (p->kfork) cudaEventDestroy(p->kfork);
   delete p;
   return VGB_OK;
 }
@@ -315,7 +451,7 @@ vgb_status vgb_basket_tune(vgb_basket_plan *p, const double *x, const double *y,
   cudaEventCreate(&e1);
   float best = -1.f;
   int bb = p->block, bt = p->tile;
-  const int blocks[] = {128, 256, 512};
+  const int blocks[] = {256, 512};
   const int mults[] = {1, 2, 4, 8, 16};
   for (int b : blocks) {
     for (int m : mults) {
@@ -482,7 +618,8 @@ template <uint32_t kOps>
 void noalloc_launch(const vgb_geometry *g, const BasketRec *rec, const int64_t *prefix,
                     int32_t nb, int64_t ntiles, const FusedIO &io, cudaStream_t s) {
   const BasketGeom G = {g->dev.params, g->dev.unplaced, g->dev.xforms};
-  const int grid = (int)std::min<int64_t>(ntiles, occupancy_grid<kOps>(kNoallocBlock));
+  static_assert(kNoallocBlock == 256, "the all-shape kernel is built for 256-thread CTAs");
+  const int grid = (int)std::min<int64_t>(ntiles, occupancy_grid<kOps>());
   k_baskets<kNoallocBlock, kOps><<<grid, kNoallocBlock, 0, s>>>(G, rec, prefix, nb, ntiles,
                                                                  kNoallocTile, io);
 }
