@@ -77,8 +77,11 @@ inline CD cbrt(CD a) { ++g_counts.trans; return CD(std::cbrt(a.v)); }
 inline CD fmod(CD a, CD b) { ++g_counts.trans; return CD(std::fmod(a.v, b.v)); }
 inline CD floor(CD a) { ++g_counts.trans; return CD(std::floor(a.v)); }
 inline CD cr_atan2(CD a, CD b) { ++g_counts.trans; return CD(std::atan2(a.v, b.v)); }
-inline CD cr_sin(CD a) { ++g_counts.trans; return CD(std::sin(a.v)); }
-inline CD cr_cos(CD a) { ++g_counts.trans; return CD(std::cos(a.v)); }
+inline void cr_sincos(CD a, CD *s, CD *c) {
+  g_counts.trans += 2;
+  *s = CD(std::sin(a.v));
+  *c = CD(std::cos(a.v));
+}
 inline CD cr_cbrt(CD a) { ++g_counts.trans; return CD(std::cbrt(a.v)); }
 inline bool isinf(CD a) { return std::isinf(a.v); }
 inline bool isnan(CD a) { return std::isnan(a.v); }

@@ -13,8 +13,5 @@
 extern "C" {
 double vgcr_atan2(double y, double x) { return vgb::cr_atan2(y, x); }
 double vgcr_cbrt(double x) { return vgb::cr_cbrt(x); }
-void vgcr_sincos(double x, double *s, double *c) {
-  *s = vgb::cr_sin(x);
-  *c = vgb::cr_cos(x);
-}
+void vgcr_sincos(double x, double *s, double *c) { vgb::cr_sincos(x, s, c); }
 }

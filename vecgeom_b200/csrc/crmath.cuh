@@ -150,22 +150,36 @@ VGB_HD void sincos_dd(double x, DD &s, DD &c) {
 
 }  // namespace crm
 
-// Correctly rounded sin/cos (|x| < 2^20; beyond, the library's value).
-VGB_HD double cr_sin(double x) {
-  if (!(fabs(x) < 0x1p20)) return sin(x);
+// The functions below are kept out of line: each holds an unrolled
+// double-double series, and one copy per kernel (instead of one per call site)
+// keeps the instruction footprint of the torus kernels small.
+
+// Correctly rounded sin and cos of one argument (|x| < 2^20; beyond, the
+// library's values), from one double-double evaluation.
+VGB_HD_NOINLINE void cr_sincos(double x, double *sn, double *cs) {
+  if (!(fabs(x) < 0x1p20)) {
+    *sn = sin(x);
+    *cs = cos(x);
+    return;
+  }
   crm::DD s, c;
   crm::sincos_dd(x, s, c);
-  return s.hi;
+  *sn = s.hi;
+  *cs = c.hi;
+}
+VGB_HD double cr_sin(double x) {
+  double s, c;
+  cr_sincos(x, &s, &c);
+  return s;
 }
 VGB_HD double cr_cos(double x) {
-  if (!(fabs(x) < 0x1p20)) return cos(x);
-  crm::DD s, c;
-  crm::sincos_dd(x, s, c);
-  return c.hi;
+  double s, c;
+  cr_sincos(x, &s, &c);
+  return c;
 }
 
 // Correctly rounded atan2 (finite, not both zero; otherwise the library's value).
-VGB_HD double cr_atan2(double y, double x) {
+VGB_HD_NOINLINE double cr_atan2(double y, double x) {
   const double t0 = atan2(y, x);
   if (!(fabs(x) < HUGE_VAL) || !(fabs(y) < HUGE_VAL) || (x == 0.0 && y == 0.0)) return t0;
   // scale (x, y) by a power of two so the products below neither overflow nor
@@ -180,7 +194,7 @@ VGB_HD double cr_atan2(double y, double x) {
 }
 
 // Correctly rounded cube root (finite, nonzero; otherwise the library's value).
-VGB_HD double cr_cbrt(double x) {
+VGB_HD_NOINLINE double cr_cbrt(double x) {
   const double y = cbrt(x);
   if (!(fabs(y) < HUGE_VAL) || y == 0.0 || !(fabs(x) > 0x1p-900) || !(fabs(x) < 0x1p900))
     return y;

@@ -61,6 +61,10 @@ template <class R> struct SphereOps {
     const R m = (R)4e-15 * (fabs(z) + rho);
     return f > m ? -1 : (f < -m ? 1 : 0);
   }
+  // atan2(rho, z) out of line: it is needed only within ~3e-15 rad of a cut,
+  // and one copy instead of one per comparison keeps the kernels' code small
+  static VGB_HD_NOINLINE R polar_atan2(R rho, R z) { return atan2(rho, z); }
+
   // theta = atan2(rho, z), evaluated only when a comparison needs its value
   struct PolarAngle {
     R rho, z, t;
@@ -68,7 +72,7 @@ template <class R> struct SphereOps {
     VGB_HD PolarAngle(R rho_, R z_) : rho(rho_), z(z_), t(0), known(false) {}
     VGB_HD R value() {
       if (!known) {
-        t = atan2(rho, z);
+        t = polar_atan2(rho, z);
         known = true;
       }
       return t;

@@ -65,8 +65,7 @@ template <class R> VGB_HD Cx<R> ccbrt(Cx<R> x) {
     rr = sqrt(x.r * x.r + x.i * x.i);
     const R angle = cr_atan2(x.i, x.r);
     const R newangle = angle / (R)3.;
-    s = cr_sin(newangle);
-    c = cr_cos(newangle);
+    cr_sincos(newangle, &s, &c);
   } else {
     rr = x.r;
     s = 0.;

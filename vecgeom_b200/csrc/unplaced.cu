@@ -590,6 +590,15 @@ std::vector<double> make_polyhedron(double phiStart, double phiDelta, int sides,
   for (int p = 0; p < nseg; ++p) {
     PhSeg &s = segs[p];
     std::memset(&s, 0, sizeof(s));
+    // Segment p's quadrilaterals start at an index = p (mod 16).  A quadrilateral
+    // is 33 doubles, so index mod 16 is its first shared-memory bank pair: the
+    // lanes of a warp on the same phi side of different segments then read
+    // different banks.  The inserted quadrilaterals are never read.
+    while ((int)(quads.size() % 16) != p % 16) {
+      PhQuad pad;
+      std::memset(&pad, 0, sizeof(pad));
+      quads.push_back(pad);
+    }
     s.has_inner = has_inner[p];
     s.outer_off = (int32_t)quads.size();
     s.outer_n = outer_n[p];
