@@ -126,8 +126,60 @@ __device__ __forceinline__ void batch_point(const P &prm, const DXform &X, const
   }
 }
 
+// Polycone DistanceToIn with warp-regrouped section walks.  The points' walks
+// take 1 to nsec section evaluations each; run one point per lane to the end
+// and a warp waits for its longest walk with its other lanes idle.  Here every
+// iteration evaluates one section for the point each lane holds, and the lanes
+// whose walk ended (a __ballot_sync over the warp) take the warp's next points
+// at once (ranked by __popc), so the warp stays full until its points run out.
+// A warp's points are those of the grid-stride order (slot s of global warp gw
+// is point 32 gw + 32 W (s / 32) + s % 32, W warps in the grid).
+template <class P>
+__device__ __forceinline__ void polycone_dti_regrouped(const P &prm, const DXform &X,
+                                                       const BatchIO &io) {
+  using Ops = PolyconeOps<double>;
+  using R = double;
+  constexpr unsigned kFull = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  double *out = static_cast<double *>(io.out);
+  int64_t next = 0;  // the warp's next slot (warp-uniform)
+  int64_t i = -1;    // the lane's point, -1: none
+  V3<R> q = {0, 0, 0}, v = {0, 0, 0};
+  R smax = 0, dist = 0;
+  typename Ops::DtiWalk w = {0, 0};
+  while (true) {
+    const bool free_lane = i < 0;
+    const unsigned m = __ballot_sync(kFull, free_lane);
+    if (free_lane) {
+      const int64_t s = next + __popc(m & ((1u << lane) - 1u));
+      const int64_t pi = 32 * gw + 32 * nw * (s >> 5) + (s & 31);
+      if (pi < io.n) {
+        i = pi;
+        const V3<R> mq = {ldg(io.x + i), ldg(io.y + i), ldg(io.z + i)};
+        const V3<R> md = {ldg(io.dx + i), ldg(io.dy + i), ldg(io.dz + i)};
+        q = xf_point(X, mq);
+        v = dti_dir<Ops>(X, md);
+        smax = ldg(io.step + i);
+        w = Ops::dti_begin(prm, q, v);
+      }
+    }
+    next += __popc(m);
+    if (!__any_sync(kFull, i >= 0)) break;
+    if (i >= 0 && Ops::dti_step(prm, q, v, smax, w, dist)) {
+      out[i] = dist;
+      i = -1;
+    }
+  }
+}
+
 template <class Ops, class P, int OP>
 __device__ __forceinline__ void batch_loop(const P &prm, const DXform &X, const BatchIO &io) {
+  if constexpr (std::is_same<Ops, PolyconeOps<double>>::value && OP == VGB_OP_DISTANCE_TO_IN) {
+    polycone_dti_regrouped(prm, X, io);
+    return;
+  }
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < io.n; i += stride)
     batch_point<Ops, P, OP>(prm, X, io, i);

@@ -57,20 +57,37 @@ template <class R> struct PolyconeOps {
     return contains(p, q) ? kInside : kOutside;
   }
 
-  // DistanceToIn (:125-165)
+  // DistanceToIn (:125-165) as a section walk: dti_begin picks the first
+  // section and the direction, each dti_step evaluates one section and says
+  // whether the walk is over (a finite distance, no z motion, or no section
+  // left); `distance` then holds the result.  The batch kernel runs the steps
+  // of many points interleaved (warp-regrouped), distance_to_in runs them in a
+  // loop: the same sections in the same order either way.
+  struct DtiWalk {
+    int index, increment;
+  };
+  static VGB_HD DtiWalk dti_begin(const PolyconeP &p, const V3<R> &q, const V3<R> &v) {
+    DtiWalk w;
+    w.increment = (v.z > 0) ? 1 : -1;
+    if (fabs(v.z) < (R)kTolerance) w.increment = 0;
+    w.index = section_index(p, q.z);
+    if (w.index == -1) w.index = 0;
+    if (w.index == -2) w.index = p.nsec - 1;
+    return w;
+  }
+  static VGB_HD bool dti_step(const PolyconeP &p, const V3<R> &q, const V3<R> &v, R smax,
+                              DtiWalk &w, R &distance) {
+    const PolySec &s = sec(p, w.index);
+    distance = C::distance_to_in(s.cone, shifted(q, s), v, smax);
+    if (distance < Lim<R>::inf() || !w.increment) return true;
+    w.index += w.increment;
+    return !(w.index >= 0 && w.index < p.nsec);
+  }
   static VGB_HD R distance_to_in(const PolyconeP &p, const V3<R> &q, const V3<R> &v, R smax) {
     R distance = Lim<R>::inf();
-    int increment = (v.z > 0) ? 1 : -1;
-    if (fabs(v.z) < (R)kTolerance) increment = 0;
-    int index = section_index(p, q.z);
-    if (index == -1) index = 0;
-    if (index == -2) index = p.nsec - 1;
-    do {
-      const PolySec &s = sec(p, index);
-      distance = C::distance_to_in(s.cone, shifted(q, s), v, smax);
-      if (distance < Lim<R>::inf() || !increment) break;
-      index += increment;
-    } while (index >= 0 && index < p.nsec);
+    DtiWalk w = dti_begin(p, q, v);
+    while (!dti_step(p, q, v, smax, w, distance)) {
+    }
     return distance;
   }
 
