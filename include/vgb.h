@@ -265,10 +265,13 @@ vgb_status vgb_SafetyToOut(const vgb_geometry *g, int32_t placed, int64_t n, con
  * DISTANCE_TO_IN, DISTANCE_TO_OUT, SAFETY_TO_IN, SAFETY_TO_OUT; outs[op] is the
  * output of each requested op.  With VGB_FUSED_DTO_INSIDE_ONLY set in flags,
  * DistanceToOut is evaluated only for points Contains() accepts; the others
- * get kInfinity.  Buffers are all device or all host memory; host buffers
+ * get kInfinity.  VGB_FUSED_LOCAL_INSIDE_ONLY does the same for DistanceToOut
+ * and SafetyToOut (the local-frame ops, meaningful for points inside), so one
+ * call covers what a caller would otherwise run as two (all points, then the
+ * inside subset).  Buffers are all device or all host memory; host buffers
  * cross to the device once per chunk for all the requested ops (staged as in
  * vgb_batch), and the call returns with the outputs written. */
-enum { VGB_FUSED_DTO_INSIDE_ONLY = 1 };
+enum { VGB_FUSED_DTO_INSIDE_ONLY = 1, VGB_FUSED_LOCAL_INSIDE_ONLY = 2 };
 vgb_status vgb_batch_fused(const vgb_geometry *g, int32_t placed, uint32_t ops, int64_t n,
                            const double *x, const double *y, const double *z, const double *dx,
                            const double *dy, const double *dz, const double *step_max,

@@ -305,3 +305,38 @@ def test_fused_host_staging_across_chunks(on_device):
     from vecgeom_b200 import workloads as W
     fused_against_per_op(spec_of_kind("sphere"), (1 << 20) * 2 + 4099, W.SEED_BASE + 43,
                          on_device)
+
+
+@pytest.mark.parametrize("kind", ["tube", "sphere", "polycone", "boolsub"])
+@pytest.mark.parametrize("on_device", [True, False], ids=["device", "host"])
+def test_fused_local_ops_inside_only(kind, on_device):
+    """VGB_FUSED_LOCAL_INSIDE_ONLY: one fused call gives every op on all points,
+    with DistanceToOut and SafetyToOut equal to the per-op results where
+    Contains() holds and kInfinity elsewhere."""
+    import torch
+    import vecgeom_b200 as V
+    from vecgeom_b200 import workloads as W
+    spec = spec_of_kind(kind)
+    n = 1 << 15
+    wl = W.make_workload(spec, n, W.SEED_BASE + 47)
+    g, pv = build_placed(spec, "generic")
+    pts, dirs = (wl.x, wl.y, wl.z), (wl.dx, wl.dy, wl.dz)
+    want = run_all_ops(pv, pts, dirs, pts, dirs, wl.step)
+    conv = dev if on_device else (lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory())
+    dt = {"contains": torch.uint8, "inside": torch.int32}
+    outs = {k: torch.zeros(n, dtype=dt.get(k, torch.float64),
+                           device="cuda" if on_device else "cpu") for k in FUSED_OPS}
+    if not on_device:
+        outs = {k: v.pin_memory() for k, v in outs.items()}
+    pv.fused(0x3f, V.SOA3D(*(conv(a) for a in pts)), {FUSED_OPS[k]: v for k, v in outs.items()},
+             V.SOA3D(*(conv(a) for a in dirs)), conv(wl.step), local_inside_only=True)
+    torch.cuda.synchronize()
+    got = {k: v.cpu().numpy() for k, v in outs.items()}
+    inside = want["contains"].astype(bool)
+    for k in FUSED_OPS:
+        a, b = got[k], want[k]
+        if k in ("distance_to_out", "safety_to_out"):
+            assert np.isinf(a[~inside]).all() and (a[~inside] > 0).all(), k
+            a, b = a[inside], b[inside]
+        same = (a == b) | (np.isnan(a) & np.isnan(b)) if a.dtype.kind == "f" else a == b
+        assert same.all(), f"{kind} fused {k}: {np.flatnonzero(~same)[:5]}"

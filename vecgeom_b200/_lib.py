@@ -34,6 +34,7 @@ PREC_FP64 = 0
 PREC_FP32_REFINE = 1
 
 FUSED_DTO_INSIDE_ONLY = 1
+FUSED_LOCAL_INSIDE_ONLY = 2
 
 
 class VgbError(RuntimeError):

@@ -126,58 +126,87 @@ __device__ __forceinline__ void batch_point(const P &prm, const DXform &X, const
   }
 }
 
-// Polycone DistanceToIn with warp-regrouped section walks.  The points' walks
-// take 1 to nsec section evaluations each; run one point per lane to the end
-// and a warp waits for its longest walk with its other lanes idle.  Here every
-// iteration evaluates one section for the point each lane holds, and the lanes
-// whose walk ended (a __ballot_sync over the warp) take the warp's next points
-// at once (ranked by __popc), so the warp stays full until its points run out.
-// A warp's points are those of the grid-stride order (slot s of global warp gw
-// is point 32 gw + 32 W (s / 32) + s % 32, W warps in the grid).
-template <class P>
-__device__ __forceinline__ void polycone_dti_regrouped(const P &prm, const DXform &X,
-                                                       const BatchIO &io) {
-  using Ops = PolyconeOps<double>;
+// Distance walks with warp-regrouped steps: polycone DistanceToIn (a walk over
+// cone sections) and polyhedron DistanceToIn/DistanceToOut (walks over
+// z-segments).  A point's walk takes from one to all of its sections; run one
+// point per lane to the end and a warp waits for its longest walk with its
+// other lanes idle.  Here each iteration evaluates one step for the point each
+// lane holds, and the lanes whose walk ended (a __ballot_sync over the warp)
+// take the warp's next points at once (ranked by __popc), so the warp stays
+// full until its points run out; the steps of each point are the ones the
+// scalar function takes, so every result is the same.  A warp's points are
+// those of the grid-stride order (slot s of global warp gw is point
+// 32 gw + 32 W (s / 32) + s % 32, W warps in the grid).
+template <class Ops, int OP> struct RegroupedWalk : std::false_type {};
+template <> struct RegroupedWalk<PolyconeOps<double>, VGB_OP_DISTANCE_TO_IN> : std::true_type {};
+template <> struct RegroupedWalk<PolyhedronOps<double>, VGB_OP_DISTANCE_TO_IN> : std::true_type {};
+template <> struct RegroupedWalk<PolyhedronOps<double>, VGB_OP_DISTANCE_TO_OUT> : std::true_type {};
+
+template <class Ops, class P, int OP>
+__device__ __forceinline__ void walk_regrouped(const P &prm, const DXform &X, const BatchIO &io) {
   using R = double;
+  constexpr bool kIn = OP == VGB_OP_DISTANCE_TO_IN;
   constexpr unsigned kFull = 0xffffffffu;
   const int lane = threadIdx.x & 31;
   const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  auto point_of = [&](int64_t s) { return 32 * gw + 32 * nw * (s >> 5) + (s & 31); };
   double *out = static_cast<double *>(io.out);
   int64_t next = 0;  // the warp's next slot (warp-uniform)
   int64_t i = -1;    // the lane's point, -1: none
   V3<R> q = {0, 0, 0}, v = {0, 0, 0};
-  R smax = 0, dist = 0;
-  typename Ops::DtiWalk w = {0, 0};
+  R smax = 0;
+  typename Ops::Walk w;
   while (true) {
     const bool free_lane = i < 0;
     const unsigned m = __ballot_sync(kFull, free_lane);
     if (free_lane) {
-      const int64_t s = next + __popc(m & ((1u << lane) - 1u));
-      const int64_t pi = 32 * gw + 32 * nw * (s >> 5) + (s & 31);
+      const int64_t pi = point_of(next + __popc(m & ((1u << lane) - 1u)));
       if (pi < io.n) {
-        i = pi;
-        const V3<R> mq = {ldg(io.x + i), ldg(io.y + i), ldg(io.z + i)};
-        const V3<R> md = {ldg(io.dx + i), ldg(io.dy + i), ldg(io.dz + i)};
-        q = xf_point(X, mq);
-        v = dti_dir<Ops>(X, md);
-        smax = ldg(io.step + i);
-        w = Ops::dti_begin(prm, q, v);
+        const V3<R> mq = {ldg(io.x + pi), ldg(io.y + pi), ldg(io.z + pi)};
+        const V3<R> md = {ldg(io.dx + pi), ldg(io.dy + pi), ldg(io.dz + pi)};
+        smax = ldg(io.step + pi);
+        R res;
+        bool done;
+        if constexpr (kIn) {
+          q = xf_point(X, mq);
+          v = dti_dir<Ops>(X, md);
+          done = Ops::dti_begin(prm, q, v, smax, w, res);
+        } else {
+          q = mq;
+          v = md;
+          done = Ops::dto_begin(prm, q, v, smax, w, res);
+        }
+        if (done)
+          out[pi] = res;  // settled in the set-up; the lane stays free
+        else
+          i = pi;
       }
     }
     next += __popc(m);
-    if (!__any_sync(kFull, i >= 0)) break;
-    if (i >= 0 && Ops::dti_step(prm, q, v, smax, w, dist)) {
-      out[i] = dist;
-      i = -1;
+    const bool more = point_of(next) < io.n;  // warp-uniform
+    if (!__any_sync(kFull, i >= 0) && !more) break;
+    if (i >= 0) {
+      bool ended;
+      if constexpr (kIn)
+        ended = Ops::dti_step(prm, q, v, smax, w);
+      else
+        ended = Ops::dto_step(prm, q, v, smax, w);
+      if (ended) {
+        if constexpr (kIn)
+          out[i] = Ops::dti_end(prm, q, v, smax, w);
+        else
+          out[i] = Ops::dto_end(prm, q, v, smax, w);
+        i = -1;
+      }
     }
   }
 }
 
 template <class Ops, class P, int OP>
 __device__ __forceinline__ void batch_loop(const P &prm, const DXform &X, const BatchIO &io) {
-  if constexpr (std::is_same<Ops, PolyconeOps<double>>::value && OP == VGB_OP_DISTANCE_TO_IN) {
-    polycone_dti_regrouped(prm, X, io);
+  if constexpr (RegroupedWalk<Ops, OP>::value) {
+    walk_regrouped<Ops, P, OP>(prm, X, io);
     return;
   }
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
@@ -215,22 +244,25 @@ __device__ __forceinline__ void fused_point(const P &prm, const DXform &X, const
   V3<R> d = {0, 0, 0};
   if (need_dir) d = {ldg(io.dx + i), ldg(io.dy + i), ldg(io.dz + i)};
   bool c = false;
-  if ((ops & (1u << VGB_OP_CONTAINS)) || (io.flags & VGB_FUSED_DTO_INSIDE_ONLY))
-    c = Ops::contains(prm, l);
+  const bool dto_inside = io.flags & (VGB_FUSED_DTO_INSIDE_ONLY | VGB_FUSED_LOCAL_INSIDE_ONLY);
+  const bool sto_inside = io.flags & VGB_FUSED_LOCAL_INSIDE_ONLY;
+  if ((ops & (1u << VGB_OP_CONTAINS)) || dto_inside) c = Ops::contains(prm, l);
   if (ops & (1u << VGB_OP_CONTAINS)) static_cast<uint8_t *>(io.out[VGB_OP_CONTAINS])[i] = c;
   if (ops & (1u << VGB_OP_INSIDE))
     static_cast<int32_t *>(io.out[VGB_OP_INSIDE])[i] = Ops::inside(prm, l);
   if (ops & (1u << VGB_OP_SAFETY_TO_IN))
     static_cast<double *>(io.out[VGB_OP_SAFETY_TO_IN])[i] = Ops::safety_to_in(prm, l);
-  if (ops & (1u << VGB_OP_SAFETY_TO_OUT))
-    static_cast<double *>(io.out[VGB_OP_SAFETY_TO_OUT])[i] = Ops::safety_to_out(prm, m);
+  if (ops & (1u << VGB_OP_SAFETY_TO_OUT)) {
+    R r = Lim<R>::inf();
+    if (!sto_inside || c) r = Ops::safety_to_out(prm, m);
+    static_cast<double *>(io.out[VGB_OP_SAFETY_TO_OUT])[i] = r;
+  }
   if (ops & (1u << VGB_OP_DISTANCE_TO_IN))
     static_cast<double *>(io.out[VGB_OP_DISTANCE_TO_IN])[i] =
         Ops::distance_to_in(prm, l, dti_dir<Ops>(X, d), ldg(io.step + i));
   if (ops & (1u << VGB_OP_DISTANCE_TO_OUT)) {
     R r = Lim<R>::inf();
-    if (!(io.flags & VGB_FUSED_DTO_INSIDE_ONLY) || c)
-      r = Ops::distance_to_out(prm, m, d, ldg(io.step + i));
+    if (!dto_inside || c) r = Ops::distance_to_out(prm, m, d, ldg(io.step + i));
     static_cast<double *>(io.out[VGB_OP_DISTANCE_TO_OUT])[i] = r;
   }
 }

@@ -31,7 +31,7 @@ using namespace vgb;
 namespace {
 
 constexpr char kMagic[8] = {'V', 'G', 'B', 'G', 'E', 'O', 'M', '1'};
-constexpr uint32_t kVersion = 2;  // 2: polyhedron quadrilaterals padded to 33 doubles
+constexpr uint32_t kVersion = 3;  // 2: polyhedron quadrilaterals of 33 doubles; 3: polycone sections of 41
 
 uint64_t fnv1a(const uint8_t *p, size_t n) {
   uint64_t h = 1469598103934665603ull;

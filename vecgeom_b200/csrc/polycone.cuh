@@ -11,11 +11,16 @@
 
 namespace vgb {
 
+// 41 doubles (82 4-byte words): consecutive sections start 18 words apart, so
+// up to 16 sections map to distinct shared-memory banks when the lanes of a
+// warp read different sections (a 40-double record put every other section on
+// the same bank).
 struct PolySec {
   ConeP cone;    // UnplacedCone(prevRmin, prevRmax, rMin, rMax, dz, phiStart, phiTotal)
   double shift;  // fShift: z of the section centre
-  double pad;
+  double pad[2];
 };
+static_assert(sizeof(PolySec) == 41 * sizeof(double), "PolySec stride");
 
 struct PolyconeP {
   int32_t nsec;
@@ -60,35 +65,41 @@ template <class R> struct PolyconeOps {
   // DistanceToIn (:125-165) as a section walk: dti_begin picks the first
   // section and the direction, each dti_step evaluates one section and says
   // whether the walk is over (a finite distance, no z motion, or no section
-  // left); `distance` then holds the result.  The batch kernel runs the steps
-  // of many points interleaved (warp-regrouped), distance_to_in runs them in a
+  // left), dti_end returns the distance.  The batch kernel runs the steps of
+  // many points interleaved (warp-regrouped), distance_to_in runs them in a
   // loop: the same sections in the same order either way.
-  struct DtiWalk {
+  struct Walk {
     int index, increment;
+    R distance;
   };
-  static VGB_HD DtiWalk dti_begin(const PolyconeP &p, const V3<R> &q, const V3<R> &v) {
-    DtiWalk w;
+  static VGB_HD bool dti_begin(const PolyconeP &p, const V3<R> &q, const V3<R> &v, R,
+                               Walk &w, R &) {
     w.increment = (v.z > 0) ? 1 : -1;
     if (fabs(v.z) < (R)kTolerance) w.increment = 0;
     w.index = section_index(p, q.z);
     if (w.index == -1) w.index = 0;
     if (w.index == -2) w.index = p.nsec - 1;
-    return w;
+    w.distance = Lim<R>::inf();
+    return false;
   }
   static VGB_HD bool dti_step(const PolyconeP &p, const V3<R> &q, const V3<R> &v, R smax,
-                              DtiWalk &w, R &distance) {
+                              Walk &w) {
     const PolySec &s = sec(p, w.index);
-    distance = C::distance_to_in(s.cone, shifted(q, s), v, smax);
-    if (distance < Lim<R>::inf() || !w.increment) return true;
+    w.distance = C::distance_to_in(s.cone, shifted(q, s), v, smax);
+    if (w.distance < Lim<R>::inf() || !w.increment) return true;
     w.index += w.increment;
     return !(w.index >= 0 && w.index < p.nsec);
   }
+  static VGB_HD R dti_end(const PolyconeP &, const V3<R> &, const V3<R> &, R, const Walk &w) {
+    return w.distance;
+  }
   static VGB_HD R distance_to_in(const PolyconeP &p, const V3<R> &q, const V3<R> &v, R smax) {
-    R distance = Lim<R>::inf();
-    DtiWalk w = dti_begin(p, q, v);
-    while (!dti_step(p, q, v, smax, w, distance)) {
+    Walk w;
+    R r;
+    if (dti_begin(p, q, v, smax, w, r)) return r;
+    while (!dti_step(p, q, v, smax, w)) {
     }
-    return distance;
+    return dti_end(p, q, v, smax, w);
   }
 
   // DistanceToOut (:167-292)

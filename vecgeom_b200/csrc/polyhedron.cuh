@@ -320,57 +320,97 @@ template <class R> struct PolyhedronOps {
     distance = dt;
   }
 
-  // ScalarDistanceToInKernel (:775-827); the batch kernel applies the generic transform
-  static VGB_HD R distance_to_in(const PolyhedronP &p, const V3<R> &pt, const V3<R> &dir, R smax) {
+  // ScalarDistanceToInKernel (:775-827) and ScalarDistanceToOutKernel
+  // (:851-890) as z-segment walks: *_begin does the set-up (and may settle the
+  // point at once), each *_step evaluates one segment and says whether the walk
+  // is over, *_end adds the endcaps and the step limit.  The batch kernel runs
+  // the steps of many points interleaved (warp-regrouped); distance_to_in/out
+  // run them in a loop: the same segments in the same order either way.  The
+  // batch kernel applies the generic transform.
+  struct Walk {
+    int zi;
+    bool right;
+    R distance;
+  };
+  static VGB_HD bool dti_begin(const PolyhedronP &p, const V3<R> &pt, const V3<R> &dir, R smax,
+                               Walk &w, R &res) {
     const V3<R> bp = {pt.x, pt.y, pt.z - (R)p.btube_offset};
     const bool inBounds = T::contains(p.btube, bp);
     if (!inBounds) {
       const R tubeDistance = T::distance_to_in(p.btube, bp, dir, smax);
-      if (tubeDistance == Lim<R>::inf()) return Lim<R>::inf();
+      if (tubeDistance == Lim<R>::inf()) {
+        res = Lim<R>::inf();
+        return true;
+      }
     }
     int zi = find_z(p, pt.z);
     const int zMax = p.nseg;
     zi = zi < 0 ? 0 : (zi >= zMax ? zMax - 1 : zi);
-    if (inBounds && segment_contains(p, pt, zi)) return (R)-1.;
-    const bool goingRight = dir.z >= 0;
-    R distance = Lim<R>::inf();
-    if (goingRight) {
-      for (; zi < zMax; ++zi) {
-        distance = dti_segment(p, zi, pt, dir);
-        if (distance >= 0 && distance < Lim<R>::inf()) break;
-      }
-    } else {
-      for (; zi >= 0; --zi) {
-        distance = dti_segment(p, zi, pt, dir);
-        if (distance >= 0 && distance < Lim<R>::inf()) break;
-      }
+    if (inBounds && segment_contains(p, pt, zi)) {
+      res = (R)-1.;
+      return true;
     }
+    w.zi = zi;
+    w.right = dir.z >= 0;
+    w.distance = Lim<R>::inf();
+    return false;
+  }
+  static VGB_HD bool dti_step(const PolyhedronP &p, const V3<R> &pt, const V3<R> &dir, R,
+                              Walk &w) {
+    w.distance = dti_segment(p, w.zi, pt, dir);
+    if (w.distance >= 0 && w.distance < Lim<R>::inf()) return true;
+    if (w.right) return !(++w.zi < p.nseg);
+    return !(--w.zi >= 0);
+  }
+  static VGB_HD R dti_end(const PolyhedronP &p, const V3<R> &pt, const V3<R> &dir, R smax,
+                          const Walk &w) {
+    R distance = w.distance;
     to_endcaps<false>(p, pt, dir, distance);
     return distance < smax ? distance : smax;
   }
+  static VGB_HD R distance_to_in(const PolyhedronP &p, const V3<R> &pt, const V3<R> &dir, R smax) {
+    Walk w;
+    R r;
+    if (dti_begin(p, pt, dir, smax, w, r)) return r;
+    while (!dti_step(p, pt, dir, smax, w)) {
+    }
+    return dti_end(p, pt, dir, smax, w);
+  }
 
-  // ScalarDistanceToOutKernel (:851-890)
-  static VGB_HD R distance_to_out(const PolyhedronP &p, const V3<R> &pt, const V3<R> &dir, R smax) {
+  static VGB_HD bool dto_begin(const PolyhedronP &p, const V3<R> &pt, const V3<R> &dir, R,
+                               Walk &w, R &) {
     int zi = find_z(p, pt.z);
     const int zMax = p.nseg;
-    zi = zi < 0 ? 0 : (zi >= zMax ? zMax - 1 : zi);
-    const bool goingRight = dir.z >= 0;
-    R distance = Lim<R>::inf();
-    if (goingRight) {
-      for (; zi < zMax; ++zi) {
-        distance = dto_segment(p, zi, zplane(p, zi), zplane(p, zi + 1), pt, dir);
-        if (distance >= 0 && distance < Lim<R>::inf()) break;
-        if (zplane(p, zi) - pt.z > distance) break;
-      }
-    } else {
-      for (; zi >= 0; --zi) {
-        distance = dto_segment(p, zi, zplane(p, zi), zplane(p, zi + 1), pt, dir);
-        if (distance >= 0 && distance < Lim<R>::inf()) break;
-        if (pt.z - zplane(p, zi) > distance) break;
-      }
+    w.zi = zi < 0 ? 0 : (zi >= zMax ? zMax - 1 : zi);
+    w.right = dir.z >= 0;
+    w.distance = Lim<R>::inf();
+    return false;
+  }
+  static VGB_HD bool dto_step(const PolyhedronP &p, const V3<R> &pt, const V3<R> &dir, R,
+                              Walk &w) {
+    const int zi = w.zi;
+    w.distance = dto_segment(p, zi, zplane(p, zi), zplane(p, zi + 1), pt, dir);
+    if (w.distance >= 0 && w.distance < Lim<R>::inf()) return true;
+    if (w.right) {
+      if (zplane(p, zi) - pt.z > w.distance) return true;
+      return !(++w.zi < p.nseg);
     }
+    if (pt.z - zplane(p, zi) > w.distance) return true;
+    return !(--w.zi >= 0);
+  }
+  static VGB_HD R dto_end(const PolyhedronP &p, const V3<R> &pt, const V3<R> &dir, R smax,
+                          const Walk &w) {
+    R distance = w.distance;
     to_endcaps<true>(p, pt, dir, distance);
     return distance < smax ? distance : smax;
+  }
+  static VGB_HD R distance_to_out(const PolyhedronP &p, const V3<R> &pt, const V3<R> &dir, R smax) {
+    Walk w;
+    R r;
+    if (dto_begin(p, pt, dir, smax, w, r)) return r;
+    while (!dto_step(p, pt, dir, smax, w)) {
+    }
+    return dto_end(p, pt, dir, smax, w);
   }
 
   // ScalarSafetyToZSegmentSquared (:502-533)

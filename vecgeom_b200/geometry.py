@@ -172,8 +172,11 @@ class PlacedVolume:
 
     def fused(self, ops: int, points: SOA3D, outs: dict, dirs: SOA3D | None = None,
               step_max=None, dto_inside_only: bool = False, precision: int = L.PREC_FP64,
-              stream=None) -> None:
-        """Several ops over the same points in one pass (vgb_batch_fused)."""
+              stream=None, local_inside_only: bool = False) -> None:
+        """Several ops over the same points in one pass (vgb_batch_fused).
+        dto_inside_only: DistanceToOut only where Contains() holds;
+        local_inside_only: DistanceToOut and SafetyToOut only there (the others
+        get kInfinity)."""
         g = self.geometry
         g._require_closed()
         arr = (ctypes.c_void_p * 6)()
@@ -185,7 +188,8 @@ class PlacedVolume:
             g.handle, self.id, ops, points.size(), _addr(points.x), _addr(points.y),
             _addr(points.z), _addr(d.x) if d else None, _addr(d.y) if d else None,
             _addr(d.z) if d else None, _addr(step_max), arr,
-            L.FUSED_DTO_INSIDE_ONLY if dto_inside_only else 0, precision, s))
+            (L.FUSED_DTO_INSIDE_ONLY if dto_inside_only else 0)
+            | (L.FUSED_LOCAL_INSIDE_ONLY if local_inside_only else 0), precision, s))
 
 
 class Geometry:
