@@ -71,41 +71,78 @@ VGB_HD DD dd_mul_d(DD a, double b) {
   return fast_two_sum(p.hi, p.lo);
 }
 
-// 1/n!, n = 0..27, double-double (hi, lo), rounded from 300-bit values.
+// 1/n!, n = 0..27, double-double (hi, lo), rounded from 300-bit values.  The
+// series below reads them in a loop that is not unrolled (one index for the
+// whole warp, so a broadcast read): the code of one evaluation stays small.
+#ifdef __CUDACC__
+static __constant__ double kCrmInvFactDev[28][2] = {
+    {0x1.0000000000000p+0, 0.0},
+    {0x1.0000000000000p+0, 0.0},
+    {0x1.0000000000000p-1, 0.0},
+    {0x1.5555555555555p-3, 0x1.5555555555555p-57},
+    {0x1.5555555555555p-5, 0x1.5555555555555p-59},
+    {0x1.1111111111111p-7, 0x1.1111111111111p-63},
+    {0x1.6c16c16c16c17p-10, -0x1.f49f49f49f49fp-65},
+    {0x1.a01a01a01a01ap-13, 0x1.a01a01a01a01ap-73},
+    {0x1.a01a01a01a01ap-16, 0x1.a01a01a01a01ap-76},
+    {0x1.71de3a556c734p-19, -0x1.c154f8ddc6c00p-73},
+    {0x1.27e4fb7789f5cp-22, 0x1.cbbc05b4fa99ap-76},
+    {0x1.ae64567f544e4p-26, -0x1.c062e06d1f209p-80},
+    {0x1.1eed8eff8d898p-29, -0x1.2aec959e14c06p-83},
+    {0x1.6124613a86d09p-33, 0x1.f28e0cc748ebep-87},
+    {0x1.93974a8c07c9dp-37, 0x1.05d6f8a2efd1fp-92},
+    {0x1.ae7f3e733b81fp-41, 0x1.1d8656b0ee8cbp-97},
+    {0x1.ae7f3e733b81fp-45, 0x1.1d8656b0ee8cbp-101},
+    {0x1.952c77030ad4ap-49, 0x1.ac981465ddc6cp-103},
+    {0x1.6827863b97d97p-53, 0x1.eec01221a8b0bp-107},
+    {0x1.2f49b46814157p-57, 0x1.2650f61dbdcb4p-112},
+    {0x1.e542ba4020225p-62, 0x1.ea72b4afe3c2fp-120},
+    {0x1.71b8ef6dcf572p-66, -0x1.d043ae40c4647p-120},
+    {0x1.0ce396db7f853p-70, -0x1.aebcdbd20331cp-124},
+    {0x1.761b41316381ap-75, -0x1.3423c7d91404fp-130},
+    {0x1.f2cf01972f578p-80, -0x1.9ada5fcc1ab14p-135},
+    {0x1.3f3ccdd165fa9p-84, -0x1.58ddadf344487p-139},
+    {0x1.88e85fc6a4e5ap-89, -0x1.71c37ebd16540p-143},
+    {0x1.d1ab1c2dccea3p-94, 0x1.054d0c78aea14p-149}};
+#endif
+static const double kCrmInvFactHost[28][2] = {
+    {0x1.0000000000000p+0, 0.0},
+    {0x1.0000000000000p+0, 0.0},
+    {0x1.0000000000000p-1, 0.0},
+    {0x1.5555555555555p-3, 0x1.5555555555555p-57},
+    {0x1.5555555555555p-5, 0x1.5555555555555p-59},
+    {0x1.1111111111111p-7, 0x1.1111111111111p-63},
+    {0x1.6c16c16c16c17p-10, -0x1.f49f49f49f49fp-65},
+    {0x1.a01a01a01a01ap-13, 0x1.a01a01a01a01ap-73},
+    {0x1.a01a01a01a01ap-16, 0x1.a01a01a01a01ap-76},
+    {0x1.71de3a556c734p-19, -0x1.c154f8ddc6c00p-73},
+    {0x1.27e4fb7789f5cp-22, 0x1.cbbc05b4fa99ap-76},
+    {0x1.ae64567f544e4p-26, -0x1.c062e06d1f209p-80},
+    {0x1.1eed8eff8d898p-29, -0x1.2aec959e14c06p-83},
+    {0x1.6124613a86d09p-33, 0x1.f28e0cc748ebep-87},
+    {0x1.93974a8c07c9dp-37, 0x1.05d6f8a2efd1fp-92},
+    {0x1.ae7f3e733b81fp-41, 0x1.1d8656b0ee8cbp-97},
+    {0x1.ae7f3e733b81fp-45, 0x1.1d8656b0ee8cbp-101},
+    {0x1.952c77030ad4ap-49, 0x1.ac981465ddc6cp-103},
+    {0x1.6827863b97d97p-53, 0x1.eec01221a8b0bp-107},
+    {0x1.2f49b46814157p-57, 0x1.2650f61dbdcb4p-112},
+    {0x1.e542ba4020225p-62, 0x1.ea72b4afe3c2fp-120},
+    {0x1.71b8ef6dcf572p-66, -0x1.d043ae40c4647p-120},
+    {0x1.0ce396db7f853p-70, -0x1.aebcdbd20331cp-124},
+    {0x1.761b41316381ap-75, -0x1.3423c7d91404fp-130},
+    {0x1.f2cf01972f578p-80, -0x1.9ada5fcc1ab14p-135},
+    {0x1.3f3ccdd165fa9p-84, -0x1.58ddadf344487p-139},
+    {0x1.88e85fc6a4e5ap-89, -0x1.71c37ebd16540p-143},
+    {0x1.d1ab1c2dccea3p-94, 0x1.054d0c78aea14p-149}};
 struct InvFact {
   double hi, lo;
 };
 VGB_HD InvFact inv_fact(int n) {
-  switch (n) {
-  case 0: return {0x1.0000000000000p+0, 0.0};
-  case 1: return {0x1.0000000000000p+0, 0.0};
-  case 2: return {0x1.0000000000000p-1, 0.0};
-  case 3: return {0x1.5555555555555p-3, 0x1.5555555555555p-57};
-  case 4: return {0x1.5555555555555p-5, 0x1.5555555555555p-59};
-  case 5: return {0x1.1111111111111p-7, 0x1.1111111111111p-63};
-  case 6: return {0x1.6c16c16c16c17p-10, -0x1.f49f49f49f49fp-65};
-  case 7: return {0x1.a01a01a01a01ap-13, 0x1.a01a01a01a01ap-73};
-  case 8: return {0x1.a01a01a01a01ap-16, 0x1.a01a01a01a01ap-76};
-  case 9: return {0x1.71de3a556c734p-19, -0x1.c154f8ddc6c00p-73};
-  case 10: return {0x1.27e4fb7789f5cp-22, 0x1.cbbc05b4fa99ap-76};
-  case 11: return {0x1.ae64567f544e4p-26, -0x1.c062e06d1f209p-80};
-  case 12: return {0x1.1eed8eff8d898p-29, -0x1.2aec959e14c06p-83};
-  case 13: return {0x1.6124613a86d09p-33, 0x1.f28e0cc748ebep-87};
-  case 14: return {0x1.93974a8c07c9dp-37, 0x1.05d6f8a2efd1fp-92};
-  case 15: return {0x1.ae7f3e733b81fp-41, 0x1.1d8656b0ee8cbp-97};
-  case 16: return {0x1.ae7f3e733b81fp-45, 0x1.1d8656b0ee8cbp-101};
-  case 17: return {0x1.952c77030ad4ap-49, 0x1.ac981465ddc6cp-103};
-  case 18: return {0x1.6827863b97d97p-53, 0x1.eec01221a8b0bp-107};
-  case 19: return {0x1.2f49b46814157p-57, 0x1.2650f61dbdcb4p-112};
-  case 20: return {0x1.e542ba4020225p-62, 0x1.ea72b4afe3c2fp-120};
-  case 21: return {0x1.71b8ef6dcf572p-66, -0x1.d043ae40c4647p-120};
-  case 22: return {0x1.0ce396db7f853p-70, -0x1.aebcdbd20331cp-124};
-  case 23: return {0x1.761b41316381ap-75, -0x1.3423c7d91404fp-130};
-  case 24: return {0x1.f2cf01972f578p-80, -0x1.9ada5fcc1ab14p-135};
-  case 25: return {0x1.3f3ccdd165fa9p-84, -0x1.58ddadf344487p-139};
-  case 26: return {0x1.88e85fc6a4e5ap-89, -0x1.71c37ebd16540p-143};
-  default: return {0x1.d1ab1c2dccea3p-94, 0x1.054d0c78aea14p-149};
-  }
+#ifdef __CUDA_ARCH__
+  return {kCrmInvFactDev[n][0], kCrmInvFactDev[n][1]};
+#else
+  return {kCrmInvFactHost[n][0], kCrmInvFactHost[n][1]};
+#endif
 }
 
 // sin and cos of r, |r| <= pi/4, in double-double: Horner over r^2.
@@ -115,6 +152,7 @@ VGB_HD void sincos_reduced(DD r, DD &s, DD &c) {
   DD as = {-f.hi, -f.lo};  // (-1)^13 / 27!
   f = inv_fact(26);
   DD ac = {-f.hi, -f.lo};  // (-1)^13 / 26!
+#pragma unroll 1
   for (int j = 12; j >= 0; --j) {
     const double sg = (j & 1) ? -1.0 : 1.0;
     const InvFact fs = inv_fact(2 * j + 1), fc = inv_fact(2 * j);
