@@ -350,68 +350,63 @@ template <class R> struct SphereOps {
         }
       };
       const R tanS2 = (R)s.tanSTheta2, tanE2 = (R)s.tanETheta2;
+      // The two cones' quadratics (t1, t2, b, c, d2, d of every branch below),
+      // evaluated once for each lane that reaches this point instead of inside
+      // the branches: points on either side of a cut take different branches,
+      // and a warp would evaluate the same quadratic once per branch group.  The
+      // expressions and their order are the reference's, and a branch uses a
+      // cone only where the reference goes on with it (t1 != 0, d2 >= 0), so
+      // every result is unchanged.  A missing cone (stheta = 0, eTheta = pi) has
+      // dist2 = inf: its c is +-inf, so it never yields a candidate, and it is
+      // not evaluated.
+      const bool haveS = s.stheta != 0, haveE = s.eTheta < kPi;
+      R t1S = 0, t2S = 0, bS = 0, d2S = -1, dS = 0;
+      R t1E = 0, t2E = 0, bE = 0, d2E = -1, dE = 0;
+      if (haveS) {
+        t1S = (R)1 - v.z * v.z * ((R)1 + tanS2);
+        t2S = pDotV2d - p.z * v.z * tanS2;
+        bS = t2S / t1S;
+        c = dist2STheta / t1S;
+        d2S = bS * bS - c;
+        dS = sqrt(d2S);
+      }
+      if (haveE) {
+        t1E = (R)1 - v.z * v.z * ((R)1 + tanE2);
+        t2E = pDotV2d - p.z * v.z * tanE2;
+        bE = t2E / t1E;
+        c = dist2ETheta / t1E;
+        d2E = bE * bE - c;
+        dE = sqrt(d2E);
+      }
+      const bool realS = haveS && (t1S != 0) && (d2S >= 0);
+      const bool realE = haveE && (t1E != 0) && (d2E >= 0);
       if (pTheta.lt(s.cut[kCutTolS])) {
-        t1 = (R)1 - v.z * v.z * ((R)1 + tanS2);
-        t2 = pDotV2d - p.z * v.z * tanS2;
-        if (t1 != 0) {
-          b = t2 / t1;
-          c = dist2STheta / t1;
-          d2 = b * b - c;
-          if (d2 >= 0) {
-            d = sqrt(d2);
-            sd = -b - d;
-            zi = p.z + sd * v.z;
-            if ((sd < 0) || (zi * (fSTheta - piby2) > 0)) sd = -b + d;
-            if ((sd >= 0) && (sd < snxt)) accept(sd, fSTheta);
-          }
+        // (unreachable without a start cone: the cut lies below theta = 0)
+        if (realS) {
+          sd = -bS - dS;
+          zi = p.z + sd * v.z;
+          if ((sd < 0) || (zi * (fSTheta - piby2) > 0)) sd = -bS + dS;
+          if ((sd >= 0) && (sd < snxt)) accept(sd, fSTheta);
         }
-        if (s.eTheta < kPi) {
-          t1 = (R)1 - v.z * v.z * ((R)1 + tanE2);
-          t2 = pDotV2d - p.z * v.z * tanE2;
-          if (t1 != 0) {
-            b = t2 / t1;
-            c = dist2ETheta / t1;
-            d2 = b * b - c;
-            if (d2 >= 0) {
-              d = sqrt(d2);
-              sd = -b + d;
-              if ((sd >= 0) && (sd < snxt)) accept(sd, eTheta);
-            }
-          }
+        if (realE) {
+          sd = -bE + dE;
+          if ((sd >= 0) && (sd < snxt)) accept(sd, eTheta);
         }
       } else if (pTheta.gt(s.cut[kCutTolE])) {
-        t1 = (R)1 - v.z * v.z * ((R)1 + tanE2);
-        t2 = pDotV2d - p.z * v.z * tanE2;
-        if (t1 != 0) {
-          b = t2 / t1;
-          c = dist2ETheta / t1;
-          d2 = b * b - c;
-          if (d2 >= 0) {
-            d = sqrt(d2);
-            sd = -b - d;
-            zi = p.z + sd * v.z;
-            if ((sd < 0) || (zi * (eTheta - piby2) > 0)) sd = -b + d;
-            if ((sd >= 0) && (sd < snxt)) accept(sd, eTheta);
-          }
+        // (unreachable without an end cone: the cut lies above theta = pi)
+        if (realE) {
+          sd = -bE - dE;
+          zi = p.z + sd * v.z;
+          if ((sd < 0) || (zi * (eTheta - piby2) > 0)) sd = -bE + dE;
+          if ((sd >= 0) && (sd < snxt)) accept(sd, eTheta);
         }
-        if (s.stheta != 0) {
-          t1 = (R)1 - v.z * v.z * ((R)1 + tanS2);
-          t2 = pDotV2d - p.z * v.z * tanS2;
-          if (t1 != 0) {
-            b = t2 / t1;
-            c = dist2STheta / t1;
-            d2 = b * b - c;
-            if (d2 >= 0) {
-              d = sqrt(d2);
-              sd = -b + d;
-              if ((sd >= 0) && (sd < snxt)) accept(sd, fSTheta);
-            }
-          }
+        if (realS) {
+          sd = -bS + dS;
+          if ((sd >= 0) && (sd < snxt)) accept(sd, fSTheta);
         }
       } else if (pTheta.lt(s.cut[kCutTolS2]) && (fSTheta > halfAngTol)) {
-        t2 = pDotV2d - p.z * v.z * tanS2;
-        if ((t2 >= 0 && tolIRMin2 < rad2 && rad2 < tolIRMax2 && s.stheta < kPi / 2) ||
-            (t2 < 0 && tolIRMin2 < rad2 && rad2 < tolIRMax2 && s.stheta > kPi / 2) ||
+        if ((t2S >= 0 && tolIRMin2 < rad2 && rad2 < tolIRMax2 && s.stheta < kPi / 2) ||
+            (t2S < 0 && tolIRMin2 < rad2 && rad2 < tolIRMax2 && s.stheta > kPi / 2) ||
             (v.z < 0 && tolIRMin2 < rad2 && rad2 < tolIRMax2 && s.stheta == kPi / 2)) {
           if (!s.fullPhi && rho2 != 0) {
             if (psi_ok(s, p.x, p.y, sqrt(rho2), s.cosHDPhiIT)) return (R)0;
@@ -419,21 +414,13 @@ template <class R> struct SphereOps {
             return (R)0;
           }
         }
-        t1 = (R)1 - v.z * v.z * ((R)1 + tanS2);
-        if (t1 != 0) {
-          b = t2 / t1;
-          c = dist2STheta / t1;
-          d2 = b * b - c;
-          if (d2 >= 0) {
-            d = sqrt(d2);
-            sd = -b + d;
-            if ((sd >= halfCarTol) && (sd < snxt) && (s.stheta < kPi / 2)) accept(sd, fSTheta);
-          }
+        if (realS) {
+          sd = -bS + dS;
+          if ((sd >= halfCarTol) && (sd < snxt) && (s.stheta < kPi / 2)) accept(sd, fSTheta);
         }
       } else if (pTheta.gt(s.cut[kCutTolE2]) && (s.eTheta < kPi - kAngTolerance)) {
-        t2 = pDotV2d - p.z * v.z * tanE2;
-        if (((t2 < 0) && (s.eTheta < kPi / 2) && (tolIRMin2 < rad2) && (rad2 < tolIRMax2)) ||
-            ((t2 >= 0) && (s.eTheta > kPi / 2) && (tolIRMin2 < rad2) && (rad2 < tolIRMax2)) ||
+        if (((t2E < 0) && (s.eTheta < kPi / 2) && (tolIRMin2 < rad2) && (rad2 < tolIRMax2)) ||
+            ((t2E >= 0) && (s.eTheta > kPi / 2) && (tolIRMin2 < rad2) && (rad2 < tolIRMax2)) ||
             ((v.z > 0) && (s.eTheta == kPi / 2) && (tolIRMin2 < rad2) && (rad2 < tolIRMax2))) {
           if (!s.fullPhi && rho2 != 0) {
             if (psi_ok(s, p.x, p.y, sqrt(rho2), s.cosHDPhiIT)) return (R)0;
@@ -441,41 +428,18 @@ template <class R> struct SphereOps {
             return (R)0;
           }
         }
-        t1 = (R)1 - v.z * v.z * ((R)1 + tanE2);
-        if (t1 != 0) {
-          b = t2 / t1;
-          c = dist2ETheta / t1;
-          d2 = b * b - c;
-          if (d2 >= 0) {
-            d = sqrt(d2);
-            sd = -b + d;
-            if ((sd >= halfCarTol) && (sd < snxt) && (s.eTheta > kPi / 2)) accept(sd, eTheta);
-          }
+        if (realE) {
+          sd = -bE + dE;
+          if ((sd >= halfCarTol) && (sd < snxt) && (s.eTheta > kPi / 2)) accept(sd, eTheta);
         }
       } else {
-        t1 = (R)1 - v.z * v.z * ((R)1 + tanS2);
-        t2 = pDotV2d - p.z * v.z * tanS2;
-        if (t1 != 0) {
-          b = t2 / t1;
-          c = dist2STheta / t1;
-          d2 = b * b - c;
-          if (d2 >= 0) {
-            d = sqrt(d2);
-            sd = -b + d;
-            if ((sd >= 0) && (sd < snxt)) accept(sd, fSTheta);
-          }
+        if (realS) {
+          sd = -bS + dS;
+          if ((sd >= 0) && (sd < snxt)) accept(sd, fSTheta);
         }
-        t1 = (R)1 - v.z * v.z * ((R)1 + tanE2);
-        t2 = pDotV2d - p.z * v.z * tanE2;
-        if (t1 != 0) {
-          b = t2 / t1;
-          c = dist2ETheta / t1;
-          d2 = b * b - c;
-          if (d2 >= 0) {
-            d = sqrt(d2);
-            sd = -b + d;
-            if ((sd >= 0) && (sd < snxt)) accept(sd, eTheta);
-          }
+        if (realE) {
+          sd = -bE + dE;
+          if ((sd >= 0) && (sd < snxt)) accept(sd, eTheta);
         }
       }
     }
