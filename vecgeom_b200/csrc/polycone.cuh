@@ -71,6 +71,11 @@ template <class R> struct PolyconeOps {
   struct Walk {
     int index, increment;
     R distance;
+    // DistanceToOut: the distance so far, the steps taken, the point in the
+    // current section's frame
+    int istep;
+    R total;
+    V3<R> pn;
   };
   static VGB_HD bool dti_begin(const PolyconeP &p, const V3<R> &q, const V3<R> &v, R,
                                Walk &w, R &) {
@@ -102,11 +107,16 @@ template <class R> struct PolyconeOps {
     return dti_end(p, q, v, smax, w);
   }
 
-  // DistanceToOut (:167-292)
-  static VGB_HD R distance_to_out(const PolyconeP &p, const V3<R> &q, const V3<R> &v, R smax) {
+  // DistanceToOut (:167-292) as a section walk, like DistanceToIn: dto_begin
+  // finds the starting section (and settles single-section polycones and points
+  // in no section), each dto_step runs one section of the loop body and says
+  // whether the walk is over, dto_end returns the accumulated distance.
+  static VGB_HD bool dto_begin(const PolyconeP &p, const V3<R> &q, const V3<R> &v, R smax,
+                               Walk &w, R &res) {
     if (p.nsec == 1) {
       const PolySec &s = sec(p, 0);
-      return C::distance_to_out(s.cone, shifted(q, s), v, smax);
+      res = C::distance_to_out(s.cone, shifted(q, s), v, smax);
+      return true;
     }
     const int indexLow = section_index(p, q.z - (R)kTolerance);
     const int indexHigh = section_index(p, q.z + (R)kTolerance);
@@ -118,45 +128,60 @@ template <class R> struct PolyconeOps {
       index = indexLow;
       if (index < 0) index = section_index(p, q.z);
     }
-    if (index < 0) return (R)0.;
-    R totalDistance = 0.;
-    R dist;
-    int increment = (v.z > 0) ? 1 : -1;
-    if (fabs(v.z) < (R)kTolerance) increment = 0;
-    int istep = 0;
-    V3<R> pn = q;
-    do {
-      const PolySec &s = sec(p, index);
-      if ((totalDistance != 0) || (istep < 2)) {
-        pn = {q.x + totalDistance * v.x, q.y + totalDistance * v.y, q.z + totalDistance * v.z};
-        pn.z = pn.z - (R)s.shift;
-        if (C::inside(s.cone, pn) == kOutside) break;
+    if (index < 0) {
+      res = (R)0.;
+      return true;
+    }
+    w.index = index;
+    w.total = 0.;
+    w.increment = (v.z > 0) ? 1 : -1;
+    if (fabs(v.z) < (R)kTolerance) w.increment = 0;
+    w.istep = 0;
+    w.pn = q;
+    return false;
+  }
+  static VGB_HD bool dto_step(const PolyconeP &p, const V3<R> &q, const V3<R> &v, R smax,
+                              Walk &w) {
+    const PolySec &s = sec(p, w.index);
+    if ((w.total != 0) || (w.istep < 2)) {
+      w.pn = {q.x + w.total * v.x, q.y + w.total * v.y, q.z + w.total * v.z};
+      w.pn.z = w.pn.z - (R)s.shift;
+      if (C::inside(s.cone, w.pn) == kOutside) return true;
+    } else {
+      w.pn.z = w.pn.z - (R)s.shift;
+    }
+    w.istep++;
+    const R dist = C::distance_to_out(s.cone, w.pn, v, smax);
+    if (fabs(dist) < (R)0.5 * (R)kTolerance) {
+      int index1 = w.index;
+      if ((w.index > 0) && (w.index < p.nsec - 1)) {
+        index1 += w.increment;
       } else {
-        pn.z = pn.z - (R)s.shift;
+        if ((w.index == 0) && (w.increment > 0)) index1 += w.increment;
+        if ((w.index == p.nsec - 1) && (w.increment < 0)) index1 += w.increment;
       }
-      istep++;
-      dist = C::distance_to_out(s.cone, pn, v, smax);
-      if (fabs(dist) < (R)0.5 * (R)kTolerance) {
-        int index1 = index;
-        if ((index > 0) && (index < p.nsec - 1)) {
-          index1 += increment;
-        } else {
-          if ((index == 0) && (increment > 0)) index1 += increment;
-          if ((index == p.nsec - 1) && (increment < 0)) index1 += increment;
-        }
-        const R td = totalDistance + dist;
-        V3<R> pte = {q.x + td * v.x, q.y + td * v.y, q.z + td * v.z};
-        const PolySec &s1 = sec(p, index1);
-        pte.z = pte.z - (R)s1.shift;
-        if (!C::contains(s1.cone, pte)) break;
-      }
-      totalDistance += dist;
-      index += increment;
-    } while (increment != 0 && index >= 0 && index < p.nsec);
-    return totalDistance;
+      const R td = w.total + dist;
+      V3<R> pte = {q.x + td * v.x, q.y + td * v.y, q.z + td * v.z};
+      const PolySec &s1 = sec(p, index1);
+      pte.z = pte.z - (R)s1.shift;
+      if (!C::contains(s1.cone, pte)) return true;
+    }
+    w.total += dist;
+    w.index += w.increment;
+    return !(w.increment != 0 && w.index >= 0 && w.index < p.nsec);
+  }
+  static VGB_HD R dto_end(const PolyconeP &, const V3<R> &, const V3<R> &, R, const Walk &w) {
+    return w.total;
+  }
+  static VGB_HD R distance_to_out(const PolyconeP &p, const V3<R> &q, const V3<R> &v, R smax) {
+    Walk w;
+    R r;
+    if (dto_begin(p, q, v, smax, w, r)) return r;
+    while (!dto_step(p, q, v, smax, w)) {
+    }
+    return dto_end(p, q, v, smax, w);
   }
 
-  // SafetyToIn (:336-408)
   static VGB_HD R safety_to_in(const PolyconeP &p, const V3<R> &q) {
     int index = section_index(p, q.z);
     bool needZ = false;
