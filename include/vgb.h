@@ -14,7 +14,9 @@
  *     (volumes/PlacedVolume.h:145-250).
  *   - DistanceToIn returns -1 for a point inside a box and kInfinity on a miss.
  * Every pointer argument may be device memory (the kernels read it in place) or
- * host memory (the call stages it through device buffers on the given stream).
+ * host memory (the call stages it through device buffers in chunks, after the
+ * work already queued on the given stream; pinned host memory lets the copies
+ * in and out of neighbouring chunks run at the same time).
  * Buffers belong to the caller.  Nothing aborts: every entry point returns a
  * vgb_status and vgb_last_error() describes the last failure on this thread.
  */

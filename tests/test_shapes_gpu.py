@@ -307,6 +307,53 @@ def test_fused_host_staging_across_chunks(on_device):
                          on_device)
 
 
+@pytest.mark.parametrize("pinned", [False, True], ids=["pageable", "pinned"])
+def test_batch_host_staging_across_chunks(pinned):
+    """vgb_batch with host buffers over more points than the staging slots hold
+    at once (3 x 2^20 + 4099: full chunks, then the halving tail, every slot
+    reused) equals the device-buffer call bit for bit: a point op, a directed
+    op, and a Minimize op, which also reads its outputs and node ids in."""
+    import torch
+    import vecgeom_b200 as V
+    from vecgeom_b200 import workloads as W
+    spec = spec_of_kind("tube")
+    n = 3 * (1 << 20) + 4099
+    wl = W.make_workload(spec, n, W.SEED_BASE + 53)
+    g, pv = build_placed(spec, "generic")
+    if pinned:
+        hconv = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()  # noqa: E731
+        hbuf = lambda a: torch.from_numpy(np.array(a)).pin_memory()  # noqa: E731
+        back = lambda t: t.numpy()  # noqa: E731
+    else:
+        hconv = hbuf = lambda a: np.array(a)  # noqa: E731
+        back = lambda t: t  # noqa: E731
+    pts, dirs = (wl.x, wl.y, wl.z), (wl.dx, wl.dy, wl.dz)
+    PD, DD, SD = V.SOA3D(*map(dev, pts)), V.SOA3D(*map(dev, dirs)), dev(wl.step)
+    PH, DH, SH = V.SOA3D(*map(hconv, pts)), V.SOA3D(*map(hconv, dirs)), hconv(wl.step)
+
+    ins_d = torch.empty(n, dtype=torch.int32, device="cuda")
+    ins_h = hbuf(np.zeros(n, np.int32))
+    pv.Inside(PD, ins_d)
+    pv.Inside(PH, ins_h)
+    dti_d = torch.empty(n, dtype=torch.float64, device="cuda")
+    dti_h = hbuf(np.zeros(n))
+    pv.DistanceToIn(PD, DD, SD, dti_d)
+    pv.DistanceToIn(PH, DH, SH, dti_h)
+    # Minimize: the current step is the input distance, node ids start at -1
+    start = wl.step * 0.5
+    min_d, ids_d = dev(start), dev(np.full(n, -1, np.int32))
+    min_h, ids_h = hbuf(start), hbuf(np.full(n, -1, np.int32))
+    pv.DistanceToInMinimize(PD, DD, 7, min_d, ids_d)
+    pv.DistanceToInMinimize(PH, DH, 7, min_h, ids_h)
+    torch.cuda.synchronize()
+    for what, a, b in (("Inside", ins_h, ins_d), ("DistanceToIn", dti_h, dti_d),
+                       ("DistanceToInMinimize", min_h, min_d), ("node ids", ids_h, ids_d)):
+        a, b = back(a), b.cpu().numpy()
+        same = (a == b) | (np.isnan(a) & np.isnan(b)) if a.dtype.kind == "f" else a == b
+        assert same.all(), f"host-staged {what}: {np.flatnonzero(~same)[:5]}"
+    assert (back(ids_h) == 7).any() and (back(ids_h) == -1).any()
+
+
 @pytest.mark.parametrize("kind", ["tube", "sphere", "polycone", "boolsub"])
 @pytest.mark.parametrize("on_device", [True, False], ids=["device", "host"])
 def test_fused_local_ops_inside_only(kind, on_device):

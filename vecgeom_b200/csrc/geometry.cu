@@ -170,9 +170,12 @@ vgb_status vgb_geometry_destroy(vgb_geometry *g) {
     cudaFree(g->dev.logicals);
     cudaFree(g->dev.daughters);
     cudaFree(g->staging);
-    if (g->staging_streams[0]) cudaStreamDestroy(g->staging_streams[0]);
-    if (g->staging_streams[1]) cudaStreamDestroy(g->staging_streams[1]);
+    for (cudaStream_t st : g->staging_streams)
+      if (st) cudaStreamDestroy(st);
     if (g->staging_start) cudaEventDestroy(g->staging_start);
+    for (auto &slot : g->staging_ev)
+      for (cudaEvent_t ev : slot)
+        if (ev) cudaEventDestroy(ev);
     cudaSetDevice(prev);
   }
   delete g;

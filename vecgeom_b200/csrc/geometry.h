@@ -110,12 +110,16 @@ struct vgb_geometry {
   bool closed = false;
   int device = -1;
   vgb::DeviceImage dev;
-  // host-pointer calls stage through one device buffer on two internal streams
+  // host-pointer calls stage through one device buffer of kStageSlots chunk slots on
+  // three internal streams (copies in, kernels, copies out) ordered by per-slot events
+  static constexpr int kStageSlots = 3;
   std::mutex staging_mu;  // serialises host-pointer calls that share the buffer
   void *staging = nullptr;
   size_t staging_bytes = 0;
-  cudaStream_t staging_streams[2] = {nullptr, nullptr};
+  cudaStream_t staging_streams[3] = {nullptr, nullptr, nullptr};
   cudaEvent_t staging_start = nullptr;
+  // per slot: its copy-in done, its kernel done, its copy-out done
+  cudaEvent_t staging_ev[kStageSlots][3] = {};
 };
 
 namespace vgb {

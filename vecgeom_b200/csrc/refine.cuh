@@ -125,7 +125,6 @@ struct SphereRefine {
     const float pDotV3d = pDotV2d + pz * vz;
     const float r = sqrtf(rad2);
     // error bounds of the point quantities
-    const FE Rho2 = {rho2, kSafe * 4.f * kU * rho2};
     const FE Rad2 = {rad2, kSafe * 5.f * kU * rad2};
     const FE B2 = {pDotV2d, kSafe * 4.f * kU * sqrtf(rho2)};
     const FE B = {pDotV3d, kSafe * 5.f * kU * r};
