@@ -671,19 +671,18 @@ template <class R> struct SphereOps {
     }
     const R rds = sqrt(p.x * p.x + p.y * p.y + p.z * p.z);
     if (!s.fullTheta && (rds != zero)) {
-      R pTheta = (R)(kPi / 2) - asin(p.z / rds);
-      if (pTheta < zero) pTheta = pTheta + (R)kPi;
-      const R dTheta1 = (R)s.stheta - pTheta;
-      const R dTheta2 = pTheta - (R)s.eTheta;
-      if (dTheta1 > dTheta2) {
-        if (dTheta1 >= zero) {
-          const R safeTheta = rds * sin(dTheta1);
-          if (safety <= safeTheta) safety = safeTheta;
-        }
-      } else if (dTheta2 >= zero) {
-        const R safeTheta = rds * sin(dTheta2);
-        if (safety <= safeTheta) safety = safeTheta;
-      }
+      // The reference takes pTheta = pi/2 - asin(z / rds) and, on the side of the
+      // cut the point lies beyond, rds sin(stheta - pTheta) or rds sin(pTheta -
+      // eTheta).  With sin pTheta = rho / rds and cos pTheta = z / rds these are
+      // z sin(stheta) - rho cos(stheta) and rho cos(eTheta) - z sin(eTheta), whose
+      // signs are those of the angle differences (both lie in [-pi, pi]; at most
+      // one is positive, as stheta < eTheta).  Same value to ~1e-15 mm (rounding
+      // of the two products against that of asin, the subtraction and sin),
+      // without the two transcendental calls.
+      const R toS = p.z * (R)s.sinSTheta - rho * (R)s.cosSTheta;
+      const R toE = rho * (R)s.cosETheta - p.z * (R)s.sinETheta;
+      const R safeTheta = toS > toE ? toS : toE;
+      if (safeTheta >= zero && safety <= safeTheta) safety = safeTheta;
     }
     if (safety < zero) safety = zero;
     return safety;
@@ -710,12 +709,13 @@ template <class R> struct SphereOps {
     }
     const R rds = sqrt(p.x * p.x + p.y * p.y + p.z * p.z);
     if (!s.fullTheta && (rds > 0)) {
-      R pTheta = (R)(kPi / 2) - asin(p.z / rds);
-      if (pTheta < zero) pTheta = pTheta + (R)kPi;
-      const R eTheta = (R)s.stheta + (R)s.dtheta;
-      const R dTheta1 = pTheta - (R)s.stheta;
-      const R dTheta2 = eTheta - pTheta;
-      const R safeTheta = (dTheta1 < dTheta2) ? rds * sin(dTheta1) : rds * sin(dTheta2);
+      // The reference's rds sin(pTheta - stheta) and rds sin(eTheta - pTheta)
+      // (pTheta = pi/2 - asin(z / rds)), expanded as in SafetyToIn; it keeps the
+      // one of the smaller angle, which for angles in [0, pi] with eTheta - stheta
+      // <= pi is the smaller of the two values.
+      const R fromS = rho * (R)s.cosSTheta - p.z * (R)s.sinSTheta;
+      const R fromE = p.z * (R)s.sinETheta - rho * (R)s.cosETheta;
+      const R safeTheta = fromS < fromE ? fromS : fromE;
       if (safety > safeTheta) safety = safeTheta;
     }
     if (safety < zero) safety = zero;
