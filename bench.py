@@ -1,7 +1,8 @@
 """Benchmark of the VecGeom hot path on B200: Mpoints/s per shape op.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl vgb|reference]
-                    [--workload shapes|box] [--precision fp64|fp32r]
+                    [--workload shapes|heavy|box|baskets|nav] [--only]
+                    [--precision fp64|fp32r]
 
 One step = every (shape, op) pair of the workload run once over its whole
 point batch through libvgb.  Workloads (seeded synthetic inputs):
@@ -11,15 +12,22 @@ point batch through libvgb.  Workloads (seeded synthetic inputs):
           surface, isotropic directions; Inside, Contains, SafetyToIn,
           DistanceToIn on all points, SafetyToOut and DistanceToOut on the
           points Contains() accepts.
+  heavy   torus, polycone, polyhedron and box minus tube, the same mix and ops.
   box     box (10, 20, 30) mm, 2^20 points uniform in 1.5x the box; the same
           ops (DistanceToOut/SafetyToOut on the inside subset).
+  baskets 4,096 mixed baskets of eight jittered shape kinds at random
+          placements, DistanceToIn + SafetyToIn, one captured graph launch.
+  nav     served navigation in a layered detector: Poisson-arriving requests of
+          straight tracks, steps/s with p50/p99 request latency.
+The default run is the shapes workload, with the others and the FP32+refine
+form as extra keys (--only: just the named workload).
 value = point-ops / device time (inputs resident in HBM, L2 flushed before
 every op, CUDA events around each launch); e2e = the same ops through the
 public API with pinned host buffers (copies inside the timed region): per
-shape one vgb_batch_fused call for the ops on all points and one for the ops
-on the Contains() subset, so each point set crosses PCIe once; e2e_per_op =
-the same with one vgb_batch call per op.
-Rank 0 prints one JSON line.
+shape one vgb_batch_fused call over all points (DistanceToOut and SafetyToOut
+where Contains() holds), so each point crosses PCIe once, with the PCIe floor
+of the same bytes beside it; e2e_per_op = the same with one vgb_batch call per
+op.  Rank 0 prints one JSON line.
 """
 from __future__ import annotations
 
@@ -69,8 +77,8 @@ def parse():
 # dominant kernels, each from one ncu capture of a 2^22-point launch; the
 # profiles/ summaries give the command and the raw figures.
 NCU_TRAFFIC_PER_POINT = {
-    # profiles/sphere_distance_to_in_fp64_2p22.md, build B
-    ("sphere", "distance_to_in", "fp64"): (201.42464e6 + 24.0576e6) / 4194304,
+    # profiles/sphere_distance_to_in_fp64_2p22.md, current build
+    ("sphere", "distance_to_in", "fp64"): (202.023424e6 + 24.235776e6) / 4194304,
 }
 
 
@@ -648,6 +656,42 @@ def measure_fma_peaks(stream) -> dict:
     return out
 
 
+def pcie_floor(h2d_bytes: int, d2h_bytes: int, reps: int = 3) -> dict:
+    """The end-to-end floor of a step that moves h2d_bytes in and d2h_bytes out:
+    both copies between pinned host buffers and the device at once, on two
+    streams (a B200's copy engines run the two directions together, each a
+    little slower than alone), timed like the end-to-end calls (wall clock
+    around synchronised repetitions, after one untimed)."""
+    import torch
+    hi = torch.empty(h2d_bytes, dtype=torch.uint8).pin_memory()
+    ho = torch.empty(d2h_bytes, dtype=torch.uint8).pin_memory()
+    di = torch.empty(h2d_bytes, dtype=torch.uint8, device="cuda")
+    do = torch.empty(d2h_bytes, dtype=torch.uint8, device="cuda")
+    s_in, s_out = torch.cuda.Stream(), torch.cuda.Stream()
+
+    def timed(copy_in: bool, copy_out: bool) -> float:
+        def once():
+            if copy_in:
+                with torch.cuda.stream(s_in):
+                    di.copy_(hi, non_blocking=True)
+            if copy_out:
+                with torch.cuda.stream(s_out):
+                    ho.copy_(do, non_blocking=True)
+        once()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            once()
+        torch.cuda.synchronize()
+        return (time.perf_counter() - t0) / reps
+    t_in, t_out, t_both = timed(True, False), timed(False, True), timed(True, True)
+    del hi, ho, di, do
+    return {"both_ms": round(t_both * 1e3, 3), "h2d_gbs": round(h2d_bytes / t_in / 1e9, 1),
+            "d2h_gbs": round(d2h_bytes / t_out / 1e9, 1),
+            "method": "the step's bytes copied in and out at once (pinned host memory, two "
+                      "streams), wall clock like the end-to-end calls"}
+
+
 def op_roofline(opname: str, points: int, seconds: float, flops_per_point, hbm_gbs: float,
                 fp64_gflops) -> dict:
     """Where one op sits: its algorithmic bytes (and flops, when counted) per
@@ -886,7 +930,12 @@ def run_shapes(args, workload: str, wls: dict, precision: str, peaks: dict, fma:
             e2e = {"value": round(world * pts_per_step / e2e_s / 1e6, 2), "unit": "Mpoints/s",
                    "h2d_bytes_per_step": int(fused_h2d), "d2h_bytes_per_step": int(fused_d2h),
                    "api": "vgb_batch_fused, host buffers, 1 call per shape (local ops where "
-                          "Contains() holds)"}
+                          "Contains() holds)",
+                   "ms_per_step": round(e2e_s * 1e3, 3)}
+            # the PCIe floor of the same bytes: the end-to-end step's bound
+            floor = pcie_floor(int(fused_h2d), int(fused_d2h))
+            floor["frac"] = round(floor["both_ms"] / (e2e_s * 1e3), 4)
+            e2e["pcie_floor"] = floor
         else:
             e2e = e2e_per_op
 

@@ -46,7 +46,10 @@ template <> struct HasBase<PolyconeP> : std::true_type {};
 template <> struct HasBase<PolyhedronP> : std::true_type {};
 template <> struct HasBase<BooleanP> : std::true_type {};
 
-template <class Ops, class P, int kBlock, uint32_t kOps>
+// kRegroup: the kind kernels run the section/segment walks regrouped; the
+// all-shape kernel keeps one point per lane (the walk's state inside its
+// switch over every shape would spill)
+template <class Ops, class P, int kBlock, uint32_t kOps, bool kRegroup = false>
 __device__ __forceinline__ void run_tile(const double *rec, const DXform *xg, int64_t first,
                                          int64_t end, const FusedIO &io, double *srec,
                                          DXform *sx) {
@@ -61,6 +64,24 @@ __device__ __forceinline__ void run_tile(const double *rec, const DXform *xg, in
     __syncthreads();
   }
   const P &prm = *sp;
+  constexpr uint32_t kDtiSti = (1u << VGB_OP_DISTANCE_TO_IN) | (1u << VGB_OP_SAFETY_TO_IN);
+  if constexpr (kRegroup && kOps == kDtiSti && RegroupedWalk<Ops, VGB_OP_DISTANCE_TO_IN>::value) {
+    // section/segment walks: SafetyToIn one point per lane, then DistanceToIn as
+    // the warp-regrouped walk over the tile (each warp's block-stride points)
+    if ((io.ops & kDtiSti) == kDtiSti) {
+      double *sti = static_cast<double *>(io.out[VGB_OP_SAFETY_TO_IN]);
+      for (int64_t i = first + threadIdx.x; i < end; i += kBlock) {
+        const V3<double> m = {ldg(io.x + i), ldg(io.y + i), ldg(io.z + i)};
+        sti[i] = Ops::safety_to_in(prm, xf_point(*sx, m));
+      }
+      const int64_t base = first + 32 * (threadIdx.x >> 5);
+      walk_regrouped<Ops, P, VGB_OP_DISTANCE_TO_IN>(
+          prm, *sx, io, static_cast<double *>(io.out[VGB_OP_DISTANCE_TO_IN]),
+          [=](int64_t s) { return base + (int64_t)kBlock * (s >> 5) + (s & 31); }, end);
+      __syncthreads();  // the next tile overwrites the staged record
+      return;
+    }
+  }
   for (int64_t i = first + threadIdx.x; i < end; i += kBlock)
     fused_point<Ops, P, kOps>(prm, *sx, io, i);
   __syncthreads();  // the next tile overwrites the staged record
@@ -125,8 +146,8 @@ __global__ void __launch_bounds__(kBlock)
     const int64_t last = b.offset + b.count;
     const int64_t end = first + tile < last ? first + tile : last;
     const UnplacedRec u = G.unplaced[b.unplaced];
-    run_tile<Ops, P, kBlock, kOps>(G.params + u.param_off, G.xforms + b.xform, first, end, io,
-                                   srec, &sx);
+    run_tile<Ops, P, kBlock, kOps, true>(G.params + u.param_off, G.xforms + b.xform, first,
+                                         end, io, srec, &sx);
   }
 }
 

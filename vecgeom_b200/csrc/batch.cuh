@@ -130,30 +130,30 @@ __device__ __forceinline__ void batch_point(const P &prm, const DXform &X, const
 // cone sections) and polyhedron DistanceToIn/DistanceToOut (walks over
 // z-segments).  Polycone DistanceToOut keeps the plain per-lane walk: regrouped
 // it measured 4.5 % slower (most of its walks end in the start section, and the
-// per-step state round trip costs more than the idle lanes it saves).  A point's walk takes from one to all of its sections; run one
-// point per lane to the end and a warp waits for its longest walk with its
-// other lanes idle.  Here each iteration evaluates one step for the point each
+// per-step state round trip costs more than the idle lanes it saves).  A
+// point's walk takes from one to all of its sections; run one point per lane to
+// the end and a warp waits for its longest walk with its other lanes idle.  Here each iteration evaluates one step for the point each
 // lane holds, and the lanes whose walk ended (a __ballot_sync over the warp)
 // take the warp's next points at once (ranked by __popc), so the warp stays
 // full until its points run out; the steps of each point are the ones the
-// scalar function takes, so every result is the same.  A warp's points are
-// those of the grid-stride order (slot s of global warp gw is point
-// 32 gw + 32 W (s / 32) + s % 32, W warps in the grid).
+// scalar function takes, so every result is the same.  A warp owns the points
+// point_of(0), point_of(1), ... below `end` (point_of increasing, the same for
+// the whole warp); the batch kernels give it the grid-stride order (slot s of
+// global warp gw is point 32 gw + 32 W (s / 32) + s % 32, W warps in the grid),
+// the basket kernels the block-stride order of one tile.  IO holds the input
+// arrays (x, y, z, dx, dy, dz, step); out receives the distances.
 template <class Ops, int OP> struct RegroupedWalk : std::false_type {};
 template <> struct RegroupedWalk<PolyconeOps<double>, VGB_OP_DISTANCE_TO_IN> : std::true_type {};
 template <> struct RegroupedWalk<PolyhedronOps<double>, VGB_OP_DISTANCE_TO_IN> : std::true_type {};
 template <> struct RegroupedWalk<PolyhedronOps<double>, VGB_OP_DISTANCE_TO_OUT> : std::true_type {};
 
-template <class Ops, class P, int OP>
-__device__ __forceinline__ void walk_regrouped(const P &prm, const DXform &X, const BatchIO &io) {
+template <class Ops, class P, int OP, class IO, class PointOf>
+__device__ __forceinline__ void walk_regrouped(const P &prm, const DXform &X, const IO &io,
+                                               double *out, PointOf point_of, int64_t end) {
   using R = double;
   constexpr bool kIn = OP == VGB_OP_DISTANCE_TO_IN;
   constexpr unsigned kFull = 0xffffffffu;
   const int lane = threadIdx.x & 31;
-  const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  auto point_of = [&](int64_t s) { return 32 * gw + 32 * nw * (s >> 5) + (s & 31); };
-  double *out = static_cast<double *>(io.out);
   int64_t next = 0;  // the warp's next slot (warp-uniform)
   int64_t i = -1;    // the lane's point, -1: none
   V3<R> q = {0, 0, 0}, v = {0, 0, 0};
@@ -164,7 +164,7 @@ __device__ __forceinline__ void walk_regrouped(const P &prm, const DXform &X, co
     const unsigned m = __ballot_sync(kFull, free_lane);
     if (free_lane) {
       const int64_t pi = point_of(next + __popc(m & ((1u << lane) - 1u)));
-      if (pi < io.n) {
+      if (pi < end) {
         const V3<R> mq = {ldg(io.x + pi), ldg(io.y + pi), ldg(io.z + pi)};
         const V3<R> md = {ldg(io.dx + pi), ldg(io.dy + pi), ldg(io.dz + pi)};
         smax = ldg(io.step + pi);
@@ -186,7 +186,7 @@ __device__ __forceinline__ void walk_regrouped(const P &prm, const DXform &X, co
       }
     }
     next += __popc(m);
-    const bool more = point_of(next) < io.n;  // warp-uniform
+    const bool more = point_of(next) < end;  // warp-uniform
     if (!__any_sync(kFull, i >= 0) && !more) break;
     if (i >= 0) {
       bool ended;
@@ -208,7 +208,11 @@ __device__ __forceinline__ void walk_regrouped(const P &prm, const DXform &X, co
 template <class Ops, class P, int OP>
 __device__ __forceinline__ void batch_loop(const P &prm, const DXform &X, const BatchIO &io) {
   if constexpr (RegroupedWalk<Ops, OP>::value) {
-    walk_regrouped<Ops, P, OP>(prm, X, io);
+    const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    walk_regrouped<Ops, P, OP>(
+        prm, X, io, static_cast<double *>(io.out),
+        [=](int64_t s) { return 32 * gw + 32 * nw * (s >> 5) + (s & 31); }, io.n);
     return;
   }
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
