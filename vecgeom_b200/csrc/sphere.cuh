@@ -562,15 +562,17 @@ template <class R> struct SphereOps {
       // one theta cone; returns true if the point leaves through it at once
       auto theta_cone = [&](bool first, R &snside) -> bool {
         const bool cond = first ? (s.stheta > 0) : (s.eTheta < kPi);
+        // without this cone (stheta = 0, or eTheta = pi) the reference still
+        // evaluates its quantities, over zero radii, and then returns false
+        // before using any of them; a scalar lane returns at once
+        if (!cond) return false;
         const R si = (R)(first ? s.sinSTheta : s.sinETheta);
         const R ci = (R)(first ? s.cosSTheta : s.cosETheta);
-        R r1 = 0, r2 = 0, z1 = 0, z2 = 0;
-        if (cond) {
-          if (ci > zero) {
-            r1 = fRmin * si; z1 = fRmin * ci; r2 = fRmax * si; z2 = fRmax * ci;
-          } else {
-            r1 = fRmax * si; z1 = fRmax * ci; r2 = fRmin * si; z2 = fRmin * ci;
-          }
+        R r1, r2, z1, z2;
+        if (ci > zero) {
+          r1 = fRmin * si; z1 = fRmin * ci; r2 = fRmax * si; z2 = fRmax * ci;
+        } else {
+          r1 = fRmax * si; z1 = fRmax * ci; r2 = fRmin * si; z2 = fRmin * ci;
         }
         const R dz = (R)0.5 * (z2 - z1);
         const V3<R> pt = {p.x, p.y, p.z - (R)0.5 * (z1 + z2)};
@@ -580,14 +582,13 @@ template <class R> struct SphereOps {
         const bool bigequ =
             first ? ((sigz * ci > zero) && (sigz * rxy2 < sigz * rin * (rin + sigz * toler)))
                   : ((sigz * ci > zero) && (sigz * rxy2 > sigz * rin * (rin - sigz * toler)));
-        R ddotn = 0;
-        if (cond && bigequ)
-          ddotn = pt.x * v.x + pt.y * v.y + (R)0.5 * (r1 - r2) * v.z * zinv * sqrt(rxy2);
-        if (cond && bigequ && (first ? (sigz * ddotn <= zero) : (sigz * ddotn >= zero)))
-          return true;
+        if (bigequ) {
+          // on or past the cone: 0 if heading out of the solid, else no candidate here
+          const R ddotn = pt.x * v.x + pt.y * v.y + (R)0.5 * (r1 - r2) * v.z * zinv * sqrt(rxy2);
+          return first ? (sigz * ddotn <= zero) : (sigz * ddotn >= zero);
+        }
         R bv = 0, deltav = 0;
         to_cone(pt, v, dz, r1, r2, bv, deltav);
-        if (!(cond && !bigequ)) return false;
         delta = deltav;
         b = bv;
         if (!(delta > zero)) return false;
