@@ -442,7 +442,21 @@ template <class R> struct PolyhedronOps {
     d2 = dt2;
   }
 
-  // ScalarSafetyKernel (:829-849), used for SafetyToIn and SafetyToOut
+  // ScalarSafetyKernel (:829-849), used for SafetyToIn and SafetyToOut.  The
+  // walk visits the segments the reference visits (its stopping rule compares the
+  // z distance with the squared safety, and is kept) and returns the same minimum.
+  // Every quadrilateral of segment z lies in the slab zplane(z) <= z <= zplane(z+1)
+  // (its corners have those z values, except that a corner within 1e-9 of z = 0 is
+  // set to 0) and each value seg_safety2 returns is the squared distance to a point
+  // of one, so the squared z distance to the slab, less 2e-9 for those corners,
+  // bounds it from below; where that bound exceeds the running minimum (with a
+  // margin far above the rounding of either), the segment cannot lower the minimum
+  // and is not evaluated.  vmin keeps its first argument against a NaN, so an
+  // unevaluated NaN changes nothing either.
+  static VGB_HD bool may_lower(R dz, R s) {
+    const R lb = dz - (R)2e-9;
+    return !(lb > 0 && lb * lb > s + (R)1e-6 * s + (R)1e-12);
+  }
   static VGB_HD R safety(const PolyhedronP &p, const V3<R> &pt) {
     R s = Lim<R>::inf();
     const int zMax = p.nseg;
@@ -450,12 +464,14 @@ template <class R> struct PolyhedronOps {
     zi = zi < 0 ? 0 : (zi >= zMax ? zMax - 1 : zi);
     const int phiIndex = find_phi(p, pt);
     for (int z = zi; z < zMax;) {
-      s = vmin(s, seg_safety2(p, z, phiIndex, pt));
+      const R dz = vmax(zplane(p, z) - pt.z, pt.z - zplane(p, z + 1));
+      if (may_lower(dz, s)) s = vmin(s, seg_safety2(p, z, phiIndex, pt));
       ++z;
       if (zplane(p, z) - pt.z > s) break;
     }
     for (int z = zi - 1; z >= 0; --z) {
-      s = vmin(s, seg_safety2(p, z, phiIndex, pt));
+      const R dz = vmax(zplane(p, z) - pt.z, pt.z - zplane(p, z + 1));
+      if (may_lower(dz, s)) s = vmin(s, seg_safety2(p, z, phiIndex, pt));
       if (pt.z - zplane(p, z) > s) break;
     }
     endcaps_safety2(p, pt, s);
