@@ -167,3 +167,60 @@ def test_gpu_theta_cuts_match_reference(name):
     assert_exact(c.cpu().numpy()[keep], want["contains"][keep], "Contains")
     assert_exact(i.cpu().numpy()[keep], want["inside"][keep], "Inside")
     assert_distances(d.cpu().numpy()[keep], want["dti"][keep], "DistanceToIn")
+
+
+def far_rays(spec, seed, n=4096):
+    """Rays from 100 to 1000 rmax away (beyond the 100 rmax at which USolids'
+    DistanceToIn splits an outer-sphere distance and re-enters from the split
+    point, USphere.cc:685-689), aimed at random points of the radial shell;
+    a quarter start on the z axis and a quarter in the z = 0 plane."""
+    p = spec.params
+    rng = np.random.default_rng(seed)
+    tgt = np.stack(W.isotropic(rng, n)) * rng.uniform(0., p["rmax"], n)
+    u = np.stack(W.isotropic(rng, n))
+    u[:, : n // 4] = np.array([[0.], [0.], [1.]])
+    u[2, n // 4: n // 2] = 0.
+    u /= np.linalg.norm(u, axis=0)
+    start = u * rng.uniform(100. * p["rmax"], 1000. * p["rmax"], n)
+    v = tgt - start
+    v /= np.linalg.norm(v, axis=0)
+    return (tuple(np.ascontiguousarray(a) for a in start), tuple(np.ascontiguousarray(a) for a in v))
+
+
+@pytest.mark.skipif(not HAVE_REF, reason="oracle/_ref not built")
+@pytest.mark.parametrize("name", list(SPECS))
+def test_host_far_rays_match_reference(hc, name):  # noqa: F811
+    spec = SPECS[name]
+    rays = far_rays(spec, 13)
+    ref = oracle.RefLib()
+    ref.placed(oracle.ref_unplaced(ref, spec))
+    want = ref.usphere_distance_to_in(spec.params, ref.last_transform, *rays)
+    assert np.isfinite(want).mean() > 0.3
+    g = Geometry(library=hc)
+    pv = g.LogicalVolume("s", W.build_unplaced(g, spec)).Place(g.Transformation3D())
+    step = np.full(len(rays[0][0]), 1e30)
+    assert_distances(host_run(hc, g, pv, 2, *rays, step), want, "DistanceToIn (far rays)")
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not HAVE_REF, reason="oracle/_ref not built")
+@pytest.mark.parametrize("name", list(SPECS))
+def test_gpu_far_rays_match_reference(name):
+    import torch
+    import vecgeom_b200 as V
+    spec = SPECS[name]
+    rays = far_rays(spec, 13)
+    ref = oracle.RefLib()
+    ref.placed(oracle.ref_unplaced(ref, spec))
+    want = ref.usphere_distance_to_in(spec.params, ref.last_transform, *rays)
+    g = V.Geometry()
+    pv = g.LogicalVolume("s", W.build_unplaced(g, spec)).Place(g.Transformation3D())
+    g.SetWorld(pv)
+    g.CloseGeometry()
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()  # noqa: E731
+    n = len(rays[0][0])
+    d = torch.zeros(n, dtype=torch.float64, device="cuda")
+    pv.DistanceToIn(V.SOA3D(*(dev(a) for a in rays[0])), V.SOA3D(*(dev(a) for a in rays[1])),
+                    dev(np.full(n, 1e30)), d)
+    torch.cuda.synchronize()
+    assert_distances(d.cpu().numpy(), want, "DistanceToIn (far rays)")

@@ -132,6 +132,10 @@ template <class R> struct PolyhedronOps {
       const R proj = dot_n(q, dir);
       valid &= proj >= 0;
       if (!valid) continue;
+      // dt / -proj < best needs -dt < best * proj; a side farther than that by
+      // more than the rounding of either side is rejected without the division
+      // (best * 0 with best = inf is NaN, which never rejects)
+      if (-dt > best * proj * (R)(1 + 1e-12)) continue;
       dt /= -proj;
       valid &= dt < best;
       if (!valid) continue;

@@ -147,10 +147,32 @@ template <class R> struct SphereOps {
     return (x * (R)s.cosCPhi + y * (R)s.sinCPhi) / rho >= (R)limit;
   }
 
-  // Depth 1 is the re-entry after a long distance was split (:685-689); it
-  // does not split again.
-  template <int Depth>
-  static VGB_HD R dti_core(const SphereP &s, const V3<R> &p, const V3<R> &v) {
+  // The reference splits an outer-sphere hit farther than dRmax = 100 rmax
+  // (:685-689): it moves the point fTerm = sd - fmod(sd, dRmax) along the ray,
+  // runs DistanceToIn again from there (without splitting again) and carries on
+  // from the original point with sd = fTerm + that distance.  far_split decides
+  // the split with the body's own expressions; distance_to_in then runs the one
+  // body twice, from the moved point (depth 1) and from the original point with
+  // the outer distance replaced (depth 0), so the kernel holds a single copy of
+  // it.  The arithmetic is the reference's, in its order.
+  static VGB_HD bool far_split(const SphereP &s, const V3<R> &p, const V3<R> &v, R &fTerm) {
+    const R fRmax = (R)s.rmax;
+    const R dRmax = (R)100. * (R)s.rmax;
+    const R rad2 = (p.x * p.x + p.y * p.y) + p.z * p.z;
+    const R pDotV3d = (p.x * v.x + p.y * v.y) + p.z * v.z;
+    const R c = rad2 - fRmax * fRmax;
+    if (!(c > (R)s.mkTolerance * fRmax)) return false;
+    const R d2 = pDotV3d * pDotV3d - c;
+    if (!(d2 >= 0)) return false;
+    const R sd = -pDotV3d - sqrt(d2);
+    if (!(sd >= 0 && sd > dRmax)) return false;
+    fTerm = sd - fmod(sd, dRmax);
+    return true;
+  }
+
+  // depth 1: the run from the split point (no further split); depth 0: the run
+  // from the point itself, where an outer distance beyond dRmax is `outer`
+  static VGB_HD R dti_core(const SphereP &s, const V3<R> &p, const V3<R> &v, int depth, R outer) {
     const R inf = Lim<R>::inf();
     R snxt = inf;
     const R dRmax = (R)100. * (R)s.rmax;
@@ -191,14 +213,7 @@ template <class R> struct SphereOps {
       if (d2 >= 0) {
         sd = -pDotV3d - sqrt(d2);
         if (sd >= 0) {
-          if constexpr (Depth == 0) {
-            if (sd > dRmax) {
-              // :685-689 split long distances and recompute
-              const R fTerm = sd - fmod(sd, dRmax);
-              const V3<R> q = {p.x + fTerm * v.x, p.y + fTerm * v.y, p.z + fTerm * v.z};
-              sd = fTerm + dti_core<1>(s, q, v);
-            }
-          }
+          if (depth == 0 && sd > dRmax) sd = outer;  // :685-689, split and recomputed
           xi = p.x + sd * v.x;
           yi = p.y + sd * v.y;
           rhoi = sqrt(xi * xi + yi * yi);
@@ -447,7 +462,23 @@ template <class R> struct SphereOps {
   }
 
   static VGB_HD R distance_to_in(const SphereP &s, const V3<R> &p, const V3<R> &v, R) {
-    return dti_core<0>(s, p, v);
+    R fTerm = 0;
+    V3<R> from = p;
+    int depth = 0;
+    if (far_split(s, p, v, fTerm)) {
+      from = {p.x + fTerm * v.x, p.y + fTerm * v.y, p.z + fTerm * v.z};
+      depth = 1;
+    }
+    R outer = 0;
+    // one call site, so the body is inlined once
+#pragma unroll 1
+    while (true) {
+      const R r = dti_core(s, from, v, depth, outer);
+      if (depth == 0) return r;
+      outer = fTerm + r;
+      from = p;
+      depth = 0;
+    }
   }
 
   // ---- DistanceToOut: SphereImplementation.h:1267-1510 and its helpers -----
