@@ -352,7 +352,8 @@ vgb_status vgb_basket_graph_launch(vgb_basket_plan *plan, void *stream);
  *    refill it as soon as the call returns.  Launch shape: 256 threads per CTA,
  *    1024 points per tile.
  *  - The first call on each device looks up the array's device address; make
- *    that first call from a thread whose current device is the geometry's.
+ *    that first call from a thread whose current device is the geometry's,
+ *    and before any stream capture begins.
  *  - Every call reuses the same array and leaves its tables in it; nothing in
  *    it needs to start at zero, since each call writes every entry it reads.
  *    Calls whose work overlaps on the GPU (two streams, or two threads) race
