@@ -126,13 +126,11 @@ __device__ __forceinline__ void batch_point(const P &prm, const DXform &X, const
   }
 }
 
-// Distance walks with warp-regrouped steps: polycone DistanceToIn (walks over
-// cone sections) and polyhedron DistanceToIn/DistanceToOut (walks over
-// z-segments).  Polycone DistanceToOut keeps the plain per-lane walk: regrouped
-// it measured 4.5 % slower (most of its walks end in the start section, and the
-// per-step state round trip costs more than the idle lanes it saves).  A
-// point's walk takes from one to all of its sections; run one point per lane to
-// the end and a warp waits for its longest walk with its other lanes idle.  Here each iteration evaluates one step for the point each
+// Distance walks with warp-regrouped steps: polycone DistanceToIn/DistanceToOut
+// (walks over cone sections) and polyhedron DistanceToIn/DistanceToOut (walks
+// over z-segments).  A point's walk takes from one to all of its sections; run
+// one point per lane to the end and a warp waits for its longest walk with its
+// other lanes idle.  Here each iteration evaluates one step for the point each
 // lane holds, and the lanes whose walk ended (a __ballot_sync over the warp)
 // take the warp's next points at once (ranked by __popc), so the warp stays
 // full until its points run out; the steps of each point are the ones the
@@ -144,6 +142,7 @@ __device__ __forceinline__ void batch_point(const P &prm, const DXform &X, const
 // arrays (x, y, z, dx, dy, dz, step); out receives the distances.
 template <class Ops, int OP> struct RegroupedWalk : std::false_type {};
 template <> struct RegroupedWalk<PolyconeOps<double>, VGB_OP_DISTANCE_TO_IN> : std::true_type {};
+template <> struct RegroupedWalk<PolyconeOps<double>, VGB_OP_DISTANCE_TO_OUT> : std::true_type {};
 template <> struct RegroupedWalk<PolyhedronOps<double>, VGB_OP_DISTANCE_TO_IN> : std::true_type {};
 template <> struct RegroupedWalk<PolyhedronOps<double>, VGB_OP_DISTANCE_TO_OUT> : std::true_type {};
 

@@ -21,7 +21,8 @@ static int grid_for(int64_t n) {
 // from the warp's own stream of points, so they keep lanes busier when each warp
 // owns more points: a quarter of the grid above (measured: polyhedron
 // DistanceToIn/Out 7.0 k/5.7 k -> 7.9 k/7.4 k Mpoints/s, polycone DistanceToIn
-// 5.8 k -> 6.2 k), while the other kernels run fastest with the full grid.
+// 5.8 k -> 6.2 k, and polycone DistanceToOut regrouped 7.6 k, against 6.8 k on
+// one lane), while the other kernels run fastest with the full grid.
 constexpr int kWalkGridCap = 148 * 8;
 
 template <class Ops, class P>
