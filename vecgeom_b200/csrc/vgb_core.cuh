@@ -63,6 +63,39 @@ template <class R> struct V3 {
 
 template <class R> VGB_HD V3<R> mk3(R x, R y, R z) { return V3<R>{x, y, z}; }
 
+// True when the ray q + t v (t >= 0) stays farther than rb from the z axis
+// wherever zlo <= z <= zhi (or never reaches that slab).  Callers widen the slab
+// and the radius by margins far above the rounding of this test and of their own
+// arithmetic.  False for a NaN or infinite input.
+template <class R>
+VGB_HD bool ray_beyond_radius(const V3<R> &q, const V3<R> &v, R zlo, R zhi, R rb) {
+  if (!(fabs(q.x) + fabs(q.y) + fabs(q.z) + fabs(v.x) + fabs(v.y) + fabs(v.z) < Lim<R>::inf()))
+    return false;
+  R t0 = 0, t1 = Lim<R>::inf();
+  if (v.z != 0) {
+    R ta = (zlo - q.z) / v.z, tb = (zhi - q.z) / v.z;
+    if (ta > tb) {
+      const R t = ta;
+      ta = tb;
+      tb = t;
+    }
+    t0 = ta > t0 ? ta : t0;
+    t1 = tb;
+    if (t0 > t1) return true;  // the slab lies behind the point
+  } else if (q.z < zlo || q.z > zhi) {
+    return true;  // parallel to the slab, outside it
+  }
+  // the closest approach to the axis over [t0, t1]
+  const R a = v.x * v.x + v.y * v.y;
+  R tm = t0;
+  if (a > 0) {
+    tm = -(q.x * v.x + q.y * v.y) / a;
+    tm = tm < t0 ? t0 : (tm > t1 ? t1 : tm);
+  }
+  const R x = q.x + tm * v.x, y = q.y + tm * v.y;
+  return x * x + y * y > rb * rb;
+}
+
 // Placement transform as uploaded to the device.  r/t hold the *effective*
 // matrix: the entries a specialised rotation code drops
 // (base/Transformation3D.h:367-480, management/TransformationSpecializations.icc)
