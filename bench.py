@@ -692,6 +692,19 @@ def pcie_floor(h2d_bytes: int, d2h_bytes: int, reps: int = 3) -> dict:
                       "streams), wall clock like the end-to-end calls"}
 
 
+def replica_rate(points: int, step_ms: float, world: int, dist=None, device: str = "cuda"):
+    """Replicas: every rank processes its own batch of `points` per step.  The
+    job's step time is the slowest rank's (an all-reduce MAX over the ranks) and
+    the whole-job rate is world x points over it, in Mpoint-ops/s.  Returns
+    (step ms, rate)."""
+    if world > 1:
+        import torch
+        t = torch.tensor([step_ms], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        step_ms = float(t.item())
+    return step_ms, world * points / (step_ms * 1e-3) / 1e6
+
+
 def op_roofline(opname: str, points: int, seconds: float, flops_per_point, hbm_gbs: float,
                 fp64_gflops) -> dict:
     """Where one op sits: its algorithmic bytes (and flops, when counted) per
@@ -861,13 +874,9 @@ def run_shapes(args, workload: str, wls: dict, precision: str, peaks: dict, fma:
     torch.cuda.synchronize()
     clk = clocks.stop()
 
-    step_ms = float(per_task_ms.sum()) / args.steps
-    if world > 1:
-        t = torch.tensor([step_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        step_ms = float(t.item())
     pts_per_step = sum(t[2] for t in tasks)
-    value = world * pts_per_step / (step_ms * 1e-3) / 1e6
+    step_ms, value = replica_rate(pts_per_step, float(per_task_ms.sum()) / args.steps, world,
+                                  dist)
 
     # rooflines: every op, and the dominant one (largest share of the step)
     hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
